@@ -1,0 +1,313 @@
+#!/usr/bin/env python3
+"""Benchmark of the spectral-element hot path: SSP-Knoth Rosenbrock-W steps/s.
+
+Workload (default): the FP64 drop-in configuration - cubed sphere nPanel 30
+(5,400 elements), OrdPoly 4, nz 45 levels stretched quadratically to 30 km,
+2 passive tracers, dt 300 s, dry baroclinic wave + seeded theta noise;
+synthetic initial state, no I/O.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+One step = one full Rosenbrock-W step (3 stages of tendency + DSS + column
+Schur solve) of the whole grid.  With N > 1 (torchrun, one process per GPU)
+every rank advances its own ensemble member (seed + rank): the work per GPU is
+fixed ("weak"), no collective on the data path; timing is the max over ranks.
+
+Rank 0 prints one JSON line.  ``value`` is device-resident throughput
+(inputs in HBM); ``e2e`` drives the same C ABI call with a pinned host state,
+so every step includes the state's host->device and device->host copies.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cgdycore.jl_b200"))
+
+METRIC = "Rosenbrock-W steps/s @nPanel30 p4 nz45: FP64 vs mixed FP32; adjoint/fwd time"
+UNIT = "steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="dropin")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def workload_config(cfg, precision):
+    return {"workload": f"{cfg.name}: cubed sphere nPanel {cfg.nPanel} ({6 * cfg.nPanel ** 2} elements), "
+                        f"OrdPoly {cfg.OrdPoly}, nz {cfg.nz} {cfg.stretch}, NumTr {cfg.NumTr}, "
+                        f"dt {cfg.dt:g} s, SSP-Knoth Rosenbrock-W, {precision.upper()}",
+            "nPanel": cfg.nPanel, "OrdPoly": cfg.OrdPoly, "nz": cfg.nz, "NumTr": cfg.NumTr, "dt": cfg.dt,
+            "parallelism": "ensemble member per GPU",
+            "l2": "inputs larger than L2 (state 218 MB + element metric 826 MB per member)"}
+
+
+def unique_dof(cfg):
+    numg = 6 * cfg.nPanel ** 2 * cfg.OrdPoly ** 2 + 2
+    return numg * cfg.nz * (5 + cfg.NumTr)
+
+
+# ---------------------------------------------------------------------------
+def oracle_steps_per_s(cfg, nsteps, warmup, threads):
+    """The CPU restatement of the reference path (oracle/) on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from cgd_b200 import physics as Ph
+    oracle.build()
+    n = oracle.set_threads(threads)
+    z = cfg.levels()
+    o = oracle.Oracle(cfg.nPanel, cfg.OrdPoly, cfg.nz, cfg.NumTr, z, H=cfg.H,
+                      nu=Ph.hyperdiffusion(cfg.nPanel, cfg.OrdPoly), Up=cfg.Up)
+    U = o.init_state(Ph.tracer_centres(cfg.NumTr, cfg.seed_tracer) if cfg.NumTr else None)
+    Ph.theta_noise(U, cfg.theta_noise, cfg.seed_theta)
+    if warmup:
+        U = o.ros_step(U, cfg.dt, warmup)
+    t0 = time.perf_counter()
+    U = o.ros_step(U, cfg.dt, nsteps)
+    t = time.perf_counter() - t0
+    assert np.all(np.isfinite(U))
+    return nsteps / t, n
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ---------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.path = tempfile.mktemp(suffix=".csv")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(dev)], stdout=open(self.path, "w"),
+                                      stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def measured_peak_hbm():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def phase2_bytes(cfg):
+    """Algorithmic bytes of one tendency (phase-2) launch: read the stage state
+    (NV fields), the DSS'd hyperviscosity cache (5+NumTr fields), the lumped
+    mass (2 fields) and the 17-component element metric; write one tendency
+    value per DOF and field."""
+    numg = 6 * cfg.nPanel ** 2 * cfg.OrdPoly ** 2 + 2
+    S = numg * cfg.nz * 8
+    E = 6 * cfg.nPanel ** 2 * (cfg.OrdPoly + 1) ** 2 * cfg.nz * 8
+    NV = 5 + cfg.NumTr
+    return NV * S + (5 + cfg.NumTr) * S + 2 * S + 17 * E + NV * S
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the phase-2 kernel from the committed ncu summary."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "phase2_dram.json")))
+        return float(d["dram_bytes_per_launch"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, cfg, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    K = max(1, min(args.steps, 5))
+    W = 1 if args.warmup > 0 else 0
+    v, n = oracle_steps_per_s(cfg, K, W, threads)
+    sample = (f"{K} full-grid Rosenbrock-W steps after {W} warm-up step(s), C++ FP64 restatement of the "
+              f"reference CPU path (Julia is not available), OpenMP on {n} threads, {cpu_model()}")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": K, "warmup": W, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(cfg, "fp64"),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": n, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, cfg, rank, world, local):
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    os.environ.setdefault("CGD_PROFILE", "1")
+    import dataclasses
+
+    from cgd_b200 import setup
+    mcfg = dataclasses.replace(cfg, seed_theta=cfg.seed_theta + rank)
+    dyc, U0, mcfg = setup(mcfg, precision=args.precision)
+    stream = torch.cuda.ExternalStream(dyc.stream())
+    Ut = torch.from_numpy(np.ascontiguousarray(U0.transpose(2, 1, 0))).cuda()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world > 1:
+            t = torch.tensor([x], dtype=torch.float64, device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    dt = cfg.dt
+    dyc.time_stepper(Ut, dt, args.warmup)          # includes the one-time graph capture
+    barrier()
+    clocks = Clocks(local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    dyc.time_stepper(Ut, dt, args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    barrier()
+    clk = clocks.stop()
+    t = max_over_ranks(t)
+    value = world * args.steps / t
+    ktimes = dyc.kernel_times()
+    assert torch.isfinite(Ut).all().item()
+
+    # end to end through the C ABI with a pinned host state
+    Uh = torch.from_numpy(np.ascontiguousarray(U0.transpose(2, 1, 0))).pin_memory()
+    dyc.time_stepper(Uh, dt, 1)
+    barrier()
+    Ke = max(1, args.e2e_steps)
+    e0.record(stream)
+    for _ in range(Ke):
+        dyc.time_stepper(Uh, dt, 1)
+    e1.record(stream)
+    e1.synchronize()
+    te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    state_bytes = int(np.prod(U0.shape)) * 8
+    e2e = {"value": world * Ke / te, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+           "d2h_bytes_per_step": state_bytes, "steps": Ke,
+           "call": "cgd_ros_step(h, host_state, dt, 1) per step (pinned host buffer)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, n = oracle_steps_per_s(cfg, args.cpu_steps, 1, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": n, "kind": "port",
+               "sample": f"{args.cpu_steps} full-grid Rosenbrock-W steps after 1 warm-up step of the same "
+                         f"configuration; C++ FP64 restatement of the reference CPU path, OpenMP on {n} "
+                         f"threads ({cpu_model()})"}
+
+    if rank == 0:
+        peak, kind = measured_peak_hbm()
+        fam = {}
+        for name, ms in ktimes:
+            fam.setdefault(name.rstrip("0123456789"), []).append(ms)
+        p2 = fam.get("phase2", [float("nan")])
+        t_p2 = float(np.mean(p2)) / 1e3
+        b_p2 = phase2_bytes(cfg)
+        ach = b_p2 / t_p2 / 1e9
+        step_ms = t / args.steps * 1e3
+        shares = {k: round(float(np.sum(v)) / max(1e-12, sum(float(np.sum(x)) for x in fam.values())), 4)
+                  for k, v in fam.items()}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic (baroclinic wave + seeded noise)",
+            "config": workload_config(cfg, args.precision),
+            "dof_updates_per_s": value * unique_dof(cfg),
+            "roofline": {"bound": "hbm", "kernel": "k_phase2 (fused tendency)", "achieved": ach, "peak": peak,
+                         "peak_kind": kind, "unit": "GB/s", "frac": ach / peak, "traffic": ncu_traffic(),
+                         "algorithmic_bytes_per_launch": b_p2, "launch_ms": t_p2 * 1e3},
+            "kernel_ms_last_step": {k: [round(x, 4) for x in v] for k, v in fam.items()},
+            "kernel_share": shares,
+            "e2e": e2e,
+            "gpu_launches": 12 * args.steps,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    dyc.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    from cgd_b200 import physics as Ph
+    cfg = Ph.CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference(args, cfg, rank)
+        return
+    run_ours(args, cfg, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,86 @@
+"""ctypes binding of libcgd_b200.so (the sm_100a hot-path library).
+
+The library is built in tree (``__graft_entry__.build()`` or
+``python -m cgd_b200.build``); importing this module never falls back to a
+CPU implementation: if the shared library is missing, loading fails loudly.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.dirname(_HERE)
+LIB_PATH = os.path.join(PKG_DIR, "libcgd_b200.so")
+
+CGD_OK = 0
+ERRORS = {
+    -1: "CGD_ERR_INVALID_ARG", -2: "CGD_ERR_SHAPE", -3: "CGD_ERR_CUDA", -4: "CGD_ERR_NONFINITE",
+    -5: "CGD_ERR_TIMEOUT", -6: "CGD_ERR_INDEX", -7: "CGD_ERR_UNSUPPORTED", -8: "CGD_ERR_NO_DEVICE",
+}
+PREC_FP64, PREC_MIXED = 0, 1
+FLAG_CHECK_FINITE = 1
+
+# every symbol declared in include/cgd_b200.h
+EXPORTS = [
+    "cgd_create", "cgd_destroy", "cgd_prepare", "cgd_hypervisc_phase1", "cgd_rhs", "cgd_jac",
+    "cgd_schur_solve", "cgd_ros_step", "cgd_mass_integral", "cgd_get_stream", "cgd_kernel_times",
+    "cgd_strerror", "cgd_version",
+]
+
+
+class CgdConfig(ctypes.Structure):
+    _fields_ = [("OrdPoly", ctypes.c_int32), ("nz", ctypes.c_int32), ("NumTr", ctypes.c_int32),
+                ("NF", ctypes.c_int32), ("NumG", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("flags", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("Grav", ctypes.c_double), ("Rd", ctypes.c_double), ("Cpd", ctypes.c_double),
+                ("p0", ctypes.c_double), ("Omega", ctypes.c_double),
+                ("HyperDCurl", ctypes.c_double), ("HyperDGrad", ctypes.c_double),
+                ("HyperDDiv", ctypes.c_double)]
+
+
+class CgdError(RuntimeError):
+    def __init__(self, code, what=""):
+        self.code = code
+        msg = lib().cgd_strerror(code).decode() if _lib is not None else ERRORS.get(code, "error")
+        super().__init__(f"{what}: {ERRORS.get(code, code)} ({msg})")
+
+
+_lib = None
+
+
+def lib():
+    """Load the library (raises OSError if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} not found: build it with __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_double
+        L.cgd_create.argtypes = [ctypes.POINTER(CgdConfig)] + [vp] * 8 + [ctypes.POINTER(vp)]
+        L.cgd_create.restype = ctypes.c_int
+        L.cgd_destroy.argtypes = [vp]
+        L.cgd_destroy.restype = None
+        for f in ("cgd_prepare", "cgd_hypervisc_phase1", "cgd_rhs", "cgd_jac"):
+            getattr(L, f).argtypes = [vp, vp, vp]
+            getattr(L, f).restype = ctypes.c_int
+        L.cgd_schur_solve.argtypes = [vp, vp, vp, dbl]
+        L.cgd_schur_solve.restype = ctypes.c_int
+        L.cgd_ros_step.argtypes = [vp, vp, dbl, i32]
+        L.cgd_ros_step.restype = ctypes.c_int
+        L.cgd_mass_integral.argtypes = [vp, vp, vp, vp]
+        L.cgd_mass_integral.restype = ctypes.c_int
+        L.cgd_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.cgd_get_stream.restype = ctypes.c_int
+        L.cgd_kernel_times.argtypes = [vp, ctypes.c_char_p, i32, vp, i32]
+        L.cgd_kernel_times.restype = ctypes.c_int
+        L.cgd_strerror.argtypes = [ctypes.c_int]
+        L.cgd_strerror.restype = ctypes.c_char_p
+        L.cgd_version.argtypes = []
+        L.cgd_version.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def check(rc, what):
+    if rc != CGD_OK:
+        raise CgdError(rc, what)
+    return rc

@@ -1,0 +1,175 @@
+"""Host-side mirror of the reference's hot-path interface.
+
+The reference injects its GPU functions into the time loop as arguments
+(``TimeStepper!(U, GPU.FcnGPU!, GPU.FcnPrepareGPU!, DyCore.JacSchurGPU!, ...)``,
+Examples/testNHSphere.jl:508-509, src/Integration/TimeStepper.jl:1).  The
+``Dycore`` object exposes the same operations, each a single call into
+libcgd_b200.so:
+
+  ==========================  ==============================================
+  Dycore method               reference
+  ==========================  ==============================================
+  fcn_prepare(U)              GPU.FcnPrepareGPU! (DiagnosticKernel.jl:180)
+  fcn(U)                      GPU.FcnGPU!(::CompressibleShallow) (FcnGPU.jl:552)
+  hypervisc_phase1(U)         first phase of FcnGPU! (FcnGPU.jl:744-802)
+  jac(U)                      DyCore.JacSchurGPU! (JacSchur.jl:3)
+  schur_solve(v, fac)         Integration.SchurSolveGPU! (SchurSolve.jl:149)
+  rosenbrock_schur(U, dt)     Integration.RosenbrockSchur! (RosenbrockSchur.jl:1)
+  time_stepper(U, dt, n)      the Rosenbrock branch of TimeStepper! (TimeStepper.jl:103-124)
+  mass_integral(U)            Parallels.GlobalIntegral (Exchange.jl:1163)
+  ==========================  ==============================================
+
+State arrays are (nz, NumG, NV) in column-major order: a Fortran-ordered
+float64 numpy array (host memory; copied through the library's buffers) or a
+contiguous float64 CUDA torch tensor of shape (NV, NumG, nz) (device memory;
+zero copy).  Errors raise ``CgdError`` with the library's error code.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .physics import PhysParameters
+
+
+def _ptr(a, shape=None, writable=False):
+    """Raw pointer of a numpy array (Fortran float64) or a torch tensor."""
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.float64 or not a.flags.f_contiguous:
+            raise ValueError("state arrays must be Fortran-ordered float64")
+        if shape is not None and a.shape != tuple(shape):
+            raise ValueError(f"expected shape {tuple(shape)}, got {a.shape}")
+        if writable and not a.flags.writeable:
+            raise ValueError("array is read-only")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        import torch
+        if a.dtype != torch.float64 or not a.is_contiguous():
+            raise ValueError("tensors must be contiguous float64")
+        if shape is not None and a.numel() != int(np.prod(shape)):
+            raise ValueError("tensor has the wrong number of elements")
+        return a.data_ptr()
+    raise TypeError("expected a numpy array or a torch tensor")
+
+
+class Dycore:
+    """One model instance on the current CUDA device."""
+
+    def __init__(self, grid, NumTr=0, nu=(0.0, 0.0, 0.0), phys=None, precision="fp64",
+                 check_finite=False):
+        self.grid = grid
+        self.phys = phys or PhysParameters(RadEarth=grid.Rad)
+        self.nz, self.NumG, self.NF = grid.nz, grid.NumG, grid.NF
+        self.NumTr, self.NV = NumTr, 5 + NumTr
+        self.shape = (self.nz, self.NumG, self.NV)
+        L = _lib.lib()
+        cfg = _lib.CgdConfig()
+        cfg.OrdPoly, cfg.nz, cfg.NumTr = grid.OrdPoly, grid.nz, NumTr
+        cfg.NF, cfg.NumG = grid.NF, grid.NumG
+        cfg.precision = _lib.PREC_MIXED if precision == "mixed" else _lib.PREC_FP64
+        cfg.flags = _lib.FLAG_CHECK_FINITE if check_finite else 0
+        ph = self.phys
+        cfg.Grav, cfg.Rd, cfg.Cpd, cfg.p0, cfg.Omega = ph.Grav, ph.Rd, ph.Cpd, ph.p0, ph.Omega
+        cfg.HyperDCurl, cfg.HyperDGrad, cfg.HyperDDiv = nu
+        self._keep = [np.asfortranarray(x, dtype=t) for x, t in (
+            (grid.glob, np.int64), (grid.DS, np.float64), (grid.DW, np.float64),
+            (grid.dXdxI, np.float64), (grid.J, np.float64), (grid.X, np.float64),
+            (grid.M, np.float64), (grid.dz, np.float64))]
+        h = ctypes.c_void_p()
+        rc = L.cgd_create(ctypes.byref(cfg), *[k.ctypes.data for k in self._keep], ctypes.byref(h))
+        self._keep = None
+        _lib.check(rc, "cgd_create")
+        self.h = h
+        self._mmass = np.asfortranarray(grid.MMass)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lib().cgd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def new_state(self):
+        return np.zeros(self.shape, order="F")
+
+    def fcn_prepare(self, U, p=None):
+        p = np.zeros((self.nz, self.NumG), order="F") if p is None else p
+        _lib.check(_lib.lib().cgd_prepare(self.h, _ptr(U, self.shape), _ptr(p, (self.nz, self.NumG), True)),
+                   "cgd_prepare")
+        return p
+
+    def fcn(self, U, F=None):
+        F = self.new_state() if F is None else F
+        _lib.check(_lib.lib().cgd_rhs(self.h, _ptr(U, self.shape), _ptr(F, self.shape, True)), "cgd_rhs")
+        return F
+
+    def hypervisc_phase1(self, U, Temp1=None):
+        T = self.new_state() if Temp1 is None else Temp1
+        _lib.check(_lib.lib().cgd_hypervisc_phase1(self.h, _ptr(U, self.shape), _ptr(T, self.shape, True)),
+                   "cgd_hypervisc_phase1")
+        return T
+
+    def jac(self, U):
+        """Bands JRhoW, JWRho, JWRhoTh, JRhoThW as an array (4, 2, nz-1, NumG);
+        each band is the reference's (2, nz-1, NumG) JCache array."""
+        b = np.zeros(4 * 2 * (self.nz - 1) * self.NumG)
+        _lib.check(_lib.lib().cgd_jac(self.h, _ptr(U, self.shape), b.ctypes.data), "cgd_jac")
+        return b.reshape((4, self.NumG, self.nz - 1, 2)).transpose(0, 3, 2, 1)
+
+    def schur_solve(self, v, fac, k=None):
+        """k = (I/fac - J)^-1 v with the bands of the last jac(); v is updated
+        in place as by the reference."""
+        k = self.new_state() if k is None else k
+        _lib.check(_lib.lib().cgd_schur_solve(self.h, _ptr(k, self.shape, True), _ptr(v, self.shape, True),
+                                              float(fac)), "cgd_schur_solve")
+        return k
+
+    def rosenbrock_schur(self, U, dt):
+        _lib.check(_lib.lib().cgd_ros_step(self.h, _ptr(U, self.shape, True), float(dt), 1), "cgd_ros_step")
+        return U
+
+    def time_stepper(self, U, dt, nsteps):
+        _lib.check(_lib.lib().cgd_ros_step(self.h, _ptr(U, self.shape, True), float(dt), int(nsteps)),
+                   "cgd_ros_step")
+        return U
+
+    def mass_integral(self, U):
+        out = ctypes.c_double()
+        _lib.check(_lib.lib().cgd_mass_integral(self.h, _ptr(U, self.shape), self._mmass.ctypes.data,
+                                                ctypes.byref(out)), "cgd_mass_integral")
+        return out.value
+
+    def stream(self):
+        """The library's cudaStream_t as an integer handle."""
+        s = ctypes.c_void_p()
+        _lib.check(_lib.lib().cgd_get_stream(self.h, ctypes.byref(s)), "cgd_get_stream")
+        return s.value or 0
+
+    def kernel_times(self, nmax=12):
+        names = ctypes.create_string_buffer(512)
+        ms = (ctypes.c_double * nmax)()
+        n = _lib.lib().cgd_kernel_times(self.h, names, 512, ms, nmax)
+        if n < 0:
+            raise _lib.CgdError(n, "cgd_kernel_times")
+        return list(zip(names.value.decode().split(";"), list(ms)[:n]))
+
+
+def setup(cfg_name_or_cfg, precision="fp64", check_finite=False, nz=None, nPanel=None):
+    """Grid + initial state + Dycore for a named configuration
+    (physics.CONFIGS).  Returns (dycore, U0, config)."""
+    from . import grid as G
+    from . import physics as Ph
+    cfg = Ph.CONFIGS[cfg_name_or_cfg] if isinstance(cfg_name_or_cfg, str) else cfg_name_or_cfg
+    if nz is not None or nPanel is not None:
+        import dataclasses
+        cfg = dataclasses.replace(cfg, nz=nz or cfg.nz, nPanel=nPanel or cfg.nPanel)
+    phys = Ph.PhysParameters()
+    z = cfg.levels()
+    grid = G.init_grid_sphere(cfg.nPanel, cfg.OrdPoly, z, cfg.H, phys.RadEarth)
+    tl = Ph.tracer_centres(cfg.NumTr, cfg.seed_tracer) if cfg.NumTr else None
+    U = Ph.initial_state(grid, phys, cfg.NumTr, tl, cfg.Up)
+    Ph.theta_noise(U, cfg.theta_noise, cfg.seed_theta)
+    nu = Ph.hyperdiffusion(cfg.nPanel, cfg.OrdPoly)
+    dyc = Dycore(grid, cfg.NumTr, nu, phys, precision=precision, check_finite=check_finite)
+    return dyc, U, cfg

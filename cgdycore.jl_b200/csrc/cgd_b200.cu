@@ -1,0 +1,599 @@
+// cgd_b200.cu - C ABI of the B200 hot path (see include/cgd_b200.h).
+//
+// Host-side runtime: validates the caller's grid, builds the owner-gather
+// maps and the compact element metric once, owns the device work buffers and
+// the stream, and drives the kernels.  One Rosenbrock-W step (3 stages x
+// {hyperviscosity + DSS, tendency + DSS, fused column stage}) is captured
+// once into a CUDA graph and replayed per step.
+#include "../../include/cgd_b200.h"
+#include "cgd_kernels.cuh"
+#include "cgd_mixed.cuh"
+
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace cgd;
+
+namespace {
+
+constexpr int NPROF = 12;   // kernels per step whose durations are recorded
+
+struct Buf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct cgd_handle {
+  cgd_config cfg{};
+  int N = 0, DoF = 0, nz = 0, NF = 0, NumG = 0, NumTr = 0, NV = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<Buf> bufs;
+  double *met = nullptr, *M = nullptr, *dz = nullptr;
+  int *glob = nullptr, *inv_ptr = nullptr;
+  long long *inv_off = nullptr;
+  double *C = nullptr, *T1 = nullptr, *Vst = nullptr, *k1 = nullptr, *k2 = nullptr;
+  double *Ubuf = nullptr, *Fbuf = nullptr, *bands = nullptr, *part = nullptr, *scal = nullptr;
+  double *mmass = nullptr;
+  int *flag = nullptr;
+  GP gp{};
+  RK rk{};
+  bool have_bands = false;
+  // step graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  double *graph_U = nullptr;
+  double graph_dt = 0.0;
+  // profiling events (recorded inside the graph when CGD_PROFILE is set)
+  bool profile = false;
+  cudaEvent_t ev[NPROF + 1] = {};
+  // mixed precision form
+  MixedState *mixed = nullptr;
+  std::string last_error;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int cuda_fail(cgd_handle *h, cudaError_t e, const char *what)
+{
+  char buf[256];
+  snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+  g_last_error = buf;
+  if (h) h->last_error = buf;
+  return CGD_ERR_CUDA;
+}
+
+#define CK(call)                                         \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
+  } while (0)
+
+template <typename T>
+int dalloc(cgd_handle *h, T **p, size_t count)
+{
+  size_t bytes = count * sizeof(T);
+  if (bytes == 0) bytes = sizeof(T);
+  void *q = nullptr;
+  CK(cudaMalloc(&q, bytes));
+  h->bufs.push_back(Buf{q, bytes});
+  *p = static_cast<T *>(q);
+  return CGD_OK;
+}
+
+bool is_device_ptr(const void *p)
+{
+  cudaPointerAttributes a;
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+template <int N>
+void launch_hv1(cgd_handle *h, const double *U, double *C)
+{
+  constexpr int LT = 256 / (N * N);
+  dim3 grid(h->NF, (h->nz + LT - 1) / LT);
+  k_hypervisc1<N><<<grid, 256, 0, h->stream>>>(h->gp, U, C);
+}
+
+template <int N>
+void launch_p2(cgd_handle *h, const double *U, const double *T1, double *C)
+{
+  constexpr int LT = 256 / (N * N) - 1;
+  dim3 grid(h->NF, (h->nz + LT - 1) / LT);
+  k_phase2<N><<<grid, 256, 0, h->stream>>>(h->gp, U, T1, C);
+}
+
+void hv1(cgd_handle *h, const double *U, double *C)
+{
+  switch (h->N) {
+    case 2: launch_hv1<2>(h, U, C); break;
+    case 3: launch_hv1<3>(h, U, C); break;
+    case 4: launch_hv1<4>(h, U, C); break;
+    default: launch_hv1<5>(h, U, C); break;
+  }
+}
+
+void phase2(cgd_handle *h, const double *U, const double *T1, double *C)
+{
+  switch (h->N) {
+    case 2: launch_p2<2>(h, U, T1, C); break;
+    case 3: launch_p2<3>(h, U, T1, C); break;
+    case 4: launch_p2<4>(h, U, T1, C); break;
+    default: launch_p2<5>(h, U, T1, C); break;
+  }
+}
+
+void gather(cgd_handle *h, const double *C, double *out)
+{
+  long long n = (long long)h->nz * h->NumG;
+  k_gather<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->gp, C, out);
+}
+
+template <int MODE>
+void column(cgd_handle *h, const ColArgs &a)
+{
+  size_t smem = (size_t)COL_WARPS * COL_NARR * 64 * sizeof(double);
+  k_column<MODE><<<(h->NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, h->stream>>>(h->gp, a);
+}
+
+void rec(cgd_handle *h, int i)
+{
+  if (h->profile) cudaEventRecord(h->ev[i], h->stream);
+}
+
+// One SSP-Knoth step on device state U (in place).
+void enqueue_step(cgd_handle *h, double *U, double dt)
+{
+  ColArgs a{};
+  a.Vn = U;
+  a.k1 = h->k1;
+  a.k2 = h->k2;
+  a.dt = dt;
+  a.fac = dt * h->rk.gamma;
+  a.rk = h->rk;
+  a.C = h->C;
+  int e = 0;
+  rec(h, e++);
+  for (int stage = 0; stage < 3; ++stage) {
+    const double *Vsrc = stage == 0 ? U : h->Vst;
+    hv1(h, Vsrc, h->C);
+    rec(h, e++);
+    gather(h, h->C, h->T1);
+    rec(h, e++);
+    phase2(h, Vsrc, h->T1, h->C);
+    rec(h, e++);
+    if (stage == 0) {
+      a.kout = h->k1; a.Vout = h->Vst;
+      column<0>(h, a);
+    } else if (stage == 1) {
+      a.kout = h->k2; a.Vout = h->Vst;
+      column<1>(h, a);
+    } else {
+      a.kout = nullptr; a.Vout = U;
+      column<2>(h, a);
+    }
+    rec(h, e++);
+  }
+}
+
+void free_graph(cgd_handle *h)
+{
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->gexec = nullptr;
+  h->graph = nullptr;
+  h->graph_U = nullptr;
+}
+
+int check_cfg(const cgd_config *c)
+{
+  if (!c) return CGD_ERR_INVALID_ARG;
+  if (c->OrdPoly < 1 || c->OrdPoly > 4) return CGD_ERR_UNSUPPORTED;
+  if (c->nz < 2 || c->nz > 64) return CGD_ERR_UNSUPPORTED;
+  if (c->NumTr < 0 || c->NumTr > MAXTR) return CGD_ERR_UNSUPPORTED;
+  if (c->NF <= 0 || c->NumG <= 0) return CGD_ERR_SHAPE;
+  if (c->precision != CGD_PREC_FP64 && c->precision != CGD_PREC_MIXED) return CGD_ERR_INVALID_ARG;
+  if (!(c->Rd > 0) || !(c->Cpd > c->Rd) || !(c->p0 > 0) || !(c->Grav > 0)) return CGD_ERR_INVALID_ARG;
+  return CGD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *cgd_version(void)
+{
+  return "cgd_b200 1.0 (sm_100a, FP64 owner-gather DSS, -fmad=false)";
+}
+
+const char *cgd_strerror(int code)
+{
+  switch (code) {
+    case CGD_OK: return "ok";
+    case CGD_ERR_INVALID_ARG: return "invalid argument";
+    case CGD_ERR_SHAPE: return "extents inconsistent with the grid";
+    case CGD_ERR_CUDA: return g_last_error.empty() ? "CUDA runtime error" : g_last_error.c_str();
+    case CGD_ERR_NONFINITE: return "non-finite value in the state";
+    case CGD_ERR_TIMEOUT: return "bounded device wait timed out";
+    case CGD_ERR_INDEX: return "Glob index out of range or global DOF without element";
+    case CGD_ERR_UNSUPPORTED: return "option not supported by this build";
+    case CGD_ERR_NO_DEVICE: return "no usable CUDA device";
+    default: return "unknown error";
+  }
+}
+
+int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, const double *DW,
+               const double *dXdxI, const double *J, const double *X, const double *M,
+               const double *dz, cgd_handle **out)
+{
+  if (!out) return CGD_ERR_INVALID_ARG;
+  *out = nullptr;
+  int rc = check_cfg(cfg);
+  if (rc) return rc;
+  if (!glob || !DS || !DW || !dXdxI || !J || !X || !M || !dz) return CGD_ERR_INVALID_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return CGD_ERR_NO_DEVICE;
+  }
+  cgd_handle *h = new cgd_handle();
+  h->cfg = *cfg;
+  h->N = cfg->OrdPoly + 1;
+  h->DoF = h->N * h->N;
+  h->nz = cfg->nz;
+  h->NF = cfg->NF;
+  h->NumG = cfg->NumG;
+  h->NumTr = cfg->NumTr;
+  h->NV = 5 + cfg->NumTr;
+  const int DoF = h->DoF, nz = h->nz, NF = h->NF, NumG = h->NumG, NV = h->NV, N = h->N;
+  cudaGetDevice(&h->device);
+
+  // ---- owner-gather map: contributors of each global DOF, ascending (IF, ID)
+  std::vector<int> cnt(NumG + 1, 0);
+  for (size_t i = 0; i < (size_t)DoF * NF; ++i) {
+    int64_t g = glob[i];
+    if (g < 1 || g > NumG) { delete h; return CGD_ERR_INDEX; }
+    cnt[g] += 1;
+  }
+  std::vector<int> ptr(NumG + 1, 0);
+  for (int g = 0; g < NumG; ++g) {
+    if (cnt[g + 1] == 0) { delete h; return CGD_ERR_INDEX; }
+    ptr[g + 1] = ptr[g] + cnt[g + 1];
+  }
+  std::vector<long long> off(ptr[NumG]);
+  std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+  std::vector<int> glob0((size_t)DoF * NF);
+  for (int IF = 0; IF < NF; ++IF)
+    for (int ID = 0; ID < DoF; ++ID) {
+      int g = (int)glob[ID + (size_t)DoF * IF] - 1;
+      glob0[ID + (size_t)DoF * IF] = g;
+      off[fill[g]++] = ((long long)IF * NV * DoF + ID) * nz;
+    }
+
+  // ---- compact metric [IF][comp][ID][nz]
+  const size_t ENL = (size_t)DoF * nz * NF;
+  std::vector<double> met(ENL * NCOMP);
+  const double Omega2 = 2.0 * cfg->Omega;
+  for (int IF = 0; IF < NF; ++IF)
+    for (int ID = 0; ID < DoF; ++ID)
+      for (int Iz = 0; Iz < nz; ++Iz) {
+        auto dx = [&](int a, int b, int K) {
+          return dXdxI[(size_t)(a - 1) + 3 * ((b - 1) + 3 * (K + 2 * (ID + (size_t)DoF * (Iz + (size_t)nz * IF))))];
+        };
+        auto jj = [&](int K) { return J[ID + (size_t)DoF * (K + 2 * (Iz + (size_t)nz * IF))]; };
+        auto xx = [&](int K, int c) { return X[ID + (size_t)DoF * (K + 2 * (c + 3 * (Iz + (size_t)nz * IF)))]; };
+        double v[NCOMP];
+        v[C_D11_0] = dx(1, 1, 0); v[C_D11_1] = dx(1, 1, 1);
+        v[C_D12_0] = dx(1, 2, 0); v[C_D12_1] = dx(1, 2, 1);
+        v[C_D21_0] = dx(2, 1, 0); v[C_D21_1] = dx(2, 1, 1);
+        v[C_D22_0] = dx(2, 2, 0); v[C_D22_1] = dx(2, 2, 1);
+        v[C_D31_0] = dx(3, 1, 0); v[C_D31_1] = dx(3, 1, 1);
+        v[C_D32_0] = dx(3, 2, 0); v[C_D32_1] = dx(3, 2, 1);
+        v[C_D33_0] = dx(3, 3, 0); v[C_D33_1] = dx(3, 3, 1);
+        v[C_J0] = jj(0); v[C_J1] = jj(1);
+        // CoriolisShallow at the layer midpoint (src/GPU/Coriolis.jl:18-28,
+        // src/GPU/MomentumKernel.jl:156-159)
+        double x = 0.5 * (xx(0, 0) + xx(1, 0));
+        double y = 0.5 * (xx(0, 1) + xx(1, 1));
+        double z = 0.5 * (xx(0, 2) + xx(1, 2));
+        double sinlat = z / std::sqrt(x * x + y * y + z * z);
+        v[C_FCOR] = Omega2 * sinlat;
+        for (int c = 0; c < NCOMP; ++c) met[(((size_t)IF * NCOMP + c) * DoF + ID) * nz + Iz] = v[c];
+      }
+
+  // ---- device resources
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete h;
+    return CGD_ERR_CUDA;
+  }
+  const size_t S = (size_t)nz * NumG;
+#define TRY(x) do { int r_ = (x); if (r_) { cgd_destroy(h); return r_; } } while (0)
+  TRY(dalloc(h, &h->met, met.size()));
+  TRY(dalloc(h, &h->M, 2 * S));
+  TRY(dalloc(h, &h->dz, S));
+  TRY(dalloc(h, &h->glob, glob0.size()));
+  TRY(dalloc(h, &h->inv_ptr, ptr.size()));
+  TRY(dalloc(h, &h->inv_off, off.size()));
+  TRY(dalloc(h, &h->C, ENL * NV));
+  TRY(dalloc(h, &h->T1, S * NV));
+  TRY(dalloc(h, &h->Vst, S * NV));
+  TRY(dalloc(h, &h->k1, S * NV));
+  TRY(dalloc(h, &h->k2, S * NV));
+  TRY(dalloc(h, &h->Ubuf, S * NV));
+  TRY(dalloc(h, &h->Fbuf, S * NV));
+  TRY(dalloc(h, &h->bands, 8 * (size_t)(nz - 1) * NumG));
+  TRY(dalloc(h, &h->part, 1024));
+  TRY(dalloc(h, &h->scal, 4));
+  TRY(dalloc(h, &h->mmass, S));
+  TRY(dalloc(h, &h->flag, 4));
+  auto up = [&](void *dst, const void *src, size_t bytes) {
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
+  };
+  if (up(h->met, met.data(), met.size() * 8) || up(h->M, M, 2 * S * 8) || up(h->dz, dz, S * 8) ||
+      up(h->glob, glob0.data(), glob0.size() * 4) || up(h->inv_ptr, ptr.data(), ptr.size() * 4) ||
+      up(h->inv_off, off.data(), off.size() * 8)) {
+    cudaError_t e = cudaGetLastError();
+    cuda_fail(h, e, "cgd_create upload");
+    cgd_destroy(h);
+    return CGD_ERR_CUDA;
+  }
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+    cuda_fail(h, cudaGetLastError(), "cgd_create sync");
+    cgd_destroy(h);
+    return CGD_ERR_CUDA;
+  }
+
+  GP &P = h->gp;
+  P.N = N; P.DoF = DoF; P.nz = nz; P.NF = NF; P.NumG = NumG; P.NumTr = h->NumTr; P.NV = NV;
+  P.met = h->met; P.M = h->M; P.dz = h->dz; P.glob = h->glob; P.inv_ptr = h->inv_ptr; P.inv_off = h->inv_off;
+  for (int i = 0; i < 25; ++i) { P.D[i] = 0.0; P.DW[i] = 0.0; }
+  for (int i = 0; i < N * N; ++i) { P.D[i] = DS[i]; P.DW[i] = DW[i]; }
+  P.Grav = cfg->Grav; P.Rd = cfg->Rd; P.p0 = cfg->p0; P.kappa = cfg->Rd / cfg->Cpd;
+  P.nuCurl = cfg->HyperDCurl; P.nuGrad = cfg->HyperDGrad; P.nuDiv = cfg->HyperDDiv;
+
+  // SSP-Knoth: a = alpha/Gamma, c = -inv(Gamma), m = Gamma'\b (RosenbrockMethod.jl:26-47)
+  RK &r = h->rk;
+  memset(&r, 0, sizeof r);
+  r.a[1][0] = 1.0; r.a[2][0] = 0.25; r.a[2][1] = 0.25;
+  r.c[1][0] = 0.0; r.c[2][0] = -0.75; r.c[2][1] = -0.75;
+  double b1 = 1.0 / 6.0, b2 = 1.0 / 6.0, b3 = 2.0 / 3.0;
+  r.m[2] = b3 / 1.0;
+  r.m[1] = (b2 - (-0.75) * r.m[2]) / 1.0;
+  r.m[0] = (b1 - (-0.75) * r.m[2]) / 1.0;
+  r.gamma = 1.0;
+
+  const char *pe = getenv("CGD_PROFILE");
+  h->profile = pe && pe[0] == '1';
+  if (h->profile)
+    for (int i = 0; i <= NPROF; ++i) cudaEventCreate(&h->ev[i]);
+
+  if (cfg->precision == CGD_PREC_MIXED) {
+    int mrc = mixed_create(h->mixed, P, h->stream, X, dz);
+    if (mrc) { cgd_destroy(h); return mrc; }
+  }
+#undef TRY
+  *out = h;
+  return CGD_OK;
+}
+
+void cgd_destroy(cgd_handle *h)
+{
+  if (!h) return;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_graph(h);
+  if (h->mixed) mixed_destroy(h->mixed);
+  for (auto &b : h->bufs) cudaFree(b.p);
+  for (int i = 0; i <= NPROF; ++i)
+    if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+// Stage a state/tendency pointer: device pointers are used in place, host
+// pointers are copied into the handle's buffer (in == true) first.
+static int stage_in(cgd_handle *h, const double *p, double *buf, bool copy, double **dev)
+{
+  if (is_device_ptr(p)) {
+    *dev = const_cast<double *>(p);
+    return CGD_OK;
+  }
+  if (copy) CK(cudaMemcpyAsync(buf, p, (size_t)h->nz * h->NumG * h->NV * 8, cudaMemcpyHostToDevice, h->stream));
+  *dev = buf;
+  return CGD_OK;
+}
+
+static int finish(cgd_handle *h)
+{
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
+  return CGD_OK;
+}
+
+int cgd_prepare(cgd_handle *h, const double *U, double *p)
+{
+  if (!h || !U || !p) return CGD_ERR_INVALID_ARG;
+  double *Ud;
+  int rc = stage_in(h, U, h->Ubuf, true, &Ud);
+  if (rc) return rc;
+  bool pdev = is_device_ptr(p);
+  double *pd = pdev ? p : h->Fbuf;
+  long long n = (long long)h->nz * h->NumG;
+  k_pressure<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->gp, Ud, pd);
+  if (!pdev) CK(cudaMemcpyAsync(p, pd, n * 8, cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
+}
+
+int cgd_hypervisc_phase1(cgd_handle *h, const double *U, double *Temp1)
+{
+  if (!h || !U || !Temp1) return CGD_ERR_INVALID_ARG;
+  double *Ud;
+  int rc = stage_in(h, U, h->Ubuf, true, &Ud);
+  if (rc) return rc;
+  bool tdev = is_device_ptr(Temp1);
+  double *td = tdev ? Temp1 : h->Fbuf;
+  hv1(h, Ud, h->C);
+  gather(h, h->C, td);
+  if (!tdev)
+    CK(cudaMemcpyAsync(Temp1, td, (size_t)h->nz * h->NumG * h->NV * 8, cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
+}
+
+int cgd_rhs(cgd_handle *h, const double *U, double *F)
+{
+  if (!h || !U || !F) return CGD_ERR_INVALID_ARG;
+  if (h->mixed) return mixed_rhs(h->mixed, h->gp, U, F, h->Ubuf, h->Fbuf) ? CGD_ERR_CUDA : CGD_OK;
+  double *Ud;
+  int rc = stage_in(h, U, h->Ubuf, true, &Ud);
+  if (rc) return rc;
+  bool fdev = is_device_ptr(F);
+  double *fd = fdev ? F : h->Fbuf;
+  hv1(h, Ud, h->C);
+  gather(h, h->C, h->T1);
+  phase2(h, Ud, h->T1, h->C);
+  gather(h, h->C, fd);
+  if (!fdev) CK(cudaMemcpyAsync(F, fd, (size_t)h->nz * h->NumG * h->NV * 8, cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
+}
+
+int cgd_jac(cgd_handle *h, const double *U, double *bands)
+{
+  if (!h || !U) return CGD_ERR_INVALID_ARG;
+  double *Ud;
+  int rc = stage_in(h, U, h->Ubuf, true, &Ud);
+  if (rc) return rc;
+  long long n = (long long)(h->nz - 1) * h->NumG;
+  k_jac<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->gp, Ud, h->bands);
+  if (bands) {
+    size_t bytes = (size_t)8 * (h->nz - 1) * h->NumG * 8;
+    CK(cudaMemcpyAsync(bands, h->bands, bytes, is_device_ptr(bands) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                       h->stream));
+  }
+  rc = finish(h);
+  if (!rc) h->have_bands = true;
+  return rc;
+}
+
+int cgd_schur_solve(cgd_handle *h, double *k, double *v, double fac)
+{
+  if (!h || !k || !v || !(fac > 0)) return CGD_ERR_INVALID_ARG;
+  if (!h->have_bands) return CGD_ERR_INVALID_ARG;
+  double *vd, *kd;
+  int rc = stage_in(h, v, h->Ubuf, true, &vd);
+  if (rc) return rc;
+  bool kdev = is_device_ptr(k);
+  kd = kdev ? k : h->Fbuf;
+  ColArgs a{};
+  a.v = vd;
+  a.kout = kd;
+  a.bands = h->bands;
+  a.fac = fac;
+  a.dt = fac;
+  column<3>(h, a);
+  size_t bytes = (size_t)h->nz * h->NumG * h->NV * 8;
+  if (!kdev) CK(cudaMemcpyAsync(k, kd, bytes, cudaMemcpyDeviceToHost, h->stream));
+  if (vd != v) CK(cudaMemcpyAsync(v, vd, bytes, cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
+}
+
+int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps)
+{
+  if (!h || !U || !(dt > 0) || nsteps < 0) return CGD_ERR_INVALID_ARG;
+  if (h->mixed) return mixed_ros_step(h->mixed, h->gp, U, dt, nsteps, h->Ubuf);
+  double *Ud;
+  int rc = stage_in(h, U, h->Ubuf, true, &Ud);
+  if (rc) return rc;
+  if (!h->gexec || h->graph_U != Ud || h->graph_dt != dt) {
+    free_graph(h);
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(h, Ud, dt);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &h->graph);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+    CK(cudaGraphInstantiate(&h->gexec, h->graph, 0));
+    h->graph_U = Ud;
+    h->graph_dt = dt;
+  }
+  for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(h->gexec, h->stream));
+  if (h->cfg.flags & CGD_FLAG_CHECK_FINITE) {
+    CK(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+    long long n = (long long)h->nz * h->NumG * h->NV;
+    k_nonfinite<<<1184, 256, 0, h->stream>>>(Ud, n, h->flag);
+  }
+  if (Ud != U)
+    CK(cudaMemcpyAsync(U, Ud, (size_t)h->nz * h->NumG * h->NV * 8, cudaMemcpyDeviceToHost, h->stream));
+  rc = finish(h);
+  if (rc) return rc;
+  if (h->cfg.flags & CGD_FLAG_CHECK_FINITE) {
+    int f = 0;
+    CK(cudaMemcpy(&f, h->flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (f) return CGD_ERR_NONFINITE;
+  }
+  return CGD_OK;
+}
+
+int cgd_mass_integral(cgd_handle *h, const double *U, const double *MMass, double *out)
+{
+  if (!h || !U || !MMass || !out) return CGD_ERR_INVALID_ARG;
+  double *Ud;
+  int rc = stage_in(h, U, h->Ubuf, true, &Ud);
+  if (rc) return rc;
+  const size_t S = (size_t)h->nz * h->NumG;
+  const double *mm = MMass;
+  if (!is_device_ptr(MMass)) {
+    CK(cudaMemcpyAsync(h->mmass, MMass, S * 8, cudaMemcpyHostToDevice, h->stream));
+    mm = h->mmass;
+  }
+  const int nb = 592;
+  k_mass_partial<<<nb, 256, 0, h->stream>>>(Ud, mm, (long long)S, h->part);
+  k_mass_final<<<1, 32, 0, h->stream>>>(h->part, nb, h->scal);
+  CK(cudaMemcpyAsync(out, h->scal, 8, cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
+}
+
+int cgd_get_stream(cgd_handle *h, void **stream)
+{
+  if (!h || !stream) return CGD_ERR_INVALID_ARG;
+  *stream = (void *)h->stream;
+  return CGD_OK;
+}
+
+int cgd_kernel_times(cgd_handle *h, char *names, int32_t names_len, double *ms, int32_t nmax)
+{
+  if (!h || !ms) return CGD_ERR_INVALID_ARG;
+  if (!h->profile) return CGD_ERR_UNSUPPORTED;
+  static const char *nm[NPROF] = {"hypervisc1", "gather", "phase2", "column1", "hypervisc1", "gather",
+                                  "phase2", "column2", "hypervisc1", "gather", "phase2", "column3"};
+  std::string all;
+  int n = nmax < NPROF ? nmax : NPROF;
+  for (int i = 0; i < n; ++i) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, h->ev[i], h->ev[i + 1]) != cudaSuccess) {
+      cudaGetLastError();
+      t = -1.f;
+    }
+    ms[i] = t;
+    all += nm[i];
+    if (i + 1 < n) all += ";";
+  }
+  if (names && names_len > 0) {
+    strncpy(names, all.c_str(), names_len - 1);
+    names[names_len - 1] = 0;
+  }
+  return n;
+}
+
+}  // extern "C"

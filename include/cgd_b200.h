@@ -1,0 +1,131 @@
+/*
+ * cgd_b200.h - C ABI of the B200 (sm_100a) implementation of CGDycore.jl's
+ * nonhydrostatic spectral-element hot path: the tendency (RHS) with its two
+ * direct-stiffness summations, the vertical acoustic Jacobian, the column
+ * Schur/tridiagonal solve and the SSP-Knoth Rosenbrock-W step.
+ *
+ * Plain pointers and sizes only.  Arrays use the reference's column-major
+ * (Julia) layouts, so a caller holding the reference's arrays passes them
+ * unchanged:
+ *   Glob   int64 (N*N, NF), 1-based                 CG.Glob
+ *   DS, DW (N, N)                                   CG.DS, CG.DW
+ *   dXdxI  (3, 3, 2, N*N, nz, NF)                   Metric.dXdxI
+ *   J      (N*N, 2, nz, NF)                         Metric.J
+ *   X      (N*N, 2, 3, nz, NF)                      Metric.X
+ *   M      (nz, NumG, 2)                            CG.M
+ *   dz     (nz, NumG)                               Metric.dz
+ *   U,F,k,v (nz, NumG, NV), NV = 5 + NumTr          state / tendency
+ *           fields: rho, u, v, w (at the top interface of each layer),
+ *           rho*theta, rho*q_1 ... rho*q_NumTr
+ *
+ * State/tendency pointers may be device memory (zero copy, e.g. a CuArray
+ * or a torch tensor) or host memory (staged through device buffers owned by
+ * the handle); the library tells them apart with cudaPointerGetAttributes.
+ * Every call is ordered on the handle's CUDA stream and returns when the
+ * result is complete.  A handle is not thread safe.
+ *
+ * Every function returns CGD_OK (0) or a negative error code; no exception
+ * crosses the ABI and no device trap is used.  cgd_strerror() names a code.
+ */
+#ifndef CGD_B200_H
+#define CGD_B200_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CGD_OK 0
+#define CGD_ERR_INVALID_ARG -1      /* null pointer, bad size or option */
+#define CGD_ERR_SHAPE -2            /* extents inconsistent with the grid */
+#define CGD_ERR_CUDA -3             /* a CUDA runtime call failed */
+#define CGD_ERR_NONFINITE -4        /* NaN/Inf detected in the state */
+#define CGD_ERR_TIMEOUT -5          /* a bounded device wait gave up */
+#define CGD_ERR_INDEX -6            /* Glob entry out of range / unused id */
+#define CGD_ERR_UNSUPPORTED -7      /* option not built into this library */
+#define CGD_ERR_NO_DEVICE -8        /* no usable CUDA device */
+
+#define CGD_PREC_FP64 0             /* everything in FP64 */
+#define CGD_PREC_MIXED 1            /* FP32 perturbations, FP64 reference/column */
+
+#define CGD_FLAG_CHECK_FINITE 1     /* cgd_ros_step scans the state for NaN/Inf */
+
+typedef struct cgd_config {
+  int32_t OrdPoly;     /* p; N = p + 1 GLL nodes per direction (1 <= p <= 4) */
+  int32_t nz;          /* layers (2 <= nz <= 64) */
+  int32_t NumTr;       /* passive tracers (0 <= NumTr <= 4) */
+  int32_t NF;          /* elements */
+  int32_t NumG;        /* horizontal global DOFs */
+  int32_t precision;   /* CGD_PREC_* */
+  int32_t flags;       /* CGD_FLAG_* */
+  int32_t reserved;
+  /* PhysParameters (src/DyCore/GlobalVariables.jl:188-230) */
+  double Grav, Rd, Cpd, p0, Omega;
+  /* hyperdiffusion coefficients (Model.HyperDCurl/HyperDGrad/HyperDDiv) */
+  double HyperDCurl, HyperDGrad, HyperDDiv;
+} cgd_config;
+
+typedef struct cgd_handle cgd_handle;
+
+/* Builds the device-side grid: owner-gather maps from Glob, the compact
+ * element metric, lumped mass, dz and the Coriolis parameter at layer
+ * midpoints.  Host pointers; nothing is kept after the call.
+ * Replaces DyCore.InitSphere's device arrays (src/DyCore/InitDriver.jl:1-55,
+ * src/DyCore/DiscretizationCG.jl:1-78) as consumed by the hot path. */
+int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS,
+               const double *DW, const double *dXdxI, const double *J,
+               const double *X, const double *M, const double *dz,
+               cgd_handle **out);
+void cgd_destroy(cgd_handle *h);
+
+/* Pressure p (nz, NumG) from the state.
+ * Replaces GPU.FcnPrepareGPU! / PressureKernel! (src/GPU/DiagnosticKernel.jl:96-115,180-218). */
+int cgd_prepare(cgd_handle *h, const double *U, double *p);
+
+/* Phase-1 hyperviscosity with its DSS: Temp1 (nz, NumG, 5 + NumTr).
+ * Replaces HyperViscKernel!/HyperViscTracerKernel! + the first
+ * ExchangeData3D (src/GPU/ViscKernel.jl:1-84,169-218; src/GPU/FcnGPU.jl:744-802). */
+int cgd_hypervisc_phase1(cgd_handle *h, const double *U, double *Temp1);
+
+/* Tendency F = Fcn(U) including FcnPrepare (pressure in register).
+ * Replaces GPU.FcnGPU!(F,U,...,::CompressibleShallow) (src/GPU/FcnGPU.jl:552-968). */
+int cgd_rhs(cgd_handle *h, const double *U, double *F);
+
+/* Vertical acoustic Jacobian bands from U, kept in the handle; optionally
+ * copied to bands (4, 2, nz-1, NumG) = JRhoW, JWRho, JWRhoTh, JRhoThW.
+ * Replaces DyCore.JacSchurGPU! (src/DyCore/JacSchur.jl:3-75). */
+int cgd_jac(cgd_handle *h, const double *U, double *bands);
+
+/* Column Schur solve with the bands of the last cgd_jac: k from v (v is
+ * overwritten as in the reference), fac = dt*gamma.
+ * Replaces Integration.SchurSolveGPU! (src/Integration/SchurSolve.jl:149-177). */
+int cgd_schur_solve(cgd_handle *h, double *k, double *v, double fac);
+
+/* nsteps SSP-Knoth Rosenbrock-W steps of size dt, in place.  One step is a
+ * captured CUDA graph (3 stages x {hyperviscosity+DSS, tendency+DSS,
+ * fused column Schur solve}).
+ * Replaces Integration.RosenbrockSchur! (src/Integration/RosenbrockSchur.jl:1-33)
+ * inside TimeStepper! (src/Integration/TimeStepper.jl:103-124). */
+int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps);
+
+/* sum(rho * MMass) over all DOFs, reduced in FP64 on the device (MMass is
+ * the caller's lumped quadrature mass (nz, NumG)).
+ * Replaces Parallels.GlobalIntegral (src/Parallels/Exchange.jl:1163-1166). */
+int cgd_mass_integral(cgd_handle *h, const double *U, const double *MMass, double *out);
+
+/* The handle's CUDA stream (cudaStream_t) so a caller can order its own
+ * work or timing events with the library's.  No counterpart in the
+ * reference (KernelAbstractions owns its queue). */
+int cgd_get_stream(cgd_handle *h, void **stream);
+
+/* Average duration (ms) of the last timed launches of each kernel family
+ * recorded when CGD_PROFILE=1; names separated by ';'.  Diagnostics only. */
+int cgd_kernel_times(cgd_handle *h, char *names, int32_t names_len, double *ms, int32_t nmax);
+
+const char *cgd_strerror(int code);
+/* Library build string (arch, options). */
+const char *cgd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CGD_B200_H */

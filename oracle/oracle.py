@@ -1,0 +1,188 @@
+"""ctypes wrapper of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+The oracle is an FP64 CPU restatement of CGDycore.jl's spectral-element hot
+path (see cgd_oracle.cpp for the file:line of every restated function).  It is
+used by the tests, by ``__graft_entry__.smoke()`` and by the CPU-baseline leg
+of ``bench.py`` to check the product; the product never imports it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libcgd_oracle.so")
+_lib = None
+
+
+class OrcCfg(ctypes.Structure):
+    _fields_ = [("nPanel", ctypes.c_int), ("OrdPoly", ctypes.c_int), ("nz", ctypes.c_int),
+                ("NumTr", ctypes.c_int), ("Rad", ctypes.c_double), ("H", ctypes.c_double),
+                ("HyperDCurl", ctypes.c_double), ("HyperDGrad", ctypes.c_double),
+                ("HyperDDiv", ctypes.c_double), ("Up", ctypes.c_double)]
+
+
+def build():
+    """Compile the oracle library in place (make)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        vp = ctypes.c_void_p
+        L.orc_create.restype = vp
+        L.orc_create.argtypes = [ctypes.POINTER(OrcCfg), vp]
+        L.orc_destroy.argtypes = [vp]
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_set_threads.restype = ctypes.c_int
+        for f in ["orc_sizes", "orc_get_glob", "orc_get_faces", "orc_get_dz"]:
+            getattr(L, f).argtypes = [vp, vp]
+        L.orc_get_gll.argtypes = [vp, vp, vp, vp, vp]
+        L.orc_get_metric.argtypes = [vp, vp, vp, vp]
+        L.orc_get_mass.argtypes = [vp, vp, vp]
+        L.orc_set_metric.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.orc_init_state.argtypes = [vp, vp, vp]
+        for f in ["orc_pressure", "orc_hypervisc1", "orc_rhs", "orc_jac"]:
+            getattr(L, f).argtypes = [vp, vp, vp]
+        L.orc_schur.argtypes = [vp, vp, vp, ctypes.c_double]
+        L.orc_ros_step.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int]
+        L.orc_mass_integral.argtypes = [vp, vp]
+        L.orc_mass_integral.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+def set_threads(n):
+    return lib().orc_set_threads(int(n))
+
+
+def _p(a):
+    return a.ctypes.data
+
+
+class Oracle:
+    """One oracle model instance (grid, metric, mass, tendencies, steps)."""
+
+    def __init__(self, nPanel, OrdPoly, nz, NumTr, zlev, Rad=6.371e6, H=30000.0,
+                 nu=(0.0, 0.0, 0.0), Up=1.0):
+        zlev = np.ascontiguousarray(zlev, dtype=np.float64)
+        assert zlev.size == nz + 1
+        cfg = OrcCfg(nPanel, OrdPoly, nz, NumTr, Rad, H, nu[0], nu[1], nu[2], Up)
+        self.h = lib().orc_create(ctypes.byref(cfg), _p(zlev))
+        if not self.h:
+            raise ValueError("orc_create failed")
+        s = np.zeros(6, np.int64)
+        lib().orc_sizes(self.h, _p(s))
+        self.NF, self.NumG, self.DoF, self.N, self.NumNodes, self.NumEdges = (int(x) for x in s)
+        self.nz, self.NumTr, self.NV = nz, NumTr, 5 + NumTr
+        self.nPanel, self.OrdPoly = nPanel, OrdPoly
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    # arrays are returned in Fortran order with the reference's shapes
+    def glob(self):
+        g = np.zeros(self.DoF * self.NF, np.int64)
+        lib().orc_get_glob(self.h, _p(g))
+        return g.reshape((self.DoF, self.NF), order="F")
+
+    def gll(self):
+        N = self.N
+        xw, w = np.zeros(N), np.zeros(N)
+        DS, DW = np.zeros(N * N), np.zeros(N * N)
+        lib().orc_get_gll(self.h, _p(xw), _p(w), _p(DS), _p(DW))
+        return xw, w, DS.reshape((N, N), order="F"), DW.reshape((N, N), order="F")
+
+    def faces(self):
+        F = np.zeros(12 * self.NF)
+        lib().orc_get_faces(self.h, _p(F))
+        return F.reshape((4, 3, self.NF), order="F")
+
+    def metric(self):
+        DoF, nz, NF = self.DoF, self.nz, self.NF
+        X = np.zeros(DoF * 6 * nz * NF)
+        dXdxI = np.zeros(18 * DoF * nz * NF)
+        J = np.zeros(DoF * 2 * nz * NF)
+        lib().orc_get_metric(self.h, _p(X), _p(dXdxI), _p(J))
+        return (X.reshape((DoF, 2, 3, nz, NF), order="F"),
+                dXdxI.reshape((3, 3, 2, DoF, nz, NF), order="F"),
+                J.reshape((DoF, 2, nz, NF), order="F"))
+
+    def mass(self):
+        M = np.zeros(self.nz * self.NumG * 2)
+        MM = np.zeros(self.nz * self.NumG)
+        lib().orc_get_mass(self.h, _p(M), _p(MM))
+        return (M.reshape((self.nz, self.NumG, 2), order="F"),
+                MM.reshape((self.nz, self.NumG), order="F"))
+
+    def dz(self):
+        d = np.zeros(self.nz * self.NumG)
+        lib().orc_get_dz(self.h, _p(d))
+        return d.reshape((self.nz, self.NumG), order="F")
+
+    def set_metric(self, X=None, dXdxI=None, J=None, M=None, dz=None):
+        def q(a):
+            return None if a is None else _p(np.asfortranarray(a, dtype=np.float64))
+        keep = [np.asfortranarray(a, dtype=np.float64) if a is not None else None
+                for a in (X, dXdxI, J, M, dz)]
+        lib().orc_set_metric(self.h, *[(_p(a) if a is not None else None) for a in keep])
+
+    def _state(self):
+        return np.zeros((self.nz, self.NumG, self.NV), order="F")
+
+    def init_state(self, tracer_lonlat=None):
+        U = self._state()
+        tl = np.zeros(max(2 * self.NumTr, 2))
+        if tracer_lonlat is not None and self.NumTr:
+            tl[:2 * self.NumTr] = np.asarray(tracer_lonlat, dtype=np.float64).ravel()
+        lib().orc_init_state(self.h, _p(U), _p(tl))
+        return U
+
+    def pressure(self, U):
+        U = np.asfortranarray(U)
+        p = np.zeros((self.nz, self.NumG), order="F")
+        lib().orc_pressure(self.h, _p(U), _p(p))
+        return p
+
+    def hypervisc1(self, U):
+        U = np.asfortranarray(U)
+        T = np.zeros((self.nz, self.NumG, 5 + self.NumTr), order="F")
+        lib().orc_hypervisc1(self.h, _p(U), _p(T))
+        return T
+
+    def rhs(self, U):
+        U = np.asfortranarray(U)
+        F = self._state()
+        lib().orc_rhs(self.h, _p(U), _p(F))
+        return F
+
+    def jac(self, U):
+        U = np.asfortranarray(U)
+        b = np.zeros(4 * 2 * (self.nz - 1) * self.NumG)
+        lib().orc_jac(self.h, _p(U), _p(b))
+        # four bands (JRhoW, JWRho, JWRhoTh, JRhoThW), each (2, nz-1, NumG) column-major
+        return b.reshape((4, self.NumG, self.nz - 1, 2)).transpose(0, 3, 2, 1)
+
+    def schur(self, v, fac):
+        v = np.array(v, order="F", dtype=np.float64, copy=True)
+        k = self._state()
+        rc = lib().orc_schur(self.h, _p(k), _p(v), float(fac))
+        if rc:
+            raise RuntimeError("orc_schur: call jac first")
+        return k, v
+
+    def ros_step(self, U, dt, nsteps=1):
+        V = np.array(U, order="F", dtype=np.float64, copy=True)
+        lib().orc_ros_step(self.h, _p(V), float(dt), int(nsteps))
+        return V
+
+    def mass_integral(self, U):
+        U = np.asfortranarray(U)
+        return lib().orc_mass_integral(self.h, _p(U))

@@ -1,0 +1,161 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle on the
+same seeded inputs.
+
+Bars (from the hot-path contract):
+  * index/DSS maps bit-exact (checked on the CPU side in test_golden_grid);
+  * FP64 tendencies within 1e-12 relative max-norm per field;
+  * the state after 10 Rosenbrock-W steps within 1e-10.
+The kernels evaluate the reference's expressions in the same order without
+contraction and sum the DSS in the oracle's order, so most comparisons are
+in fact bit-exact; the tests assert the tolerance and record exactness.
+"""
+import numpy as np
+import pytest
+
+from _cases import make_case, rel_err_per_field
+
+pytestmark = pytest.mark.gpu
+
+TOL_RHS = 1e-12
+TOL_STEP = 1e-10
+
+
+@pytest.fixture(scope="module")
+def lib_ready(built_lib, cuda_ok):
+    return True
+
+
+def _dycore(grid, NumTr, nu, **kw):
+    from cgd_b200 import Dycore
+    return Dycore(grid, NumTr, nu, **kw)
+
+
+CASES = {
+    "small": dict(nPanel=6, p=4, nz=10, NumTr=0, stretch="uniform"),
+    "tracers_p3": dict(nPanel=5, p=3, nz=12, NumTr=2, stretch="quadratic"),
+    "nz64": dict(nPanel=4, p=4, nz=64, NumTr=1, stretch="quadratic"),
+    "p2": dict(nPanel=6, p=2, nz=7, NumTr=0, stretch="uniform"),
+}
+
+
+@pytest.fixture(scope="module", params=list(CASES))
+def case(request, oracle_mod, lib_ready):
+    c = CASES[request.param]
+    o, g, U, nu = make_case(oracle_mod, c["nPanel"], c["p"], c["nz"], c["NumTr"], c["stretch"])
+    d = _dycore(g, c["NumTr"], nu)
+    yield request.param, o, g, U, nu, d
+    d.close()
+
+
+def test_pressure_bit_exact(case):
+    name, o, g, U, nu, d = case
+    assert np.array_equal(d.fcn_prepare(U), o.pressure(U))
+
+
+def test_hypervisc_phase1(case):
+    name, o, g, U, nu, d = case
+    Tg = d.hypervisc_phase1(U)
+    To = o.hypervisc1(U)
+    err = rel_err_per_field(Tg, To)
+    assert err.max() <= TOL_RHS, (name, err)
+    assert np.array_equal(Tg, To), (name, err)
+
+
+def test_rhs(case):
+    name, o, g, U, nu, d = case
+    Fg = d.fcn(U)
+    Fo = o.rhs(U)
+    err = rel_err_per_field(Fg, Fo)
+    assert err.max() <= TOL_RHS, (name, err)
+    assert np.array_equal(Fg, Fo), (name, err)
+
+
+def test_jacobian_and_schur(case):
+    name, o, g, U, nu, d = case
+    bo = o.jac(U)
+    bg = d.jac(U)
+    assert np.array_equal(bg, bo)
+    rng = np.random.default_rng(11)
+    v = np.asfortranarray(rng.standard_normal(U.shape))
+    ko, vo = o.schur(v, 300.0)
+    vg = v.copy(order="F")
+    kg = d.schur_solve(vg, 300.0)
+    assert np.array_equal(kg, ko)
+    assert np.array_equal(vg, vo)
+
+
+def test_ten_steps(case):
+    name, o, g, U, nu, d = case
+    dt = 600.0 if name == "small" else 300.0
+    Vo = o.ros_step(U, dt, 10)
+    Vg = U.copy(order="F")
+    d.time_stepper(Vg, dt, 10)
+    err = rel_err_per_field(Vg - U, Vo - U)   # relative to the change over 10 steps
+    assert np.all(np.isfinite(Vg))
+    assert rel_err_per_field(Vg, Vo).max() <= TOL_STEP, (name, err)
+    assert np.array_equal(Vg, Vo), (name, err)
+
+
+def test_device_pointers_match_host(case):
+    """Zero-copy device arrays (torch CUDA tensors) give the same result as
+    host arrays staged through the library."""
+    import torch
+    name, o, g, U, nu, d = case
+    Fh = d.fcn(U)
+    Ut = torch.from_numpy(np.ascontiguousarray(U.transpose(2, 1, 0))).cuda()
+    Ft = torch.empty_like(Ut)
+    d.fcn(Ut, Ft)
+    assert np.array_equal(Ft.cpu().numpy().transpose(2, 1, 0), Fh)
+    Vh = U.copy(order="F")
+    d.time_stepper(Vh, 300.0, 2)
+    d.time_stepper(Ut, 300.0, 2)
+    torch.cuda.synchronize()
+    assert np.array_equal(Ut.cpu().numpy().transpose(2, 1, 0), Vh)
+
+
+def test_deterministic(case):
+    name, o, g, U, nu, d = case
+    a = U.copy(order="F")
+    b = U.copy(order="F")
+    d.time_stepper(a, 300.0, 3)
+    d.time_stepper(b, 300.0, 3)
+    assert np.array_equal(a, b)
+
+
+def test_mass_integral(case):
+    name, o, g, U, nu, d = case
+    m0 = d.mass_integral(U)
+    assert abs(m0 - o.mass_integral(U)) <= 1e-14 * abs(m0)
+    V = U.copy(order="F")
+    d.time_stepper(V, 300.0, 5)
+    assert abs(d.mass_integral(V) - m0) <= 1e-13 * abs(m0)
+
+
+def test_nonfinite_state_reported(oracle_mod, lib_ready):
+    """A NaN written into the state on the host is detected after the step and
+    reported as CGD_ERR_NONFINITE (no device trap)."""
+    from cgd_b200 import CgdError
+    o, g, U, nu = make_case(oracle_mod, 3, 4, 6, 0)
+    d = _dycore(g, 0, nu, check_finite=True)
+    V = U.copy(order="F")
+    d.time_stepper(V, 300.0, 1)
+    V[2, 5, 4] = np.nan
+    with pytest.raises(CgdError) as e:
+        d.time_stepper(V, 300.0, 1)
+    assert e.value.code == -4
+    d.close()
+
+
+def test_dropin_configuration(oracle_mod, lib_ready):
+    """nPanel 30, p 4, nz 45 quadratic, 2 tracers: the full-size drop-in case."""
+    o, g, U, nu = make_case(oracle_mod, 30, 4, 45, 2, "quadratic")
+    d = _dycore(g, 2, nu)
+    Fg, Fo = d.fcn(U), o.rhs(U)
+    err = rel_err_per_field(Fg, Fo)
+    assert err.max() <= TOL_RHS, err
+    Vo = o.ros_step(U, 300.0, 1)
+    Vg = U.copy(order="F")
+    d.time_stepper(Vg, 300.0, 1)
+    assert rel_err_per_field(Vg, Vo).max() <= TOL_STEP
+    assert np.array_equal(Vg, Vo)
+    d.close()
