@@ -84,7 +84,10 @@ class Dycore:
 
     def close(self):
         if getattr(self, "h", None):
-            _lib.lib().cgd_destroy(self.h)
+            try:
+                _lib.lib().cgd_destroy(self.h)
+            except (TypeError, AttributeError):   # interpreter shutdown
+                pass
             self.h = None
 
     def __del__(self):

@@ -158,10 +158,15 @@ class RunConfig:
 CONFIGS = {
     # small CPU-runnable case: 10 steps at dt 600 s
     "small": RunConfig("small", 6, 4, 10, 0, 600.0, 10, "uniform"),
-    # the GPU drop-in case: nPanel 30, p 4, nz 45 quadratic, 2 tracers, 1 day at 300 s
-    "dropin": RunConfig("dropin", 30, 4, 45, 2, 300.0, 288, "quadratic"),
-    # mixed-precision case: nPanel 60, nz 64, 1 day at 150 s
-    "mixed": RunConfig("mixed", 60, 4, 64, 0, 150.0, 576, "quadratic"),
-    # adjoint case: drop-in grid without tracers, 48 steps
-    "adjoint": RunConfig("adjoint", 30, 4, 45, 0, 300.0, 48, "quadratic"),
+    # the GPU drop-in grid: nPanel 30, p 4, nz 45 quadratic, 2 tracers, dt 120 s.
+    # The horizontal acoustics of this W-method are explicit: at dt 300 s the run
+    # blows up within 5 steps (max|w| 0.05 -> 8 m/s -> NaN), at 150 s within 40
+    # steps; 120, 100 and 75 s stay stable for 600 steps (max|w| decays to
+    # 3e-3 m/s).  1 day = 720 steps.
+    "dropin": RunConfig("dropin", 30, 4, 45, 2, 120.0, 720, "quadratic",
+                        extra={"dt_requested": 300.0}),
+    # mixed-precision case: nPanel 60 halves the spacing, so dt 60 s; 1 day = 1440 steps
+    "mixed": RunConfig("mixed", 60, 4, 64, 0, 60.0, 1440, "quadratic", extra={"dt_requested": 150.0}),
+    # adjoint case: drop-in grid without tracers, 4 h at dt 120 s = 120 steps
+    "adjoint": RunConfig("adjoint", 30, 4, 45, 0, 120.0, 120, "quadratic", extra={"dt_requested": 300.0}),
 }

@@ -7,6 +7,7 @@
 // once into a CUDA graph and replayed per step.
 #include "../../include/cgd_b200.h"
 #include "cgd_kernels.cuh"
+#include "cgd_phase2.cuh"
 #include "cgd_mixed.cuh"
 
 #include <cuda_runtime.h>
@@ -101,6 +102,12 @@ bool is_device_ptr(const void *p)
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+template <int N, int LC>
+size_t smem_max()
+{
+  return SweepCfg<N, LC>::smem(MAXTR);
+}
+
 template <int N>
 void launch_hv1(cgd_handle *h, const double *U, double *C)
 {
@@ -112,9 +119,15 @@ void launch_hv1(cgd_handle *h, const double *U, double *C)
 template <int N>
 void launch_p2(cgd_handle *h, const double *U, const double *T1, double *C)
 {
-  constexpr int LT = 256 / (N * N) - 1;
-  dim3 grid(h->NF, (h->nz + LT - 1) / LT);
-  k_phase2<N><<<grid, 256, 0, h->stream>>>(h->gp, U, T1, C);
+  constexpr int LC = 256 / (N * N);
+  using CF = SweepCfg<N, LC>;
+  size_t smem = CF::smem(h->NumTr);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_phase2_sweep<N, LC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max<N, LC>());
+    attr = true;
+  }
+  k_phase2_sweep<N, LC><<<h->NF, CF::THREADS, smem, h->stream>>>(h->gp, U, T1, C);
 }
 
 void hv1(cgd_handle *h, const double *U, double *C)
@@ -312,6 +325,21 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
         double z = 0.5 * (xx(0, 2) + xx(1, 2));
         double sinlat = z / std::sqrt(x * x + y * y + z * z);
         v[C_FCOR] = Omega2 * sinlat;
+        // RecU4 (src/GPU/OperatorKernel.jl:1044-1059): the J-only factors of the
+        // interface between Iz and Iz+1, with the column-end clamping of
+        // DivRhoTrUpwind3New2Kernel! (OperatorKernel.jl:667-683)
+        v[C_RK0] = v[C_RK1] = v[C_RK2] = v[C_RK3] = 0.0;
+        if (Iz < nz - 1) {
+          auto js = [&](int lev) {
+            return J[ID + (size_t)DoF * (0 + 2 * (lev + (size_t)nz * IF))] +
+                   J[ID + (size_t)DoF * (1 + 2 * (lev + (size_t)nz * IF))];
+          };
+          double JLL = js(Iz > 0 ? Iz - 1 : 0), JL = js(Iz), JR = js(Iz + 1), JRR = js(Iz + 2 < nz ? Iz + 2 : nz - 1);
+          v[C_RK0] = (JL / (JL + JR)) * ((JLL + JL) / (JLL + JL + JR));
+          v[C_RK1] = (JL / (JLL + JL)) * (JR / (JLL + JL + JR));
+          v[C_RK2] = (JR / (JR + JL)) * ((JRR + JR) / (JL + JR + JRR));
+          v[C_RK3] = (JR / (JRR + JR)) * (JL / (JL + JR + JRR));
+        }
         for (int c = 0; c < NCOMP; ++c) met[(((size_t)IF * NCOMP + c) * DoF + ID) * nz + Iz] = v[c];
       }
 

@@ -1253,8 +1253,8 @@ static void phase2_element(Model &m, const Ctx &c, const double *T1, int IF, std
   // ---- assemble the element-node contributions (fixed order) ----
   //  rho   : vflux(top of Iz) , vflux(top of Iz-1) , horizontal divergence
   //  u, v  : hyperviscosity , momentum , pressure/kinetic gradient
-  //  w(Iz) : momentum(Iz, upper node) , momentum(Iz+1, lower node) ,
-  //          gradient(Iz, upper node) , gradient(Iz+1, lower node)
+  //  w(Iz) : (momentum(Iz, upper node) + gradient(Iz, upper node)) +
+  //          (momentum(Iz+1, lower node) + gradient(Iz+1, lower node))
   //  rho*theta, rho*q : hyperviscosity , vflux(top of Iz) , vflux(top of Iz-1) ,
   //          horizontal divergence
   for (int Iz = 0; Iz < nz; ++Iz) {
@@ -1273,7 +1273,9 @@ static void phase2_element(Model &m, const Ctx &c, const double *T1, int IF, std
       acc = 0.0;
       if (Iz < nz - 1) {
         const P2Terms &tu = tm[(size_t)(Iz + 1) * DoF + ID];
-        acc += t.mwhi; acc += tu.mwlo; acc += t.gwhi; acc += tu.gwlo;
+        double hi = t.mwhi + t.gwhi;
+        double lo = tu.mwlo + tu.gwlo;
+        acc = hi + lo;
       }
       out[3 * DoF + ID] = acc;
       acc = 0.0; acc += t.vth;
