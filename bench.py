@@ -270,7 +270,7 @@ def run_ours(args, cfg, rank, world, local):
         peak, kind = measured_peak_hbm()
         fam = {}
         for name, ms in ktimes:
-            fam.setdefault(name.rstrip("0123456789"), []).append(ms)
+            fam.setdefault(name, []).append(ms)
         p2 = fam.get("phase2", [float("nan")])
         t_p2 = float(np.mean(p2)) / 1e3
         b_p2 = phase2_bytes(cfg)

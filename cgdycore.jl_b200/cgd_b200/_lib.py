@@ -9,7 +9,8 @@ import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.dirname(_HERE)
-LIB_PATH = os.path.join(PKG_DIR, "libcgd_b200.so")
+LIB_PATH = os.path.join(PKG_DIR, "libcgd_b200.so")               # fast build
+LIB_PATH_EXACT = os.path.join(PKG_DIR, "libcgd_b200_exact.so")   # bit-exact build
 
 CGD_OK = 0
 ERRORS = {
@@ -40,20 +41,21 @@ class CgdConfig(ctypes.Structure):
 class CgdError(RuntimeError):
     def __init__(self, code, what=""):
         self.code = code
-        msg = lib().cgd_strerror(code).decode() if _lib is not None else ERRORS.get(code, "error")
+        msg = lib().cgd_strerror(code).decode() if _libs else ERRORS.get(code, "error")
         super().__init__(f"{what}: {ERRORS.get(code, code)} ({msg})")
 
 
-_lib = None
+_libs = {}
 
 
-def lib():
-    """Load the library (raises OSError if it has not been built)."""
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            raise OSError(f"{LIB_PATH} not found: build it with __graft_entry__.build()")
-        L = ctypes.CDLL(LIB_PATH)
+def lib(exact=False):
+    """Load the fast (default) or the exact build (raises OSError if it has
+    not been built; there is no fallback)."""
+    path = LIB_PATH_EXACT if exact else LIB_PATH
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise OSError(f"{path} not found: build it with __graft_entry__.build()")
+        L = ctypes.CDLL(path)
         vp, i32, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_double
         L.cgd_create.argtypes = [ctypes.POINTER(CgdConfig)] + [vp] * 8 + [ctypes.POINTER(vp)]
         L.cgd_create.restype = ctypes.c_int
@@ -76,8 +78,8 @@ def lib():
         L.cgd_strerror.restype = ctypes.c_char_p
         L.cgd_version.argtypes = []
         L.cgd_version.restype = ctypes.c_char_p
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return _libs[path]
 
 
 def check(rc, what):

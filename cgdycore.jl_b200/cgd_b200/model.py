@@ -56,13 +56,14 @@ class Dycore:
     """One model instance on the current CUDA device."""
 
     def __init__(self, grid, NumTr=0, nu=(0.0, 0.0, 0.0), phys=None, precision="fp64",
-                 check_finite=False):
+                 check_finite=False, exact=False):
         self.grid = grid
         self.phys = phys or PhysParameters(RadEarth=grid.Rad)
         self.nz, self.NumG, self.NF = grid.nz, grid.NumG, grid.NF
         self.NumTr, self.NV = NumTr, 5 + NumTr
         self.shape = (self.nz, self.NumG, self.NV)
-        L = _lib.lib()
+        self.exact = exact
+        self._L = L = _lib.lib(exact)
         cfg = _lib.CgdConfig()
         cfg.OrdPoly, cfg.nz, cfg.NumTr = grid.OrdPoly, grid.nz, NumTr
         cfg.NF, cfg.NumG = grid.NF, grid.NumG
@@ -85,7 +86,7 @@ class Dycore:
     def close(self):
         if getattr(self, "h", None):
             try:
-                _lib.lib().cgd_destroy(self.h)
+                self._L.cgd_destroy(self.h)
             except (TypeError, AttributeError):   # interpreter shutdown
                 pass
             self.h = None
@@ -98,18 +99,18 @@ class Dycore:
 
     def fcn_prepare(self, U, p=None):
         p = np.zeros((self.nz, self.NumG), order="F") if p is None else p
-        _lib.check(_lib.lib().cgd_prepare(self.h, _ptr(U, self.shape), _ptr(p, (self.nz, self.NumG), True)),
+        _lib.check(self._L.cgd_prepare(self.h, _ptr(U, self.shape), _ptr(p, (self.nz, self.NumG), True)),
                    "cgd_prepare")
         return p
 
     def fcn(self, U, F=None):
         F = self.new_state() if F is None else F
-        _lib.check(_lib.lib().cgd_rhs(self.h, _ptr(U, self.shape), _ptr(F, self.shape, True)), "cgd_rhs")
+        _lib.check(self._L.cgd_rhs(self.h, _ptr(U, self.shape), _ptr(F, self.shape, True)), "cgd_rhs")
         return F
 
     def hypervisc_phase1(self, U, Temp1=None):
         T = self.new_state() if Temp1 is None else Temp1
-        _lib.check(_lib.lib().cgd_hypervisc_phase1(self.h, _ptr(U, self.shape), _ptr(T, self.shape, True)),
+        _lib.check(self._L.cgd_hypervisc_phase1(self.h, _ptr(U, self.shape), _ptr(T, self.shape, True)),
                    "cgd_hypervisc_phase1")
         return T
 
@@ -117,48 +118,48 @@ class Dycore:
         """Bands JRhoW, JWRho, JWRhoTh, JRhoThW as an array (4, 2, nz-1, NumG);
         each band is the reference's (2, nz-1, NumG) JCache array."""
         b = np.zeros(4 * 2 * (self.nz - 1) * self.NumG)
-        _lib.check(_lib.lib().cgd_jac(self.h, _ptr(U, self.shape), b.ctypes.data), "cgd_jac")
+        _lib.check(self._L.cgd_jac(self.h, _ptr(U, self.shape), b.ctypes.data), "cgd_jac")
         return b.reshape((4, self.NumG, self.nz - 1, 2)).transpose(0, 3, 2, 1)
 
     def schur_solve(self, v, fac, k=None):
         """k = (I/fac - J)^-1 v with the bands of the last jac(); v is updated
         in place as by the reference."""
         k = self.new_state() if k is None else k
-        _lib.check(_lib.lib().cgd_schur_solve(self.h, _ptr(k, self.shape, True), _ptr(v, self.shape, True),
+        _lib.check(self._L.cgd_schur_solve(self.h, _ptr(k, self.shape, True), _ptr(v, self.shape, True),
                                               float(fac)), "cgd_schur_solve")
         return k
 
     def rosenbrock_schur(self, U, dt):
-        _lib.check(_lib.lib().cgd_ros_step(self.h, _ptr(U, self.shape, True), float(dt), 1), "cgd_ros_step")
+        _lib.check(self._L.cgd_ros_step(self.h, _ptr(U, self.shape, True), float(dt), 1), "cgd_ros_step")
         return U
 
     def time_stepper(self, U, dt, nsteps):
-        _lib.check(_lib.lib().cgd_ros_step(self.h, _ptr(U, self.shape, True), float(dt), int(nsteps)),
+        _lib.check(self._L.cgd_ros_step(self.h, _ptr(U, self.shape, True), float(dt), int(nsteps)),
                    "cgd_ros_step")
         return U
 
     def mass_integral(self, U):
         out = ctypes.c_double()
-        _lib.check(_lib.lib().cgd_mass_integral(self.h, _ptr(U, self.shape), self._mmass.ctypes.data,
+        _lib.check(self._L.cgd_mass_integral(self.h, _ptr(U, self.shape), self._mmass.ctypes.data,
                                                 ctypes.byref(out)), "cgd_mass_integral")
         return out.value
 
     def stream(self):
         """The library's cudaStream_t as an integer handle."""
         s = ctypes.c_void_p()
-        _lib.check(_lib.lib().cgd_get_stream(self.h, ctypes.byref(s)), "cgd_get_stream")
+        _lib.check(self._L.cgd_get_stream(self.h, ctypes.byref(s)), "cgd_get_stream")
         return s.value or 0
 
     def kernel_times(self, nmax=12):
         names = ctypes.create_string_buffer(512)
         ms = (ctypes.c_double * nmax)()
-        n = _lib.lib().cgd_kernel_times(self.h, names, 512, ms, nmax)
+        n = self._L.cgd_kernel_times(self.h, names, 512, ms, nmax)
         if n < 0:
             raise _lib.CgdError(n, "cgd_kernel_times")
         return list(zip(names.value.decode().split(";"), list(ms)[:n]))
 
 
-def setup(cfg_name_or_cfg, precision="fp64", check_finite=False, nz=None, nPanel=None):
+def setup(cfg_name_or_cfg, precision="fp64", check_finite=False, nz=None, nPanel=None, exact=False):
     """Grid + initial state + Dycore for a named configuration
     (physics.CONFIGS).  Returns (dycore, U0, config)."""
     from . import grid as G
@@ -174,5 +175,5 @@ def setup(cfg_name_or_cfg, precision="fp64", check_finite=False, nz=None, nPanel
     U = Ph.initial_state(grid, phys, cfg.NumTr, tl, cfg.Up)
     Ph.theta_noise(U, cfg.theta_noise, cfg.seed_theta)
     nu = Ph.hyperdiffusion(cfg.nPanel, cfg.OrdPoly)
-    dyc = Dycore(grid, cfg.NumTr, nu, phys, precision=precision, check_finite=check_finite)
+    dyc = Dycore(grid, cfg.NumTr, nu, phys, precision=precision, check_finite=check_finite, exact=exact)
     return dyc, U, cfg

@@ -54,6 +54,7 @@ struct cgd_handle {
   double graph_dt = 0.0;
   // profiling events (recorded inside the graph when CGD_PROFILE is set)
   bool profile = false;
+  bool capturing = false;
   cudaEvent_t ev[NPROF + 1] = {};
   // mixed precision form
   MixedState *mixed = nullptr;
@@ -112,7 +113,7 @@ template <int N>
 void launch_hv1(cgd_handle *h, const double *U, double *C)
 {
   constexpr int LT = 256 / (N * N);
-  dim3 grid(h->NF, (h->nz + LT - 1) / LT);
+  dim3 grid((h->nz + LT - 1) / LT, h->NF);   // the level tiles of one element run back to back
   k_hypervisc1<N><<<grid, 256, 0, h->stream>>>(h->gp, U, C);
 }
 
@@ -159,13 +160,21 @@ void gather(cgd_handle *h, const double *C, double *out)
 template <int MODE>
 void column(cgd_handle *h, const ColArgs &a)
 {
-  size_t smem = (size_t)COL_WARPS * COL_NARR * 64 * sizeof(double);
+  size_t smem = (size_t)COL_WARPS * (h->NV + 12) * h->nz * sizeof(double);
+  static bool attr = false;
+  if (!attr) {   // up to 8 warps x (9 + 12) arrays x 64 levels
+    cudaFuncSetAttribute(k_column<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         COL_WARPS * (MAXNV + 12) * 64 * (int)sizeof(double));
+    attr = true;
+  }
   k_column<MODE><<<(h->NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, h->stream>>>(h->gp, a);
 }
 
+// Event between two kernels of a step launched without the graph (the
+// profiled step, see cgd_ros_step).
 void rec(cgd_handle *h, int i)
 {
-  if (h->profile) cudaEventRecord(h->ev[i], h->stream);
+  if (h->profile && !h->capturing) cudaEventRecord(h->ev[i], h->stream);
 }
 
 // One SSP-Knoth step on device state U (in place).
@@ -230,7 +239,11 @@ extern "C" {
 
 const char *cgd_version(void)
 {
-  return "cgd_b200 1.0 (sm_100a, FP64 owner-gather DSS, -fmad=false)";
+#ifdef CGD_FAST
+  return "cgd_b200 1.0 fast (sm_100a, FP64 owner-gather DSS, -fmad=false, reciprocal mass/Jacobian/density)";
+#else
+  return "cgd_b200 1.0 exact (sm_100a, FP64 owner-gather DSS, -fmad=false, bit-identical to the CPU restatement)";
+#endif
 }
 
 const char *cgd_strerror(int code)
@@ -548,14 +561,21 @@ int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps)
   if (!h->gexec || h->graph_U != Ud || h->graph_dt != dt) {
     free_graph(h);
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    h->capturing = true;
     enqueue_step(h, Ud, dt);
+    h->capturing = false;
     cudaError_t e = cudaStreamEndCapture(h->stream, &h->graph);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
     CK(cudaGraphInstantiate(&h->gexec, h->graph, 0));
     h->graph_U = Ud;
     h->graph_dt = dt;
   }
-  for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(h->gexec, h->stream));
+  // With CGD_PROFILE=1 the last step of the call is launched kernel by kernel
+  // with events in between (same kernels, same stream), so the per-kernel
+  // durations of that step can be read with cgd_kernel_times.
+  const int ngraph = h->profile && nsteps > 0 ? nsteps - 1 : nsteps;
+  for (int s = 0; s < ngraph; ++s) CK(cudaGraphLaunch(h->gexec, h->stream));
+  if (ngraph < nsteps) enqueue_step(h, Ud, dt);
   if (h->cfg.flags & CGD_FLAG_CHECK_FINITE) {
     CK(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
     long long n = (long long)h->nz * h->NumG * h->NV;
@@ -603,8 +623,8 @@ int cgd_kernel_times(cgd_handle *h, char *names, int32_t names_len, double *ms, 
 {
   if (!h || !ms) return CGD_ERR_INVALID_ARG;
   if (!h->profile) return CGD_ERR_UNSUPPORTED;
-  static const char *nm[NPROF] = {"hypervisc1", "gather", "phase2", "column1", "hypervisc1", "gather",
-                                  "phase2", "column2", "hypervisc1", "gather", "phase2", "column3"};
+  static const char *nm[NPROF] = {"hypervisc1", "gather", "phase2", "column", "hypervisc1", "gather",
+                                  "phase2", "column", "hypervisc1", "gather", "phase2", "column"};
   std::string all;
   int n = nmax < NPROF ? nmax : NPROF;
   for (int i = 0; i < n; ++i) {

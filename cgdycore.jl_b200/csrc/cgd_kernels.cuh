@@ -16,12 +16,27 @@
 // and equal to the CPU restatement's.
 //
 // Every floating-point expression below is written in the reference's
-// evaluation order; the file is compiled with -fmad=false so that no
-// multiply-add is contracted (the bit-exactness contract with the oracle).
+// evaluation order (see CGD_FAST below for the two builds).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "../../include/cgd_math.h"
+
+// Two builds come from this source, both compiled without multiply-add
+// contraction (-fmad=false).  The exact build evaluates the reference's
+// expressions literally - every division is a division - so results are
+// bit-identical to the CPU restatement.  The fast build (CGD_FAST) replaces
+// the final division of a chain by the time-invariant sums J0+J1 (element
+// Jacobian) and M0+M1 (lumped mass), or by rho, with a multiply by a
+// reciprocal computed once per node and level (one rounding more, at the
+// end of the chain).
+#ifdef CGD_FAST
+#define CGD_DIVJ(x) ((x) * rJs)
+#define CGD_DIVM(x) ((x) * rMC)
+#else
+#define CGD_DIVJ(x) ((x) / Js)
+#define CGD_DIVM(x) ((x) / MC)
+#endif
 
 namespace cgd {
 
@@ -86,11 +101,11 @@ __global__ void __launch_bounds__(256) k_hypervisc1(const GP P, const double *__
   constexpr int DoF = N * N;
   constexpr int LT = 256 / DoF;
   __shared__ double s[9][LT * DoF];
-  const int IF = blockIdx.x;
+  const int IF = blockIdx.y;
   const int t = threadIdx.x;
   const int lvl = t % LT, ID = t / LT;
   const int I = ID % N, Jn = ID / N;
-  const int l = blockIdx.y * LT + lvl;
+  const int l = blockIdx.x * LT + lvl;
   const int nz = P.nz, NumG = P.NumG;
   const bool act = (ID < DoF) && (l < nz);
   const int si = lvl * DoF + ID, row = lvl * DoF;
@@ -115,6 +130,8 @@ __global__ void __launch_bounds__(256) k_hypervisc1(const GP P, const double *__
     s[4][si] = Ug[4 * fs] / Ug[0];
     MC = P.M[l + (size_t)nz * g] + P.M[l + (size_t)nz * (g + (size_t)NumG)];
   }
+  const double rJs = 1.0 / Js, rMC = 1.0 / MC;
+  (void)rJs; (void)rMC;
   __syncthreads();
   if (act) {
     const double *uC = s[0] + row, *vC = s[1] + row, *uD = s[2] + row, *vD = s[3] + row, *Th = s[4] + row;
@@ -129,10 +146,10 @@ __global__ void __launch_bounds__(256) k_hypervisc1(const GP P, const double *__
       cu += P.D[I + N * k] * uC[k + N * Jn] + P.D[Jn + N * k] * vC[I + N * k];
       dv += P.D[I + N * k] * uD[k + N * Jn] + P.D[Jn + N * k] * vD[I + N * k];
     }
-    s[5][si] = cu / Js;
-    s[6][si] = dv / Js;
-    double GradDx = (d11 * Dxc + d21 * Dyc) / Js;   // Grad12 with J
-    double GradDy = (d12 * Dxc + d22 * Dyc) / Js;
+    s[5][si] = CGD_DIVJ(cu);
+    s[6][si] = CGD_DIVJ(dv);
+    double GradDx = CGD_DIVJ(d11 * Dxc + d21 * Dyc);   // Grad12 with J
+    double GradDy = CGD_DIVJ(d12 * Dxc + d22 * Dyc);
     s[7][si] = d11 * GradDx + d12 * GradDy;         // Contra12
     s[8][si] = d21 * GradDx + d22 * GradDy;
   }
@@ -155,11 +172,11 @@ __global__ void __launch_bounds__(256) k_hypervisc1(const GP P, const double *__
     double FvC = -d11 * DxCurl - d21 * DyCurl;
     double FuD = d11 * DxDiv + d21 * DyDiv;         // Grad12
     double FvD = d12 * DxDiv + d22 * DyDiv;
-    out[0 * cs] = -FuC / MC;
-    out[1 * cs] = -FvC / MC;
-    out[2 * cs] = FuD / MC;
-    out[3 * cs] = FvD / MC;
-    out[4 * cs] = DivTh / MC;
+    out[0 * cs] = CGD_DIVM(-FuC);
+    out[1 * cs] = CGD_DIVM(-FvC);
+    out[2 * cs] = CGD_DIVM(FuD);
+    out[3 * cs] = CGD_DIVM(FvD);
+    out[4 * cs] = CGD_DIVM(DivTh);
   }
   for (int iT = 0; iT < P.NumTr; ++iT) {
     if (act) {
@@ -177,8 +194,8 @@ __global__ void __launch_bounds__(256) k_hypervisc1(const GP P, const double *__
         Dxc += P.D[I + N * k] * Tr[k + N * Jn];
         Dyc += P.D[Jn + N * k] * Tr[I + N * k];
       }
-      double GradDx = (d11 * Dxc + d21 * Dyc) / Js;
-      double GradDy = (d12 * Dxc + d22 * Dyc) / Js;
+      double GradDx = CGD_DIVJ(d11 * Dxc + d21 * Dyc);
+      double GradDy = CGD_DIVJ(d12 * Dxc + d22 * Dyc);
       s[7][si] = d11 * GradDx + d12 * GradDy;
       s[8][si] = d21 * GradDx + d22 * GradDy;
     }
@@ -188,7 +205,7 @@ __global__ void __launch_bounds__(256) k_hypervisc1(const GP P, const double *__
       double DivTr = P.DW[I] * Cx[N * Jn] + P.DW[Jn] * Cy[I];
 #pragma unroll
       for (int k = 1; k < N; ++k) DivTr += P.DW[I + N * k] * Cx[k + N * Jn] + P.DW[Jn + N * k] * Cy[I + N * k];
-      out[(5 + iT) * cs] = DivTr / MC;
+      out[(5 + iT) * cs] = CGD_DIVM(DivTr);
     }
     __syncthreads();
   }
@@ -270,8 +287,8 @@ struct ColArgs {
   RK rk;
 };
 
-constexpr int COL_WARPS = 4;
-constexpr int COL_NARR = MAXNV + 8 + 3 + 1;   // fv[NV], 8 bands, tri[3], x
+constexpr int COL_WARPS = 8;
+// per warp: fv[NV], 8 bands, tri[3], x; each nz long
 
 __device__ __forceinline__ void jac_at(const GP &P, double RhoL, double RhoR, double RhoThL0, double RhoThR0,
                                        double dzL, double dzR, double *jb)
@@ -301,11 +318,12 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
   const int g = blockIdx.x * COL_WARPS + warp;
   if (g >= P.NumG) return;
   const int nz = P.nz, n = nz - 1, NV = P.NV, NumG = P.NumG;
-  double *sw = csm + (size_t)warp * COL_NARR * 64;
-  double *fv = sw;                      // [NV][64]
-  double *jb = sw + MAXNV * 64;         // [8][64]
-  double *tri = jb + 8 * 64;            // [3][64]
-  double *xs = tri + 3 * 64;            // [64]
+  const int LS = nz;                    // per-warp arrays of nz entries
+  double *sw = csm + (size_t)warp * (NV + 12) * LS;
+  double *fv = sw;                      // [NV][nz]
+  double *jb = sw + NV * LS;            // [8][nz]
+  double *tri = jb + 8 * LS;            // [3][nz]
+  double *xs = tri + 3 * LS;            // [nz]
   const size_t fs = (size_t)nz * NumG;
   const double fac = A.fac;
 
@@ -319,27 +337,27 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
         double x = gacc[f];
         if (MODE >= 1) x = x + A.rk.c[MODE][0] / A.dt * A.k1[l + (size_t)nz * g + f * fs];
         if (MODE >= 2) x = x + A.rk.c[MODE][1] / A.dt * A.k2[l + (size_t)nz * g + f * fs];
-        fv[f * 64 + l] = x;
+        fv[f * LS + l] = x;
       }
       if (l < n) {
         double b[8];
         const double *V0 = A.Vn + (size_t)nz * g;
         jac_at(P, V0[l], V0[l + 1], V0[l + 4 * fs], V0[l + 1 + 4 * fs],
                P.dz[l + (size_t)nz * g], P.dz[l + 1 + (size_t)nz * g], b);
-        for (int r = 0; r < 8; ++r) jb[r * 64 + l] = b[r];
+        for (int r = 0; r < 8; ++r) jb[r * LS + l] = b[r];
       }
     } else {
-      for (int f = 0; f < NV; ++f) fv[f * 64 + l] = A.v[l + (size_t)nz * g + f * fs];
+      for (int f = 0; f < NV; ++f) fv[f * LS + l] = A.v[l + (size_t)nz * g + f * fs];
       if (l < n) {
         const size_t bs = (size_t)2 * n * NumG;
         for (int arr = 0; arr < 4; ++arr)
-          for (int r = 0; r < 2; ++r) jb[(2 * arr + r) * 64 + l] = A.bands[arr * bs + r + 2 * (l + (size_t)n * g)];
+          for (int r = 0; r < 2; ++r) jb[(2 * arr + r) * LS + l] = A.bands[arr * bs + r + 2 * (l + (size_t)n * g)];
       }
     }
   }
   __syncwarp();
   // jb rows: 0,1 JRhoW ; 2,3 JWRho ; 4,5 JWRhoTh ; 6,7 JRhoThW  (row r = Julia index r%2+1)
-#define JB(arr, r, i) jb[((arr) * 2 + (r)) * 64 + (i)]
+#define JB(arr, r, i) jb[((arr) * 2 + (r)) * LS + (i)]
   const double invfac = 1.0 / fac;
   const double invfac2 = invfac / fac;
   double v3new[2];
@@ -352,21 +370,21 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
       else t0 = -JB(1, 0, l - 1) * JB(0, 0, l) - JB(2, 0, l - 1) * JB(3, 0, l);
       if (l == n - 1) t2 = 0.0;
       else t2 = -JB(1, 1, l + 1) * JB(0, 1, l) - JB(2, 1, l + 1) * JB(3, 1, l);
-      tri[l] = t0; tri[64 + l] = t1; tri[128 + l] = t2;
+      tri[l] = t0; tri[LS + l] = t1; tri[2 * LS + l] = t2;
       // SchurSolveFKernel!
-      v3new[it] = fv[3 * 64 + l] / fac + JB(1, 1, l) * fv[l] + JB(1, 0, l) * fv[l + 1] +
-                  JB(2, 1, l) * fv[4 * 64 + l] + JB(2, 0, l) * fv[4 * 64 + l + 1];
+      v3new[it] = fv[3 * LS + l] / fac + JB(1, 1, l) * fv[l] + JB(1, 0, l) * fv[l + 1] +
+                  JB(2, 1, l) * fv[4 * LS + l] + JB(2, 0, l) * fv[4 * LS + l + 1];
     }
   }
   __syncwarp();
-  for (int it = 0, l = lane; l < n; l += 32, ++it) fv[3 * 64 + l] = v3new[it];
+  for (int it = 0, l = lane; l < n; l += 32, ++it) fv[3 * LS + l] = v3new[it];
   __syncwarp();
   if (lane == 0) {   // triSolve! (Thomas), b = fv[3], x = xs
-    double *b = fv + 3 * 64;
-    xs[0] = tri[64 + 0];
+    double *b = fv + 3 * LS;
+    xs[0] = tri[LS + 0];
     for (int i = 0; i < n - 1; ++i) {
-      xs[i + 1] = tri[64 + i + 1] - tri[128 + i] / xs[i] * tri[i + 1];
-      b[i + 1] = b[i + 1] - tri[128 + i] / xs[i] * b[i];
+      xs[i + 1] = tri[LS + i + 1] - tri[2 * LS + i] / xs[i] * tri[i + 1];
+      b[i + 1] = b[i + 1] - tri[2 * LS + i] / xs[i] * b[i];
     }
     xs[n - 1] = b[n - 1] / xs[n - 1];
     for (int i = n - 2; i >= 0; --i) xs[i] = (b[i] - tri[i + 1] * xs[i + 1]) / xs[i];
@@ -376,7 +394,7 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
   double res[2][MAXNV];
   for (int it = 0, l = lane; l < nz; l += 32, ++it) {
     double kw = l < n ? xs[l] : 0.0;
-    double v0 = fv[l], v4 = fv[4 * 64 + l];
+    double v0 = fv[l], v4 = fv[4 * LS + l];
     if (l == 0) {
       v0 += JB(0, 0, l) * xs[l];
       v4 += JB(3, 0, l) * xs[l];
@@ -392,7 +410,7 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
       if (f == 3) k = kw;
       else if (f == 0) k = fac * v0;
       else if (f == 4) k = fac * v4;
-      else k = fac * fv[f * 64 + l];
+      else k = fac * fv[f * LS + l];
       res[it][f] = k;
     }
     if (MODE == 3) {

@@ -136,6 +136,8 @@ __global__ void __launch_bounds__(SweepCfg<N, LC>::THREADS)
       TP(19, ID) = -rho * (d11 * u + d12 * v);                // Contra12(-Rho, u, v)
       TP(20, ID) = -rho * (d21 * u + d22 * v);
     }
+    const double rJs = 1.0 / Js, rMC = 1.0 / MC;
+    (void)rJs; (void)rMC;
     __syncthreads();
     double b1 = 0, b2 = 0, b3 = 0, b4 = 0;
     if (pact) {
@@ -153,10 +155,10 @@ __global__ void __launch_bounds__(SweepCfg<N, LC>::THREADS)
           cu += D[I + N * k] * a1[k + N * Jn] + D[Jn + N * k] * a2[I + N * k];
           dv += D[I + N * k] * a3[k + N * Jn] + D[Jn + N * k] * a4[I + N * k];
         }
-        b1 = cu / Js;
-        b2 = dv / Js;
-        double GradDx = (d11 * Dxc + d21 * Dyc) / Js;
-        double GradDy = (d12 * Dxc + d22 * Dyc) / Js;
+        b1 = CGD_DIVJ(cu);
+        b2 = CGD_DIVJ(dv);
+        double GradDx = CGD_DIVJ(d11 * Dxc + d21 * Dyc);
+        double GradDy = CGD_DIVJ(d12 * Dxc + d22 * Dyc);
         b3 = rho * (d11 * GradDx + d12 * GradDy);
         b4 = rho * (d21 * GradDx + d22 * GradDy);
       }
@@ -228,15 +230,15 @@ __global__ void __launch_bounds__(SweepCfg<N, LC>::THREADS)
           DivRhoTr += D[I + N * k] * uc[k + N * Jn] * cc[k + N * Jn] + D[Jn + N * k] * vc[I + N * k] * cc[I + N * k];
           DivRho += D[I + N * k] * uc[k + N * Jn] + D[Jn + N * k] * vc[I + N * k];
         }
-        RG(R_HTH, l, ID) = DivRhoTr / MC;
-        RG(R_HR, l, ID) = DivRho / MC;
+        RG(R_HTH, l, ID) = CGD_DIVM(DivRhoTr);
+        RG(R_HR, l, ID) = CGD_DIVM(DivRho);
         for (int q = 0; q < NT; ++q) {
           const double *ct = &RG(R_TR0 + 4 * q, l, 0);
           double Dv = D[I] * uc[N * Jn] * ct[N * Jn] + D[Jn] * vc[I] * ct[I];
 #pragma unroll
           for (int k = 1; k < N; ++k)
             Dv += D[I + N * k] * uc[k + N * Jn] * ct[k + N * Jn] + D[Jn + N * k] * vc[I + N * k] * ct[I + N * k];
-          RG(R_TR0 + 4 * q + 2, l, ID) = Dv / MC;
+          RG(R_TR0 + 4 * q + 2, l, ID) = CGD_DIVM(Dv);
         }
       }
     }
@@ -262,9 +264,9 @@ __global__ void __launch_bounds__(SweepCfg<N, LC>::THREADS)
       double FvC = -d11 * DxCurl - d21 * DyCurl;
       double FuD = d11 * DxDiv + d21 * DyDiv;
       double FvD = d12 * DxDiv + d22 * DyDiv;
-      RG(R_VU, l, ID) = -(-P.nuCurl * FuC + P.nuGrad * FuD) / MC;
-      RG(R_VV, l, ID) = -(-P.nuCurl * FvC + P.nuGrad * FvD) / MC;
-      RG(R_VTH, l, ID) = -P.nuDiv * DivTh / MC;
+      RG(R_VU, l, ID) = CGD_DIVM(-(-P.nuCurl * FuC + P.nuGrad * FuD));
+      RG(R_VV, l, ID) = CGD_DIVM(-(-P.nuCurl * FvC + P.nuGrad * FvD));
+      RG(R_VTH, l, ID) = CGD_DIVM(-P.nuDiv * DivTh);
     }
     for (int q = 0; q < NT; ++q) {   // tracer hyperviscosity
       __syncthreads();
@@ -280,8 +282,8 @@ __global__ void __launch_bounds__(SweepCfg<N, LC>::THREADS)
           Dxc += D[I + N * k] * a5[k + N * Jn];
           Dyc += D[Jn + N * k] * a5[I + N * k];
         }
-        double GradDx = (d11 * Dxc + d21 * Dyc) / Js;
-        double GradDy = (d12 * Dxc + d22 * Dyc) / Js;
+        double GradDx = CGD_DIVJ(d11 * Dxc + d21 * Dyc);
+        double GradDy = CGD_DIVJ(d12 * Dxc + d22 * Dyc);
         e3v = rho * (d11 * GradDx + d12 * GradDy);
         e4v = rho * (d21 * GradDx + d22 * GradDy);
         TP(5, ID) = e3v;
@@ -294,7 +296,7 @@ __global__ void __launch_bounds__(SweepCfg<N, LC>::THREADS)
         double DivTr = DW[I] * e3[N * Jn] + DW[Jn] * e4[I];
 #pragma unroll
         for (int k = 1; k < N; ++k) DivTr += DW[I + N * k] * e3[k + N * Jn] + DW[Jn + N * k] * e4[I + N * k];
-        RG(R_TR0 + 4 * q + 1, l, ID) = -P.nuDiv * DivTr / MC;
+        RG(R_TR0 + 4 * q + 1, l, ID) = CGD_DIVM(-P.nuDiv * DivTr);
       }
     }
     __syncthreads();
@@ -334,7 +336,14 @@ __global__ void __launch_bounds__(SweepCfg<N, LC>::THREADS)
       const int lv = L0 - 3 + lvl;
       if (active && lv >= 0 && lv < nz) {
         const double rho_ = RG(R_RHO, lv, ID), u_ = RG(R_U, lv, ID), v_ = RG(R_V, lv, ID);
-        const double wl_ = RG(R_WLO, lv, ID), wh_ = RG(R_W, lv, ID), MC_ = RG(R_MC, lv, ID);
+        const double wl_ = RG(R_WLO, lv, ID), wh_ = RG(R_W, lv, ID);
+        const double MC = RG(R_MC, lv, ID);
+#ifdef CGD_FAST
+        const double rMC = 1.0 / MC, rrho = 1.0 / rho_;
+#define CGD_DIVR(x) ((x) * rrho)
+#else
+#define CGD_DIVR(x) ((x) / rho_)
+#endif
         const double e310 = RG(R_D310, lv, ID), e311 = RG(R_D311, lv, ID), e320 = RG(R_D320, lv, ID);
         const double e321 = RG(R_D321, lv, ID), e330 = RG(R_D330, lv, ID), e331 = RG(R_D331, lv, ID);
         const bool top = lv < nz - 1, bot = lv > 0;
@@ -381,8 +390,8 @@ __global__ void __launch_bounds__(SweepCfg<N, LC>::THREADS)
         FW2 += FwCor * J1_;
         const double U1 = RG(R_U1, lv, ID), U2 = RG(R_U2, lv, ID), V1 = RG(R_V1, lv, ID);
         const double V2 = RG(R_V2, lv, ID), W1 = RG(R_W1, lv, ID), W2 = RG(R_W2, lv, ID);
-        const double mu = (-v_ * W1 - wl_ * V1 - v_ * W2 - wh_ * V2 + FU) / MC_;
-        const double mv = (u_ * W1 - wl_ * U1 + u_ * W2 - wh_ * U2 + FV) / MC_;
+        const double mu = CGD_DIVM(-v_ * W1 - wl_ * V1 - v_ * W2 - wh_ * V2 + FU);
+        const double mv = CGD_DIVM(u_ * W1 - wl_ * U1 + u_ * W2 - wh_ * U2 + FV);
         (void)FW1;
         // --- kinetic energy / pressure gradient
         const double K1s = 0.5 * (u_ * u_ + v_ * v_) + 0.5 * (wl_ * wl_);
@@ -412,8 +421,8 @@ __global__ void __launch_bounds__(SweepCfg<N, LC>::THREADS)
         GvF2 += -GZ * e321;
         GvF1 += -GZ * e320;
         GwF2 += -rho_ * GZ * e331;
-        const double gu = (GuF1 + GuF2 - RG(R_GRADU, lv, ID) / rho_) / MC_;
-        const double gv = (GvF1 + GvF2 - RG(R_GRADV, lv, ID) / rho_) / MC_;
+        const double gu = CGD_DIVM(GuF1 + GuF2 - CGD_DIVR(RG(R_GRADU, lv, ID)));
+        const double gv = CGD_DIVM(GvF1 + GvF2 - CGD_DIVR(RG(R_GRADV, lv, ID)));
         // --- w at the top interface: upper node of lv + lower node of lv+1
         double wcontrib = 0.0;
         if (top) {
@@ -445,13 +454,13 @@ __global__ void __launch_bounds__(SweepCfg<N, LC>::THREADS)
         double fr_top = 0, fr_bot = 0, fth_top = 0, fth_bot = 0;
         if (top) {
           const double Flr = 0.5 * RG(R_WCON, lv, ID);
-          fr_top = -Flr / MC_;
-          fth_top = -RG(R_FTH, lv, ID) / MC_;
+          fr_top = CGD_DIVM(-Flr);
+          fth_top = CGD_DIVM(-RG(R_FTH, lv, ID));
         }
         if (bot) {
           const double Flr = 0.5 * RG(R_WCON, lv - 1, ID);
-          fr_bot = Flr / MC_;
-          fth_bot = RG(R_FTH, lv - 1, ID) / MC_;
+          fr_bot = CGD_DIVM(Flr);
+          fth_bot = CGD_DIVM(RG(R_FTH, lv - 1, ID));
         }
         // --- assemble (same order as the CPU restatement)
         double *out = C + ((size_t)IF * P.NV * DoF + ID) * nz + lv;
@@ -472,11 +481,12 @@ __global__ void __launch_bounds__(SweepCfg<N, LC>::THREADS)
         out[4 * cs] = acc;
         for (int q = 0; q < NT; ++q) {
           acc = 0.0; acc += RG(R_TR0 + 4 * q + 1, lv, ID);
-          if (top) acc += -RG(R_TR0 + 4 * q + 3, lv, ID) / MC_;
-          if (bot) acc += RG(R_TR0 + 4 * q + 3, lv - 1, ID) / MC_;
+          if (top) acc += CGD_DIVM(-RG(R_TR0 + 4 * q + 3, lv, ID));
+          if (bot) acc += CGD_DIVM(RG(R_TR0 + 4 * q + 3, lv - 1, ID));
           acc += RG(R_TR0 + 4 * q + 2, lv, ID);
           out[(5 + q) * cs] = acc;
         }
+#undef CGD_DIVR
       }
     }
     __syncthreads();

@@ -22,15 +22,17 @@ def _declared(header):
     return sorted(set(re.findall(r"\b(cgd_[a-z0-9_]+)\s*\(", txt)))
 
 
-def test_library_exports_every_declared_symbol(built_lib):
+@pytest.mark.parametrize("exact", [False, True])
+def test_library_exports_every_declared_symbol(built_lib, exact):
     from cgd_b200 import _lib
-    L = ctypes.CDLL(built_lib)
+    path = _lib.LIB_PATH_EXACT if exact else _lib.LIB_PATH
+    L = ctypes.CDLL(path)
     names = _declared("cgd_b200.h")
     assert names, "no declarations parsed"
     for n in names:
         assert hasattr(L, n), f"{n} declared in include/cgd_b200.h but not exported"
     assert set(names) == set(_lib.EXPORTS)
-    out = subprocess.run(["nm", "-D", "--defined-only", built_lib], capture_output=True, text=True).stdout
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True).stdout
     for n in names:
         assert re.search(rf"\bT {n}\b", out), n
 
@@ -39,9 +41,11 @@ def test_library_is_sm100a(built_lib):
     """The build command targets compute_100a/sm_100a (no PTX for other archs)."""
     from cgd_b200 import build
     flags = " ".join(build.NVCC_FLAGS)
-    assert "arch=compute_100a,code=sm_100a" in flags and "-fmad=false" in flags
+    assert "arch=compute_100a,code=sm_100a" in flags
+    assert build.VARIANTS[build.LIB_PATH_EXACT] == ["-fmad=false"]
     from cgd_b200 import _lib
-    assert b"sm_100a" in _lib.lib().cgd_version()
+    assert b"sm_100a" in _lib.lib().cgd_version() and b"fast" in _lib.lib().cgd_version()
+    assert b"exact" in _lib.lib(exact=True).cgd_version()
 
 
 def test_argument_errors_without_device(built_lib):

@@ -5,9 +5,11 @@ Bars (from the hot-path contract):
   * index/DSS maps bit-exact (checked on the CPU side in test_golden_grid);
   * FP64 tendencies within 1e-12 relative max-norm per field;
   * the state after 10 Rosenbrock-W steps within 1e-10.
-The kernels evaluate the reference's expressions in the same order without
-contraction and sum the DSS in the oracle's order, so most comparisons are
-in fact bit-exact; the tests assert the tolerance and record exactness.
+Two builds are checked.  The exact build evaluates the reference's
+expressions in the same order without contraction and sums the DSS in the
+oracle's order, so its results are asserted bit-identical.  The fast build
+(FMA contraction, reciprocal multiplies by time-invariant sums) is held to
+the tolerances.
 """
 import numpy as np
 import pytest
@@ -30,6 +32,15 @@ def _dycore(grid, NumTr, nu, **kw):
     return Dycore(grid, NumTr, nu, **kw)
 
 
+def _same(a, b, exact, tol):
+    """Bit-identical for the exact build, within tol (relative max-norm per
+    field) for the fast build."""
+    err = rel_err_per_field(a, b)
+    assert err.max() <= tol, err
+    if exact:
+        assert np.array_equal(a, b), err
+
+
 CASES = {
     "small": dict(nPanel=6, p=4, nz=10, NumTr=0, stretch="uniform"),
     "tracers_p3": dict(nPanel=5, p=3, nz=12, NumTr=2, stretch="quadratic"),
@@ -38,50 +49,53 @@ CASES = {
 }
 
 
-@pytest.fixture(scope="module", params=list(CASES))
+@pytest.fixture(scope="module", params=[(c, v) for c in CASES for v in ("exact", "fast")],
+                ids=lambda p: f"{p[0]}-{p[1]}")
 def case(request, oracle_mod, lib_ready):
-    c = CASES[request.param]
+    name, variant = request.param
+    c = CASES[name]
     o, g, U, nu = make_case(oracle_mod, c["nPanel"], c["p"], c["nz"], c["NumTr"], c["stretch"])
-    d = _dycore(g, c["NumTr"], nu)
-    yield request.param, o, g, U, nu, d
+    d = _dycore(g, c["NumTr"], nu, exact=(variant == "exact"))
+    yield name, o, g, U, nu, d
     d.close()
 
 
-def test_pressure_bit_exact(case):
+def test_pressure(case):
     name, o, g, U, nu, d = case
-    assert np.array_equal(d.fcn_prepare(U), o.pressure(U))
+    pg, po = d.fcn_prepare(U), o.pressure(U)
+    assert np.abs(pg - po).max() <= 1e-15 * np.abs(po).max()
+    if d.exact:
+        assert np.array_equal(pg, po)
 
 
 def test_hypervisc_phase1(case):
+    """The phase-1 cache holds second derivatives of theta = rho*theta/rho
+    (~300 K with 1e-2 K structure), so any change of rounding moves it by
+    ~1e-12 of its own scale; the fast build is held to 1e-11 here and to the
+    1e-12 bar on the tendency it feeds (test_rhs)."""
     name, o, g, U, nu, d = case
-    Tg = d.hypervisc_phase1(U)
-    To = o.hypervisc1(U)
-    err = rel_err_per_field(Tg, To)
-    assert err.max() <= TOL_RHS, (name, err)
-    assert np.array_equal(Tg, To), (name, err)
+    _same(d.hypervisc_phase1(U), o.hypervisc1(U), d.exact, TOL_RHS if d.exact else 1e-11)
 
 
 def test_rhs(case):
     name, o, g, U, nu, d = case
-    Fg = d.fcn(U)
-    Fo = o.rhs(U)
-    err = rel_err_per_field(Fg, Fo)
-    assert err.max() <= TOL_RHS, (name, err)
-    assert np.array_equal(Fg, Fo), (name, err)
+    _same(d.fcn(U), o.rhs(U), d.exact, TOL_RHS)
 
 
 def test_jacobian_and_schur(case):
     name, o, g, U, nu, d = case
     bo = o.jac(U)
     bg = d.jac(U)
-    assert np.array_equal(bg, bo)
+    assert np.abs(bg - bo).max() <= 1e-14 * np.abs(bo).max()
     rng = np.random.default_rng(11)
     v = np.asfortranarray(rng.standard_normal(U.shape))
     ko, vo = o.schur(v, 300.0)
     vg = v.copy(order="F")
     kg = d.schur_solve(vg, 300.0)
-    assert np.array_equal(kg, ko)
-    assert np.array_equal(vg, vo)
+    _same(kg, ko, d.exact, TOL_RHS)
+    _same(vg, vo, d.exact, TOL_RHS)
+    if d.exact:
+        assert np.array_equal(bg, bo)
 
 
 def test_ten_steps(case):
@@ -90,10 +104,8 @@ def test_ten_steps(case):
     Vo = o.ros_step(U, dt, 10)
     Vg = U.copy(order="F")
     d.time_stepper(Vg, dt, 10)
-    err = rel_err_per_field(Vg - U, Vo - U)   # relative to the change over 10 steps
     assert np.all(np.isfinite(Vg))
-    assert rel_err_per_field(Vg, Vo).max() <= TOL_STEP, (name, err)
-    assert np.array_equal(Vg, Vo), (name, err)
+    _same(Vg, Vo, d.exact, TOL_STEP)
 
 
 def test_device_pointers_match_host(case):
@@ -103,6 +115,7 @@ def test_device_pointers_match_host(case):
     name, o, g, U, nu, d = case
     Fh = d.fcn(U)
     Ut = torch.from_numpy(np.ascontiguousarray(U.transpose(2, 1, 0))).cuda()
+    torch.cuda.synchronize()
     Ft = torch.empty_like(Ut)
     d.fcn(Ut, Ft)
     assert np.array_equal(Ft.cpu().numpy().transpose(2, 1, 0), Fh)
@@ -146,16 +159,14 @@ def test_nonfinite_state_reported(oracle_mod, lib_ready):
     d.close()
 
 
-def test_dropin_configuration(oracle_mod, lib_ready):
+@pytest.mark.parametrize("variant", ["exact", "fast"])
+def test_dropin_configuration(oracle_mod, lib_ready, variant):
     """nPanel 30, p 4, nz 45 quadratic, 2 tracers: the full-size drop-in case."""
     o, g, U, nu = make_case(oracle_mod, 30, 4, 45, 2, "quadratic")
-    d = _dycore(g, 2, nu)
-    Fg, Fo = d.fcn(U), o.rhs(U)
-    err = rel_err_per_field(Fg, Fo)
-    assert err.max() <= TOL_RHS, err
-    Vo = o.ros_step(U, 300.0, 1)
+    d = _dycore(g, 2, nu, exact=(variant == "exact"))
+    _same(d.fcn(U), o.rhs(U), d.exact, TOL_RHS)
+    Vo = o.ros_step(U, 120.0, 2)
     Vg = U.copy(order="F")
-    d.time_stepper(Vg, 300.0, 1)
-    assert rel_err_per_field(Vg, Vo).max() <= TOL_STEP
-    assert np.array_equal(Vg, Vo)
+    d.time_stepper(Vg, 120.0, 2)
+    _same(Vg, Vo, d.exact, TOL_STEP)
     d.close()
