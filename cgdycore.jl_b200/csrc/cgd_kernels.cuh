@@ -237,10 +237,13 @@ __device__ __forceinline__ void gather_node(const GP &P, const double *__restric
       }
     }
   } else {
-    for (int f = 0; f < P.NV; ++f) {
-      double a = 0.0;
-      for (int q = q0; q < q1; ++q) a += C[P.inv_off[q] + f * fstr + l];
-      acc[f] = a;
+#pragma unroll
+    for (int f = 0; f < MAXNV; ++f) {
+      if (f < P.NV) {
+        double a = 0.0;
+        for (int q = q0; q < q1; ++q) a += C[P.inv_off[q] + f * fstr + l];
+        acc[f] = a;
+      }
     }
   }
 }
@@ -259,7 +262,9 @@ __global__ void __launch_bounds__(256) k_gather(const GP P, const double *__rest
   const size_t fstr = (size_t)P.DoF * nz;
   double acc[MAXNV];
   gather_node(P, C, g, l, fstr, acc);
-  for (int f = 0; f < P.NV; ++f) out[l + (size_t)nz * (g + (size_t)P.NumG * f)] = acc[f];
+#pragma unroll
+  for (int f = 0; f < MAXNV; ++f)
+    if (f < P.NV) out[l + (size_t)nz * (g + (size_t)P.NumG * f)] = acc[f];
 }
 
 // ---------------------------------------------------------------------------
@@ -315,9 +320,10 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
 {
   extern __shared__ double csm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = blockIdx.x * COL_WARPS + warp;
-  if (g >= P.NumG) return;
+  const int g0 = blockIdx.x * COL_WARPS;
+  const int g = g0 + warp;
   const int nz = P.nz, n = nz - 1, NV = P.NV, NumG = P.NumG;
+  const bool valid = g < NumG;   // no early return: the block synchronises below
   const int LS = nz;                    // per-warp arrays of nz entries
   double *sw = csm + (size_t)warp * (NV + 12) * LS;
   double *fv = sw;                      // [NV][nz]
@@ -328,12 +334,14 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
   const double fac = A.fac;
 
   // 1. tendency (owner gather) + stage corrections ; bands
-  for (int l = lane; l < nz; l += 32) {
+  for (int l = lane; valid && l < nz; l += 32) {
     if (MODE <= 2) {
       const size_t fstr = (size_t)P.DoF * nz;
       double gacc[MAXNV];
       gather_node(P, A.C, g, l, fstr, gacc);
-      for (int f = 0; f < NV; ++f) {
+#pragma unroll
+      for (int f = 0; f < MAXNV; ++f) {
+        if (f >= NV) break;
         double x = gacc[f];
         if (MODE >= 1) x = x + A.rk.c[MODE][0] / A.dt * A.k1[l + (size_t)nz * g + f * fs];
         if (MODE >= 2) x = x + A.rk.c[MODE][1] / A.dt * A.k2[l + (size_t)nz * g + f * fs];
@@ -360,9 +368,11 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
 #define JB(arr, r, i) jb[((arr) * 2 + (r)) * LS + (i)]
   const double invfac = 1.0 / fac;
   const double invfac2 = invfac / fac;
-  double v3new[2];
-  for (int it = 0, l = lane; l < nz; l += 32, ++it) {
-    if (l < n) {   // TriDiagKernel!
+  double v3new[2] = {0.0, 0.0};
+#pragma unroll
+  for (int it = 0; it < 2; ++it) {
+    const int l = lane + 32 * it;
+    if (valid && l < n) {   // TriDiagKernel!
       double t0, t1, t2;
       t1 = invfac2 - JB(1, 1, l) * JB(0, 0, l) - JB(1, 0, l) * JB(0, 1, l) -
            JB(2, 1, l) * JB(3, 0, l) - JB(2, 0, l) * JB(3, 1, l);
@@ -377,23 +387,35 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
     }
   }
   __syncwarp();
-  for (int it = 0, l = lane; l < n; l += 32, ++it) fv[3 * LS + l] = v3new[it];
-  __syncwarp();
-  if (lane == 0) {   // triSolve! (Thomas), b = fv[3], x = xs
-    double *b = fv + 3 * LS;
-    xs[0] = tri[LS + 0];
+#pragma unroll
+  for (int it = 0; it < 2; ++it)
+    if (valid && lane + 32 * it < n) fv[3 * LS + lane + 32 * it] = v3new[it];
+  __syncthreads();
+  // triSolve! (Thomas), b = fv[3], x = xs: the serial sweeps of the block's
+  // columns run concurrently, one per lane of the first warp
+  if (threadIdx.x < COL_WARPS && g0 + (int)threadIdx.x < NumG) {
+    double *sc = csm + (size_t)threadIdx.x * (NV + 12) * LS;
+    double *b = sc + 3 * LS;
+    const double *tr = sc + (NV + 8) * LS;
+    double *x = sc + (NV + 11) * LS;
+    x[0] = tr[LS + 0];
     for (int i = 0; i < n - 1; ++i) {
-      xs[i + 1] = tri[LS + i + 1] - tri[2 * LS + i] / xs[i] * tri[i + 1];
-      b[i + 1] = b[i + 1] - tri[2 * LS + i] / xs[i] * b[i];
+      const double m = tr[2 * LS + i] / x[i];   // the reference's tri[3,i]/x[i], used twice
+      x[i + 1] = tr[LS + i + 1] - m * tr[i + 1];
+      b[i + 1] = b[i + 1] - m * b[i];
     }
-    xs[n - 1] = b[n - 1] / xs[n - 1];
-    for (int i = n - 2; i >= 0; --i) xs[i] = (b[i] - tri[i + 1] * xs[i + 1]) / xs[i];
+    x[n - 1] = b[n - 1] / x[n - 1];
+    for (int i = n - 2; i >= 0; --i) x[i] = (b[i] - tr[i + 1] * x[i + 1]) / x[i];
   }
-  __syncwarp();
-  // SchurSolveBKernel! and the stage update
-  double res[2][MAXNV];
-  for (int it = 0, l = lane; l < nz; l += 32, ++it) {
-    double kw = l < n ? xs[l] : 0.0;
+  __syncthreads();
+  if (!valid) return;
+  // SchurSolveBKernel! and the stage update; each lane owns levels lane and
+  // lane + 32 (compile-time unrolled so nothing is kept in local memory)
+#pragma unroll
+  for (int it = 0; it < 2; ++it) {
+    const int l = lane + 32 * it;
+    if (l >= nz) continue;
+    const double kw = l < n ? xs[l] : 0.0;
     double v0 = fv[l], v4 = fv[4 * LS + l];
     if (l == 0) {
       v0 += JB(0, 0, l) * xs[l];
@@ -405,42 +427,50 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
       v0 += JB(0, 0, l) * xs[l] + JB(0, 1, l - 1) * xs[l - 1];
       v4 += JB(3, 0, l) * xs[l] + JB(3, 1, l - 1) * xs[l - 1];
     }
-    for (int f = 0; f < NV; ++f) {
-      double k;
-      if (f == 3) k = kw;
-      else if (f == 0) k = fac * v0;
-      else if (f == 4) k = fac * v4;
-      else k = fac * fv[f * LS + l];
-      res[it][f] = k;
-    }
     if (MODE == 3) {
       // v after SchurSolveF/B (the Thomas sweep works on a copy, as in
       // SchurSolveTriKernel!'s shared-memory vCol)
       A.v[l + (size_t)nz * g] = v0;
       A.v[l + (size_t)nz * g + 4 * fs] = v4;
-      if (l < n) A.v[l + (size_t)nz * g + 3 * fs] = v3new[it];
+      if (l < n) A.v[l + (size_t)nz * g + 3 * fs] = it == 0 ? v3new[0] : v3new[1];
     }
-  }
-#undef JB
-  // all lanes have finished reading Vn (for the bands) before anything is written
-  __syncwarp();
-  for (int it = 0, l = lane; l < nz; l += 32, ++it) {
-    for (int f = 0; f < NV; ++f) {
-      const size_t o = l + (size_t)nz * g + f * fs;
-      double k = res[it][f];
-      if (MODE == 0) {
-        A.kout[o] = k;
-        A.Vout[o] = A.Vn[o] + A.rk.a[1][0] * k;
-      } else if (MODE == 1) {
-        A.kout[o] = k;
-        A.Vout[o] = A.Vn[o] + A.rk.a[2][0] * A.k1[o] + A.rk.a[2][1] * k;
-      } else if (MODE == 2) {
-        A.Vout[o] = A.Vn[o] + A.rk.m[0] * A.k1[o] + A.rk.m[1] * A.k2[o] + A.rk.m[2] * k;
-      } else {
-        A.kout[o] = k;
+    // all loads of this level first (Vout may alias Vn), then the stores
+    double kk[MAXNV], vn[MAXNV], x1[MAXNV], x2[MAXNV];
+#pragma unroll
+    for (int f = 0; f < MAXNV; ++f) {
+      if (f < NV) {
+        if (f == 3) kk[f] = kw;
+        else if (f == 0) kk[f] = fac * v0;
+        else if (f == 4) kk[f] = fac * v4;
+        else kk[f] = fac * fv[f * LS + l];
+        const size_t o = l + (size_t)nz * g + f * fs;
+        if (MODE <= 2) vn[f] = A.Vn[o];
+        if (MODE >= 1 && MODE <= 2) x1[f] = A.k1[o];
+        if (MODE == 2) x2[f] = A.k2[o];
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < MAXNV; ++f) {
+      if (f < NV) {
+        const size_t o = l + (size_t)nz * g + f * fs;
+        const double k = kk[f];
+        if (MODE == 0) {
+          A.kout[o] = k;
+          A.Vout[o] = vn[f] + A.rk.a[1][0] * k;
+        } else if (MODE == 1) {
+          A.kout[o] = k;
+          A.Vout[o] = vn[f] + A.rk.a[2][0] * x1[f] + A.rk.a[2][1] * k;
+        } else if (MODE == 2) {
+          // Vout may alias Vn: this lane alone reads and writes index o, and all
+          // lanes finished reading Vn for the bands before the block barrier above
+          A.Vout[o] = vn[f] + A.rk.m[0] * x1[f] + A.rk.m[1] * x2[f] + A.rk.m[2] * k;
+        } else {
+          A.kout[o] = k;
+        }
       }
     }
   }
+#undef JB
 }
 
 // Jacobian bands into memory (cgd_jac): one thread per (interface, column)
