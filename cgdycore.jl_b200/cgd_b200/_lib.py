@@ -18,13 +18,14 @@ ERRORS = {
     -5: "CGD_ERR_TIMEOUT", -6: "CGD_ERR_INDEX", -7: "CGD_ERR_UNSUPPORTED", -8: "CGD_ERR_NO_DEVICE",
 }
 PREC_FP64, PREC_MIXED = 0, 1
+NOALLOC_SCRATCH_DOUBLES = 4 * 1024 * 1024
 FLAG_CHECK_FINITE = 1
 
 # every symbol declared in include/cgd_b200.h
 EXPORTS = [
     "cgd_create", "cgd_destroy", "cgd_prepare", "cgd_hypervisc_phase1", "cgd_rhs", "cgd_jac",
-    "cgd_schur_solve", "cgd_ros_step", "cgd_mass_integral", "cgd_get_stream", "cgd_kernel_times",
-    "cgd_strerror", "cgd_version",
+    "cgd_schur_solve", "cgd_ros_step", "cgd_mass_integral", "cgd_jac_schur_solve_noalloc", "cgd_get_stream",
+    "cgd_kernel_times", "cgd_strerror", "cgd_version",
 ]
 
 
@@ -70,6 +71,8 @@ def lib(exact=False):
         L.cgd_ros_step.restype = ctypes.c_int
         L.cgd_mass_integral.argtypes = [vp, vp, vp, vp]
         L.cgd_mass_integral.restype = ctypes.c_int
+        L.cgd_jac_schur_solve_noalloc.argtypes = [ctypes.POINTER(CgdConfig), vp, vp, vp, vp, dbl, vp]
+        L.cgd_jac_schur_solve_noalloc.restype = ctypes.c_int
         L.cgd_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
         L.cgd_get_stream.restype = ctypes.c_int
         L.cgd_kernel_times.argtypes = [vp, ctypes.c_char_p, i32, vp, i32]

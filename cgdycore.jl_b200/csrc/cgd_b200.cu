@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -62,6 +63,12 @@ struct cgd_handle {
 };
 
 namespace {
+
+// Band scratch of the allocation-free Schur solve (cgd_jac_schur_solve_noalloc).
+__device__ __align__(256) double g_noalloc_scratch[CGD_NOALLOC_SCRATCH_DOUBLES];
+constexpr int NOALLOC_MAX_DEVICES = 64;
+double *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+std::mutex g_noalloc_mu;
 
 thread_local std::string g_last_error;
 
@@ -610,6 +617,59 @@ int cgd_mass_integral(cgd_handle *h, const double *U, const double *MMass, doubl
   k_mass_final<<<1, 32, 0, h->stream>>>(h->part, nb, h->scal);
   CK(cudaMemcpyAsync(out, h->scal, 8, cudaMemcpyDeviceToHost, h->stream));
   return finish(h);
+}
+
+int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const double *dz,
+                                double *k, double *v, double fac, void *stream)
+{
+  cgd_handle *h = nullptr;   // for CK(): errors are reported through g_last_error
+  if (!cfg || !U || !dz || !k || !v || !(fac > 0)) return CGD_ERR_INVALID_ARG;
+  if (cfg->nz < 2 || cfg->nz > 64 || cfg->NumTr < 0 || cfg->NumTr > MAXTR) return CGD_ERR_UNSUPPORTED;
+  if (cfg->NumG <= 0) return CGD_ERR_SHAPE;
+  if (!(cfg->Rd > 0) || !(cfg->Cpd > cfg->Rd) || !(cfg->p0 > 0) || !(cfg->Grav > 0)) return CGD_ERR_INVALID_ARG;
+  const size_t need = (size_t)8 * (cfg->nz - 1) * cfg->NumG;
+  if (need > CGD_NOALLOC_SCRATCH_DOUBLES) {
+    char buf[200];
+    snprintf(buf, sizeof buf, "8*(nz-1)*NumG = %zu doubles exceeds the static scratch of %u doubles", need,
+             CGD_NOALLOC_SCRATCH_DOUBLES);
+    g_last_error = buf;
+    return CGD_ERR_SHAPE;
+  }
+  if (!is_device_ptr(U) || !is_device_ptr(dz) || !is_device_ptr(k) || !is_device_ptr(v)) return CGD_ERR_INVALID_ARG;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return CGD_ERR_UNSUPPORTED;
+  double *bands = nullptr;
+  {
+    // once per device, with that device current: the device address of the
+    // static array (its host-side name is only a stand-in)
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void *p = nullptr;
+      CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+      CK(cudaFuncSetAttribute(k_column<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              COL_WARPS * (MAXNV + 12) * 64 * (int)sizeof(double)));
+      g_noalloc_ptr[dev] = static_cast<double *>(p);
+    }
+    bands = g_noalloc_ptr[dev];
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  GP P{};
+  P.nz = cfg->nz; P.NumG = cfg->NumG; P.NumTr = cfg->NumTr; P.NV = 5 + cfg->NumTr;
+  P.dz = dz; P.Grav = cfg->Grav; P.Rd = cfg->Rd; P.p0 = cfg->p0; P.kappa = cfg->Rd / cfg->Cpd;
+  const long long n = (long long)(P.nz - 1) * P.NumG;
+  k_jac<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, U, bands);
+  ColArgs a{};
+  a.v = v;
+  a.kout = k;
+  a.bands = bands;
+  a.fac = fac;
+  a.dt = fac;
+  const size_t smem = (size_t)COL_WARPS * (P.NV + 12) * P.nz * sizeof(double);
+  k_column<3><<<(P.NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, st>>>(P, a);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  return CGD_OK;
 }
 
 int cgd_get_stream(cgd_handle *h, void **stream)

@@ -112,6 +112,29 @@ int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps);
  * Replaces Parallels.GlobalIntegral (src/Parallels/Exchange.jl:1163-1166). */
 int cgd_mass_integral(cgd_handle *h, const double *U, const double *MMass, double *out);
 
+/* Allocation-free Jacobian + column Schur solve, for callers that cannot let
+ * a library call cudaMalloc/cudaFree: code running inside its own stream
+ * capture or a host runtime whose device memory is owned by a pool
+ * allocator (CUDA.jl, PyTorch), where an allocation would synchronise the
+ * device or is not allowed.  No counterpart in the reference (its solve
+ * always uses the JCache arrays allocated with the model).
+ * Computes the vertical acoustic Jacobian bands of U and solves k from v
+ * (v is updated as by cgd_schur_solve), with fac = dt*gamma.  Uses only
+ * cfg->nz, NumG, NumTr, Grav, Rd, Cpd, p0.  U, dz, k, v must be device
+ * memory; the call enqueues on `stream` (a cudaStream_t, NULL = default
+ * stream) and waits for it.
+ * Scratch: the bands live in one file-scope device array of
+ * CGD_NOALLOC_SCRATCH_DOUBLES doubles (32 MiB, held by every GPU that loads
+ * the library until the process exits); 8*(nz-1)*NumG must not exceed it,
+ * otherwise CGD_ERR_SHAPE.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress), so make that first call before any
+ * stream capture.  Every call overwrites the whole band region it uses, so
+ * nothing needs clearing between calls; calls that overlap on the GPU share
+ * the array and race. */
+#define CGD_NOALLOC_SCRATCH_DOUBLES (4u * 1024u * 1024u)
+int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const double *dz,
+                                double *k, double *v, double fac, void *stream);
+
 /* The handle's CUDA stream (cudaStream_t) so a caller can order its own
  * work or timing events with the library's.  No counterpart in the
  * reference (KernelAbstractions owns its queue). */
