@@ -53,6 +53,44 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
+class Ranks:
+    """Rank plumbing: one process per GPU, no collective on the data path.
+    A barrier brackets the timed region and the reported time is the max over
+    ranks.  `device` is the CUDA device for NCCL, None for a CPU (gloo) group."""
+
+    def __init__(self, rank, world, device=None):
+        self.rank, self.world, self.device = rank, world, device
+
+    def barrier(self):
+        import torch
+        if self.world > 1:
+            torch.distributed.barrier()
+        if self.device is not None:
+            torch.cuda.synchronize()
+
+    def max(self, x):
+        import torch
+        if self.world > 1:
+            t = torch.tensor([float(x)], dtype=torch.float64,
+                             device=self.device if self.device is not None else "cpu")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            return float(t.item())
+        return float(x)
+
+
+def member_config(cfg, rank):
+    """Ensemble member of a rank: the configuration with its theta-noise seed
+    offset by the rank."""
+    import dataclasses
+    return dataclasses.replace(cfg, seed_theta=cfg.seed_theta + rank)
+
+
+def aggregate(world, steps, t):
+    """Whole-job steps/s: every rank advanced its own member `steps` times
+    within the max-over-ranks time t."""
+    return world * steps / t
+
+
 def workload_config(cfg, precision):
     return {"workload": f"{cfg.name}: cubed sphere nPanel {cfg.nPanel} ({6 * cfg.nPanel ** 2} elements), "
                         f"OrdPoly {cfg.OrdPoly}, nz {cfg.nz} {cfg.stretch}, NumTr {cfg.NumTr}, "
@@ -154,16 +192,42 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def phase2_bytes(cfg):
-    """Algorithmic bytes of one tendency (phase-2) launch: read the stage state
-    (NV fields), the DSS'd hyperviscosity cache (5+NumTr fields), the lumped
-    mass (2 fields) and the 17-component element metric; write one tendency
-    value per DOF and field."""
+def _units(cfg):
+    """S (bytes of one FP64 field over all column-levels), E (one FP64 value
+    per element-node-level), S' (one per column interface) and NV."""
     numg = 6 * cfg.nPanel ** 2 * cfg.OrdPoly ** 2 + 2
     S = numg * cfg.nz * 8
     E = 6 * cfg.nPanel ** 2 * (cfg.OrdPoly + 1) ** 2 * cfg.nz * 8
-    NV = 5 + cfg.NumTr
-    return NV * S + (5 + cfg.NumTr) * S + 2 * S + 17 * E + NV * S
+    return S, E, numg * (cfg.nz - 1) * 8, 5 + cfg.NumTr
+
+
+def phase2_bytes(cfg):
+    """Algorithmic bytes of one tendency (phase-2) launch: the phase-2 term of
+    the per-stage RHS count with the stage state read once (it arrives
+    combined; the combination is counted with the column kernel that forms
+    it): stage state NV*S + DSS'd hyperviscosity cache (5+NumTr)*S + the
+    lumped-mass sum S + 22 metric values per element-node-level (14 dXdxI,
+    2 J, 6 X in the reference layout) + the tendency NV*S."""
+    S, E, _, NV = _units(cfg)
+    return NV * S + (5 + cfg.NumTr) * S + 22 * E + S + NV * S
+
+
+def step_bytes(cfg):
+    """Algorithmic bytes of one SSP-Knoth Rosenbrock-W step (3 stages, FP64,
+    stage combinations counted fused, pressure in register):
+      stage i: RHS phase 1 (4+NT)*i*S + 10E + S + (5+NT)*S
+               RHS phase 2 NV*i*S + (5+NT)*S + 22E + S + NV*S
+               Schur       NV*S + (i-1)*NV*S + 8S' + NV*S
+      per step: Jacobian 3S + 8S', final update 5*NV*S.
+    13.35 GB at nPanel 30, p 4, nz 45, 2 tracers."""
+    S, E, Sp, NV = _units(cfg)
+    NT = cfg.NumTr
+    tot = 0
+    for i in (1, 2, 3):
+        tot += (4 + NT) * i * S + 10 * E + S + (5 + NT) * S
+        tot += NV * i * S + (5 + NT) * S + 22 * E + S + NV * S
+        tot += NV * S + (i - 1) * NV * S + 8 * Sp + NV * S
+    return tot + 3 * S + 8 * Sp + 5 * NV * S
 
 
 def ncu_traffic():
@@ -203,25 +267,12 @@ def run_ours(args, cfg, rank, world, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     os.environ.setdefault("CGD_PROFILE", "1")
-    import dataclasses
-
     from cgd_b200 import setup
-    mcfg = dataclasses.replace(cfg, seed_theta=cfg.seed_theta + rank)
-    dyc, U0, mcfg = setup(mcfg, precision=args.precision)
+    dyc, U0, mcfg = setup(member_config(cfg, rank), precision=args.precision)
     stream = torch.cuda.ExternalStream(dyc.stream())
     Ut = torch.from_numpy(np.ascontiguousarray(U0.transpose(2, 1, 0))).cuda()
-
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if world > 1:
-            t = torch.tensor([x], dtype=torch.float64, device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            return float(t.item())
-        return x
+    ranks = Ranks(rank, world, torch.device("cuda", local))
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     dt = cfg.dt
     dyc.time_stepper(Ut, dt, args.warmup)          # includes the one-time graph capture
@@ -237,7 +288,7 @@ def run_ours(args, cfg, rank, world, local):
     barrier()
     clk = clocks.stop()
     t = max_over_ranks(t)
-    value = world * args.steps / t
+    value = aggregate(world, args.steps, t)
     ktimes = dyc.kernel_times()
     assert torch.isfinite(Ut).all().item()
 
@@ -253,7 +304,7 @@ def run_ours(args, cfg, rank, world, local):
     e1.synchronize()
     te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
     state_bytes = int(np.prod(U0.shape)) * 8
-    e2e = {"value": world * Ke / te, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+    e2e = {"value": aggregate(world, Ke, te), "unit": UNIT, "h2d_bytes_per_step": state_bytes,
            "d2h_bytes_per_step": state_bytes, "steps": Ke,
            "call": "cgd_ros_step(h, host_state, dt, 1) per step (pinned host buffer)"}
 
@@ -276,6 +327,7 @@ def run_ours(args, cfg, rank, world, local):
         b_p2 = phase2_bytes(cfg)
         ach = b_p2 / t_p2 / 1e9
         step_ms = t / args.steps * 1e3
+        b_step = step_bytes(cfg)
         shares = {k: round(float(np.sum(v)) / max(1e-12, sum(float(np.sum(x)) for x in fam.values())), 4)
                   for k, v in fam.items()}
         line = {
@@ -287,7 +339,9 @@ def run_ours(args, cfg, rank, world, local):
             "dof_updates_per_s": value * unique_dof(cfg),
             "roofline": {"bound": "hbm", "kernel": "k_phase2 (fused tendency)", "achieved": ach, "peak": peak,
                          "peak_kind": kind, "unit": "GB/s", "frac": ach / peak, "traffic": ncu_traffic(),
-                         "algorithmic_bytes_per_launch": b_p2, "launch_ms": t_p2 * 1e3},
+                         "algorithmic_bytes_per_launch": b_p2, "launch_ms": t_p2 * 1e3,
+                         "step": {"algorithmic_bytes": b_step, "achieved": b_step / (step_ms * 1e-3) / 1e9,
+                                  "frac": b_step / (step_ms * 1e-3) / 1e9 / peak}},
             "kernel_ms_last_step": {k: [round(x, 4) for x in v] for k, v in fam.items()},
             "kernel_share": shares,
             "e2e": e2e,

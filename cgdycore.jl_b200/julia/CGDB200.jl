@@ -1,0 +1,146 @@
+# CGDB200.jl - Julia binding of libcgd_b200.so for CGDycore.jl.
+#
+# Drop-in replacements for the functions that CGDycore.jl passes into
+# Integration.TimeStepper! (src/Integration/TimeStepper.jl:1,103-124):
+#
+#   Fcn!             = GPU.FcnGPU!          (src/GPU/FcnGPU.jl:552)
+#   FcnPrepare!      = GPU.FcnPrepareGPU!   (src/GPU/DiagnosticKernel.jl:180)
+#   Jac!             = DyCore.JacSchurGPU!  (src/DyCore/JacSchur.jl:3)
+#   RosenbrockSchur! = Integration.RosenbrockSchur! (src/Integration/RosenbrockSchur.jl:1)
+#
+# The arguments are the reference's own (CG, Metric, Phys, Cache, Exchange,
+# Global, Param, DiscType); the library keeps its device copies of the grid
+# in a handle created once from them.  State arrays (CuArray or Array,
+# Float64, layout (nz, NumG, NV)) are passed by pointer without copies when
+# they live on the device.
+module CGDB200
+
+const libcgd = get(ENV, "CGD_B200_LIB", joinpath(@__DIR__, "..", "libcgd_b200.so"))
+
+# struct cgd_config (include/cgd_b200.h)
+struct CgdConfig
+  OrdPoly::Int32
+  nz::Int32
+  NumTr::Int32
+  NF::Int32
+  NumG::Int32
+  precision::Int32
+  flags::Int32
+  reserved::Int32
+  Grav::Float64
+  Rd::Float64
+  Cpd::Float64
+  p0::Float64
+  Omega::Float64
+  HyperDCurl::Float64
+  HyperDGrad::Float64
+  HyperDDiv::Float64
+end
+
+mutable struct Handle
+  ptr::Ptr{Cvoid}
+end
+
+check(rc, what) = rc == 0 || error("$what: " * unsafe_string(ccall((:cgd_strerror, libcgd), Cstring, (Cint,), rc)))
+
+hostcopy(a) = Array{eltype(a)}(a)
+
+# One handle per (CG, Metric) pair; created on first use.
+const HANDLES = IdDict{Any,Handle}()
+
+function config(CG, Global, Phys; mixed = false, check_finite = false)
+  CgdConfig(CG.OrdPoly, Global.Grid.nz, Global.Model.NumTr, Global.Grid.NumFaces, CG.NumG,
+            mixed ? 1 : 0, check_finite ? 1 : 0, 0,
+            Phys.Grav, Phys.Rd, Phys.Cpd, Phys.p0, Phys.Omega,
+            Global.Model.HyperDCurl, Global.Model.HyperDGrad, Global.Model.HyperDDiv)
+end
+
+function handle(CG, Metric, Phys, Global)
+  get!(HANDLES, Metric) do
+    cfg = Ref(config(CG, Global, Phys))
+    glob = Int64.(hostcopy(CG.Glob))
+    DS, DW = hostcopy(CG.DS), hostcopy(CG.DW)
+    dXdxI, J, X = hostcopy(Metric.dXdxI), hostcopy(Metric.J), hostcopy(Metric.X)
+    M, dz = hostcopy(CG.M), hostcopy(Metric.dz)
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    rc = ccall((:cgd_create, libcgd), Cint,
+               (Ref{CgdConfig}, Ptr{Int64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+                Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ref{Ptr{Cvoid}}),
+               cfg, glob, DS, DW, dXdxI, J, X, M, dz, out)
+    check(rc, "cgd_create")
+    h = Handle(out[])
+    finalizer(x -> ccall((:cgd_destroy, libcgd), Cvoid, (Ptr{Cvoid},), x.ptr), h)
+    h
+  end
+end
+
+# Pointer of a host Array or a CuArray (CUDA.jl converts CuArray to CuPtr;
+# the library accepts either kind of address).
+dptr(a::Array{Float64}) = pointer(a)
+dptr(a) = reinterpret(Ptr{Float64}, UInt(pointer(a)))
+
+# FcnPrepare!(U, CG, Metric, Phys, Cache, Exchange, Global, Param, DiscType):
+# the pressure is recomputed in registers by every kernel that needs it, so
+# this only refreshes Cache.AuxG[:,:,1] when the caller wants p on the host side.
+function FcnPrepareB200!(U, CG, Metric, Phys, Cache, Exchange, Global, Param, DiscType)
+  h = handle(CG, Metric, Phys, Global)
+  p = Cache.AuxG
+  GC.@preserve U p begin
+    check(ccall((:cgd_prepare, libcgd), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}),
+                h.ptr, dptr(U), dptr(p)), "cgd_prepare")
+  end
+end
+
+# Fcn!(F, U, CG, Metric, Phys, Cache, Exchange, Global, Param, DiscType)
+function FcnB200!(F, U, CG, Metric, Phys, Cache, Exchange, Global, Param, DiscType)
+  h = handle(CG, Metric, Phys, Global)
+  GC.@preserve F U begin
+    check(ccall((:cgd_rhs, libcgd), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}),
+                h.ptr, dptr(U), dptr(F)), "cgd_rhs")
+  end
+end
+
+# Jac!(JCache, U, CG, Metric, Phys, Cache, Global, Param, DiscType): bands stay
+# in the handle for SchurSolveB200!.
+function JacB200!(JCache, U, CG, Metric, Phys, Cache, Global, Param, DiscType)
+  h = handle(CG, Metric, Phys, Global)
+  GC.@preserve U begin
+    check(ccall((:cgd_jac, libcgd), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}),
+                h.ptr, dptr(U), C_NULL), "cgd_jac")
+  end
+end
+
+# SchurSolveGPU!(k, v, JCache, fac, Cache, Global) with the handle of the
+# last JacB200! call.
+function SchurSolveB200!(k, v, CG, Metric, Phys, Global, fac)
+  h = handle(CG, Metric, Phys, Global)
+  GC.@preserve k v begin
+    check(ccall((:cgd_schur_solve, libcgd), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Cdouble),
+                h.ptr, dptr(k), dptr(v), fac), "cgd_schur_solve")
+  end
+end
+
+# RosenbrockSchur!(V, dt, Fcn!, FcnPrepare!, Jac, CG, Metric, Phys, Cache,
+# JCache, Exchange, Global, Param, DiscType): one SSP-Knoth step in place, as
+# one CUDA graph.  Fcn!/FcnPrepare!/Jac are ignored (the library fuses them).
+function RosenbrockSchurB200!(V, dt, Fcn!, FcnPrepare!, Jac, CG, Metric, Phys, Cache, JCache,
+                              Exchange, Global, Param, DiscType)
+  h = handle(CG, Metric, Phys, Global)
+  GC.@preserve V begin
+    check(ccall((:cgd_ros_step, libcgd), Cint, (Ptr{Cvoid}, Ptr{Float64}, Cdouble, Int32),
+                h.ptr, dptr(V), dt, Int32(1)), "cgd_ros_step")
+  end
+end
+
+# Allocation-free Jacobian + Schur solve (no counterpart in the reference):
+# bands in a static 32 MiB device array; 8*(nz-1)*NumG <= 4_194_304.
+function JacSchurSolveNoAlloc!(k, v, U, dz, CG, Global, Phys, fac; stream = C_NULL)
+  cfg = Ref(config(CG, Global, Phys))
+  GC.@preserve k v U dz begin
+    check(ccall((:cgd_jac_schur_solve_noalloc, libcgd), Cint,
+                (Ref{CgdConfig}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Cdouble, Ptr{Cvoid}),
+                cfg, dptr(U), dptr(dz), dptr(k), dptr(v), fac, stream), "cgd_jac_schur_solve_noalloc")
+  end
+end
+
+end # module
