@@ -110,11 +110,6 @@ bool is_device_ptr(const void *p)
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
-template <int N, int LC>
-size_t smem_max()
-{
-  return SweepCfg<N, LC>::smem(MAXTR);
-}
 
 template <int N>
 void launch_hv1(cgd_handle *h, const double *U, double *C)
@@ -127,15 +122,15 @@ void launch_hv1(cgd_handle *h, const double *U, double *C)
 template <int N>
 void launch_p2(cgd_handle *h, const double *U, const double *T1, double *C)
 {
-  constexpr int LC = 256 / (N * N);
-  using CF = SweepCfg<N, LC>;
-  size_t smem = CF::smem(h->NumTr);
+  using CF = P2Cfg<N>;
+  const size_t smem = CF::smem(h->NumTr);
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_phase2_sweep<N, LC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max<N, LC>());
+    cudaFuncSetAttribute(k_phase2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::smem(MAXTR));
     attr = true;
   }
-  k_phase2_sweep<N, LC><<<h->NF, CF::THREADS, smem, h->stream>>>(h->gp, U, T1, C);
+  dim3 grid((h->nz + CF::LC - 1) / CF::LC, h->NF);
+  k_phase2<N><<<grid, CF::THREADS, smem, h->stream>>>(h->gp, U, T1, C);
 }
 
 void hv1(cgd_handle *h, const double *U, double *C)
@@ -158,10 +153,11 @@ void phase2(cgd_handle *h, const double *U, const double *T1, double *C)
   }
 }
 
-void gather(cgd_handle *h, const double *C, double *out)
+void gather(cgd_handle *h, const double *C, double *out, bool wsplit)
 {
   long long n = (long long)h->nz * h->NumG;
-  k_gather<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->gp, C, out);
+  if (wsplit) k_gather<true><<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->gp, C, out);
+  else k_gather<false><<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->gp, C, out);
 }
 
 template <int MODE>
@@ -201,7 +197,7 @@ void enqueue_step(cgd_handle *h, double *U, double dt)
     const double *Vsrc = stage == 0 ? U : h->Vst;
     hv1(h, Vsrc, h->C);
     rec(h, e++);
-    gather(h, h->C, h->T1);
+    gather(h, h->C, h->T1, false);
     rec(h, e++);
     phase2(h, Vsrc, h->T1, h->C);
     rec(h, e++);
@@ -314,7 +310,7 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
     for (int ID = 0; ID < DoF; ++ID) {
       int g = (int)glob[ID + (size_t)DoF * IF] - 1;
       glob0[ID + (size_t)DoF * IF] = g;
-      off[fill[g]++] = ((long long)IF * NV * DoF + ID) * nz;
+      off[fill[g]++] = ((long long)IF * (NV + 1) * DoF + ID) * nz;
     }
 
   // ---- compact metric [IF][comp][ID][nz]
@@ -377,7 +373,7 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
   TRY(dalloc(h, &h->glob, glob0.size()));
   TRY(dalloc(h, &h->inv_ptr, ptr.size()));
   TRY(dalloc(h, &h->inv_off, off.size()));
-  TRY(dalloc(h, &h->C, ENL * NV));
+  TRY(dalloc(h, &h->C, ENL * (NV + 1)));
   TRY(dalloc(h, &h->T1, S * NV));
   TRY(dalloc(h, &h->Vst, S * NV));
   TRY(dalloc(h, &h->k1, S * NV));
@@ -407,7 +403,7 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
   }
 
   GP &P = h->gp;
-  P.N = N; P.DoF = DoF; P.nz = nz; P.NF = NF; P.NumG = NumG; P.NumTr = h->NumTr; P.NV = NV;
+  P.N = N; P.DoF = DoF; P.nz = nz; P.NF = NF; P.NumG = NumG; P.NumTr = h->NumTr; P.NV = NV; P.NC = NV + 1;
   P.met = h->met; P.M = h->M; P.dz = h->dz; P.glob = h->glob; P.inv_ptr = h->inv_ptr; P.inv_off = h->inv_off;
   for (int i = 0; i < 25; ++i) { P.D[i] = 0.0; P.DW[i] = 0.0; }
   for (int i = 0; i < N * N; ++i) { P.D[i] = DS[i]; P.DW[i] = DW[i]; }
@@ -495,7 +491,7 @@ int cgd_hypervisc_phase1(cgd_handle *h, const double *U, double *Temp1)
   bool tdev = is_device_ptr(Temp1);
   double *td = tdev ? Temp1 : h->Fbuf;
   hv1(h, Ud, h->C);
-  gather(h, h->C, td);
+  gather(h, h->C, td, false);
   if (!tdev)
     CK(cudaMemcpyAsync(Temp1, td, (size_t)h->nz * h->NumG * h->NV * 8, cudaMemcpyDeviceToHost, h->stream));
   return finish(h);
@@ -511,9 +507,9 @@ int cgd_rhs(cgd_handle *h, const double *U, double *F)
   bool fdev = is_device_ptr(F);
   double *fd = fdev ? F : h->Fbuf;
   hv1(h, Ud, h->C);
-  gather(h, h->C, h->T1);
+  gather(h, h->C, h->T1, false);
   phase2(h, Ud, h->T1, h->C);
-  gather(h, h->C, fd);
+  gather(h, h->C, fd, true);
   if (!fdev) CK(cudaMemcpyAsync(F, fd, (size_t)h->nz * h->NumG * h->NV * 8, cudaMemcpyDeviceToHost, h->stream));
   return finish(h);
 }
@@ -655,7 +651,7 @@ int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const do
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   GP P{};
-  P.nz = cfg->nz; P.NumG = cfg->NumG; P.NumTr = cfg->NumTr; P.NV = 5 + cfg->NumTr;
+  P.nz = cfg->nz; P.NumG = cfg->NumG; P.NumTr = cfg->NumTr; P.NV = 5 + cfg->NumTr; P.NC = P.NV + 1;
   P.dz = dz; P.Grav = cfg->Grav; P.Rd = cfg->Rd; P.p0 = cfg->p0; P.kappa = cfg->Rd / cfg->Cpd;
   const long long n = (long long)(P.nz - 1) * P.NumG;
   k_jac<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, U, bands);

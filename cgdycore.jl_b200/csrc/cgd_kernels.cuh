@@ -6,7 +6,9 @@
 //                          and level (14 used dXdxI entries, J bottom/top,
 //                          2*Omega*sin(lat) at the layer midpoint, the four
 //                          J-only coefficients of RecU4 at the interface above)
-//   C  (contributions)     [IF][field][ID][nz]  element-local DSS inputs
+//   C  (contributions)     [IF][slot][ID][nz]  element-local DSS inputs; NV + 1
+//                          slots (the tendency fields, then the lower-node
+//                          part of the phase-2 w contribution, one level down)
 //   M                      (nz, NumG, 2)
 //
 // Direct-stiffness summation is an owner gather: the element kernels write
@@ -54,12 +56,13 @@ constexpr int MAXNV = 5 + MAXTR;
 // Everything a kernel needs about the grid, passed by value.
 struct GP {
   int N, DoF, nz, NF, NumG, NumTr, NV;
+  int NC;                   // contribution slots per element node: NV fields + the lower-node w of phase 2
   const double *met;        // [IF][comp][ID][nz]
   const double *M;          // (nz, NumG, 2)
   const double *dz;         // (nz, NumG)
   const int *glob;          // [IF*DoF + ID], 0-based
   const int *inv_ptr;       // NumG + 1
-  const long long *inv_off; // (IF*NV*DoF + ID)*nz for every contributor
+  const long long *inv_off; // (IF*NC*DoF + ID)*nz for every contributor
   double D[25], DW[25];     // D[i + N*j] = DS[i,j]
   double Grav, Rd, p0, kappa, nuCurl, nuGrad, nuDiv;
 };
@@ -154,7 +157,7 @@ __global__ void __launch_bounds__(256) k_hypervisc1(const GP P, const double *__
     s[8][si] = d21 * GradDx + d22 * GradDy;
   }
   __syncthreads();
-  double *out = C + ((size_t)IF * P.NV * DoF + ID) * nz + l;
+  double *out = C + ((size_t)IF * P.NC * DoF + ID) * nz + l;
   if (act) {
     const double *Cu = s[5] + row, *Dv = s[6] + row, *Cx = s[7] + row, *Cy = s[8] + row;
     double DxCurl = P.DW[I] * Cu[N * Jn], DyCurl = P.DW[Jn] * Cu[I];
@@ -213,22 +216,36 @@ __global__ void __launch_bounds__(256) k_hypervisc1(const GP P, const double *__
 
 // Sum the contributions of the element nodes sharing global DOF g at level l
 // (ascending element, node order) for every field.  Up to four contributors
-// (every cubed-sphere node) are loaded with independent loads.
+// (every cubed-sphere node) are loaded with independent loads.  WSPLIT (the
+// phase-2 tendency): a node's contribution to w at interface l is its upper
+// part (slot 3, level l) plus its lower part (slot NV, stored at level l),
+// zero at the top level.
+template <bool WSPLIT>
 __device__ __forceinline__ void gather_node(const GP &P, const double *__restrict__ C, int g, int l, size_t fstr,
                                             double *acc)
 {
   const int q0 = P.inv_ptr[g], q1 = P.inv_ptr[g + 1];
   const int nq = q1 - q0;
+  const bool wtop = WSPLIT && l == P.nz - 1;
   if (nq <= 4) {
     long long o[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) o[j] = j < nq ? P.inv_off[q0 + j] + l : 0;
+    double wlo[4];
+    if (WSPLIT) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) wlo[j] = j < nq && !wtop ? C[o[j] + P.NV * fstr] : 0.0;
+    }
 #pragma unroll
     for (int f = 0; f < MAXNV; ++f) {
       if (f < P.NV) {
         double x[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) x[j] = j < nq ? C[o[j] + f * fstr] : 0.0;
+        for (int j = 0; j < 4; ++j) x[j] = j < nq && !(WSPLIT && f == 3 && wtop) ? C[o[j] + f * fstr] : 0.0;
+        if (WSPLIT && f == 3) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) x[j] = wtop ? 0.0 : x[j] + wlo[j];
+        }
         double a = 0.0;
 #pragma unroll
         for (int j = 0; j < 4; ++j)
@@ -241,7 +258,12 @@ __device__ __forceinline__ void gather_node(const GP &P, const double *__restric
     for (int f = 0; f < MAXNV; ++f) {
       if (f < P.NV) {
         double a = 0.0;
-        for (int q = q0; q < q1; ++q) a += C[P.inv_off[q] + f * fstr + l];
+        for (int q = q0; q < q1; ++q) {
+          const long long o = P.inv_off[q] + l;
+          double x = C[o + f * fstr];
+          if (WSPLIT && f == 3) x = wtop ? 0.0 : x + C[o + P.NV * fstr];
+          a += x;
+        }
         acc[f] = a;
       }
     }
@@ -252,6 +274,7 @@ __device__ __forceinline__ void gather_node(const GP &P, const double *__restric
 // Owner gather (DSS): out(l, g, f) = sum over contributors in ascending
 // (element, node) order.  Thread per (g, l), level fastest.
 // ---------------------------------------------------------------------------
+template <bool WSPLIT>
 __global__ void __launch_bounds__(256) k_gather(const GP P, const double *__restrict__ C,
                                                 double *__restrict__ out)
 {
@@ -261,7 +284,7 @@ __global__ void __launch_bounds__(256) k_gather(const GP P, const double *__rest
   const int g = (int)(tid / nz), l = (int)(tid % nz);
   const size_t fstr = (size_t)P.DoF * nz;
   double acc[MAXNV];
-  gather_node(P, C, g, l, fstr, acc);
+  gather_node<WSPLIT>(P, C, g, l, fstr, acc);
 #pragma unroll
   for (int f = 0; f < MAXNV; ++f)
     if (f < P.NV) out[l + (size_t)nz * (g + (size_t)P.NumG * f)] = acc[f];
@@ -338,7 +361,7 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
     if (MODE <= 2) {
       const size_t fstr = (size_t)P.DoF * nz;
       double gacc[MAXNV];
-      gather_node(P, A.C, g, l, fstr, gacc);
+      gather_node<true>(P, A.C, g, l, fstr, gacc);
 #pragma unroll
       for (int f = 0; f < MAXNV; ++f) {
         if (f >= NV) break;
