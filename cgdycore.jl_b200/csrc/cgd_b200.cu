@@ -119,18 +119,29 @@ void launch_hv1(cgd_handle *h, const double *U, double *C)
   k_hypervisc1<N><<<grid, 256, 0, h->stream>>>(h->gp, U, C);
 }
 
-template <int N>
+template <int N, int NT>
 void launch_p2(cgd_handle *h, const double *U, const double *T1, double *C)
 {
-  using CF = P2Cfg<N>;
-  const size_t smem = CF::smem(h->NumTr);
+  using CF = P2Cfg<N, NT>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_phase2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::smem(MAXTR));
+    cudaFuncSetAttribute(k_phase2<N, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
     attr = true;
   }
   dim3 grid((h->nz + CF::LC - 1) / CF::LC, h->NF);
-  k_phase2<N><<<grid, CF::THREADS, smem, h->stream>>>(h->gp, U, T1, C);
+  k_phase2<N, NT><<<grid, CF::THREADS, CF::SMEM, h->stream>>>(h->gp, U, T1, C);
+}
+
+template <int N>
+void launch_p2(cgd_handle *h, const double *U, const double *T1, double *C)
+{
+  switch (h->NumTr) {
+    case 0: launch_p2<N, 0>(h, U, T1, C); break;
+    case 1: launch_p2<N, 1>(h, U, T1, C); break;
+    case 2: launch_p2<N, 2>(h, U, T1, C); break;
+    case 3: launch_p2<N, 3>(h, U, T1, C); break;
+    default: launch_p2<N, 4>(h, U, T1, C); break;
+  }
 }
 
 void hv1(cgd_handle *h, const double *U, double *C)

@@ -5,15 +5,18 @@
 // LPW = 32 / N^2 levels).  Grid: (chunks, elements), chunks fastest so the
 // chunks of one element, which share their halo planes, run together.
 //
+// The number of tracers NT is a template parameter.
+//
 //   1. The CTA stages the pointwise quantities of its LC levels plus two halo
 //      planes on each side (state, vertical metric, lumped mass, pressure,
 //      theta and tracer ratios) in shared memory.  One barrier.
-//   2. Each warp then works on its own level alone.  Every horizontal D/DW
+//   2. One thread per (node, interface) forms the vertical mass flux and the
+//      limited upwind fluxes of the interfaces L0-1 .. L0+LC-1 (the one below
+//      the chunk is formed by both neighbouring chunks, with identical
+//      operations).  One barrier.
+//   3. Each warp then works on its own level alone.  Every horizontal D/DW
 //      derivative sum goes through a per-warp scratch with __syncwarp only;
 //      the terms that couple levels read the neighbour planes staged in 1.
-//      The upwind fluxes of both interfaces of a level are formed by that
-//      level (the interface between two chunks is formed by both, with
-//      identical operations).
 //
 // The vertical momentum equation lives on interfaces: the contribution of
 // the element node to w at interface l is hi(l) + lo(l+1), hi from the upper
@@ -36,52 +39,71 @@ enum {
   Q_M0, Q_M1, Q_P, Q_J0, Q_CTH,
   Q_TR0   // + one per tracer: rho*q / rho
 };
+// quantities of the CTA's own levels per (level, node)
+enum {
+  O_D110 = 0, O_D111, O_D120, O_D121, O_D210, O_D211, O_D220, O_D221, O_J1, O_FC,
+  O_T1    // + 5 + NumTr: the DSS'd hyperviscosity cache
+};
 constexpr int P2_WARPS = 8;
 constexpr int P2_NSCR = 12;   // scratch quantities per warp (the largest derivative round)
 
-template <int N>
+template <int N, int NT>
 struct P2Cfg {
   static constexpr int DoF = N * N;
   static constexpr int LPW = 32 / DoF;           // levels per warp
   static constexpr int LC = P2_WARPS * LPW;      // levels per CTA
   static constexpr int R = LC + 4;               // staged planes
   static constexpr int THREADS = 32 * P2_WARPS;
-  static size_t smem(int NT)
-  {
-    return ((size_t)(Q_TR0 + NT) * R * DoF + (size_t)P2_WARPS * P2_NSCR * 32) * sizeof(double);
-  }
+  static constexpr size_t SMEM = ((size_t)(Q_TR0 + NT) * R * DoF + (size_t)(O_T1 + 5 + NT) * LC * DoF +
+                                   (size_t)(2 + NT) * (LC + 1) * DoF + (size_t)P2_WARPS * P2_NSCR * 32) *
+                                  sizeof(double);
 };
 
-template <int N>
-__global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
+template <int N, int NT>
+__global__ void __launch_bounds__(P2Cfg<N, NT>::THREADS, 2)
     k_phase2(const GP P, const double *__restrict__ U, const double *__restrict__ T1, double *__restrict__ C)
 {
-  using CF = P2Cfg<N>;
+  using CF = P2Cfg<N, NT>;
   constexpr int DoF = CF::DoF, LPW = CF::LPW, LC = CF::LC, R = CF::R;
   extern __shared__ double sm[];
-  const int NT = P.NumTr;
   const int nz = P.nz, NumG = P.NumG;
   const int IF = blockIdx.y;
   const int L0 = blockIdx.x * LC;
   const size_t cs = (size_t)DoF * nz, fs = (size_t)nz * NumG;
   double *pw = sm;                                             // [Q][R][DoF]
-  double *scr = sm + (size_t)(Q_TR0 + NT) * R * DoF;            // [warp][P2_NSCR][32]
+  double *ow = pw + (size_t)(Q_TR0 + NT) * R * DoF;             // [O][LC][DoF]
+  double *fx = ow + (size_t)(O_T1 + 5 + NT) * LC * DoF;         // [2+NT][LC+1][DoF] interface fluxes
+  double *scr = fx + (size_t)(2 + NT) * (LC + 1) * DoF;         // [warp][P2_NSCR][32]
   const double *mte = P.met + (size_t)IF * NCOMP * cs;
 #define PW(q, p, id) pw[((size_t)(q) * R + (p)) * DoF + (id)]
 
   // ---------------- 1. stage the pointwise planes L0-2 .. L0+LC+1 ----------------
+  // (level fastest: every load is a run of consecutive levels of one column
+  // or one metric row) and the own levels' metric and cache
   for (int s = threadIdx.x; s < DoF * R; s += CF::THREADS) {
-    const int ID = s / R, p = s % R;   // level fastest: runs of consecutive levels per column
+    const int ID = s / R, p = s % R;
     const int lev = L0 - 2 + p;
     if (lev < 0 || lev >= nz) continue;
     const int g = P.glob[IF * DoF + ID];
     const double *Ug = U + (size_t)nz * g + lev;
+    const double *mt = mte + (size_t)ID * nz + lev;
+    if (p >= 2 && p <= LC + 1) {
+      double *o = ow + (size_t)(p - 2) * DoF + ID;
+      constexpr size_t os = (size_t)LC * DoF;
+      o[O_D110 * os] = mt[C_D11_0 * cs]; o[O_D111 * os] = mt[C_D11_1 * cs];
+      o[O_D120 * os] = mt[C_D12_0 * cs]; o[O_D121 * os] = mt[C_D12_1 * cs];
+      o[O_D210 * os] = mt[C_D21_0 * cs]; o[O_D211 * os] = mt[C_D21_1 * cs];
+      o[O_D220 * os] = mt[C_D22_0 * cs]; o[O_D221 * os] = mt[C_D22_1 * cs];
+      o[O_J1 * os] = mt[C_J1 * cs];
+      o[O_FC * os] = mt[C_FCOR * cs];
+      const double *T = T1 + (size_t)nz * g + lev;
+      for (int f = 0; f < 5 + NT; ++f) o[(O_T1 + f) * os] = T[f * fs];
+    }
     const double rho = Ug[0], rth = Ug[4 * fs];
     PW(Q_RHO, p, ID) = rho;
     PW(Q_CTH, p, ID) = rth / rho;
     for (int q = 0; q < NT; ++q) PW(Q_TR0 + q, p, ID) = Ug[(5 + q) * fs] / rho;
     if (p == 0 || p == R - 1) continue;   // the outer halo planes feed the upwind stencil only
-    const double *mt = mte + (size_t)ID * nz + lev;
     PW(Q_U, p, ID) = Ug[fs];
     PW(Q_V, p, ID) = Ug[2 * fs];
     PW(Q_W, p, ID) = Ug[3 * fs];
@@ -95,7 +117,42 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
   }
   __syncthreads();
 
-  // ---------------- 2. one level per warp (LPW levels for N < 5) ----------------
+  // ---------------- 2. interface fluxes ----------------
+  // wCon and the limited upwind fluxes (RecU4, OperatorKernel.jl:1044-1059,
+  // J-only coefficients precomputed) of the interface il between levels il
+  // and il+1, stored unscaled per interface
+  for (int s = threadIdx.x; s < DoF * (LC + 1); s += CF::THREADS) {
+    const int ID = s / (LC + 1), i = s % (LC + 1);
+    const int il = L0 - 1 + i;
+    if (il < 0 || il >= nz - 1) continue;
+    const int pl = i + 1;   // plane of level il
+    const double wI = PW(Q_W, pl, ID);
+    const double wCon =
+        PW(Q_RHO, pl, ID) * (PW(Q_D311, pl, ID) * PW(Q_U, pl, ID) + PW(Q_D321, pl, ID) * PW(Q_V, pl, ID) +
+                             PW(Q_D331, pl, ID) * wI) +
+        PW(Q_RHO, pl + 1, ID) * (PW(Q_D310, pl + 1, ID) * PW(Q_U, pl + 1, ID) +
+                                 PW(Q_D320, pl + 1, ID) * PW(Q_V, pl + 1, ID) + PW(Q_D330, pl + 1, ID) * wI);
+    const double *mt = mte + (size_t)ID * nz + il;
+    const double kR1 = mt[C_RK0 * cs], kL1 = mt[C_RK1 * cs], kL2 = mt[C_RK2 * cs], kR2 = mt[C_RK3 * cs];
+    const int pm = il > 0 ? pl - 1 : pl, pp2 = il + 2 < nz ? pl + 2 : pl + 1;
+    const double aw = fabs(wCon);
+    auto upwind = [&](int q) {
+      const double cLL = PW(q, pm, ID), cL = PW(q, pl, ID), cR = PW(q, pl + 1, ID), cRR = PW(q, pp2, ID);
+      double r = (cL - cLL) / (cR - cL + 1.e-20);
+      const double cFL = cL + cgd_max(0.0, cgd_min(r, cgd_min(kL1 * r + kR1, 1.0))) * (cR - cL);
+      r = (cR - cRR) / (cL - cR + 1.e-20);
+      const double cFR = cR + cgd_max(0.0, cgd_min(r, cgd_min(kR2 * r + kL2, 1.0))) * (cL - cR);
+      return 0.25 * ((aw + wCon) * cFL + (-aw + wCon) * cFR);
+    };
+    double *f = fx + (size_t)i * DoF + ID;
+    f[0] = wCon;
+    f[(LC + 1) * DoF] = upwind(Q_CTH);
+#pragma unroll
+    for (int q = 0; q < NT; ++q) f[(2 + q) * (LC + 1) * DoF] = upwind(Q_TR0 + q);
+  }
+  __syncthreads();
+
+  // ---------------- 3. one level per warp (LPW levels for N < 5) ----------------
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / DoF, ID = lane - sub * DoF;
   const int lv = L0 + warp * LPW + sub;
@@ -113,26 +170,17 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
     DJ[k] = P.D[Jn + N * k];
   }
   // own quantities
-  int g = 0;
-  double rho = 1, u = 0, v = 0, wl = 0, wh = 0, M0 = 1, M1 = 0, MC = 1, Js = 1, J0 = 0, J1 = 0, fc = 0;
-  double d110 = 0, d111 = 0, d120 = 0, d121 = 0, d210 = 0, d211 = 0, d220 = 0, d221 = 0;
-  double d11 = 0, d12 = 0, d21 = 0, d22 = 0;
+  const int li = lv - L0;                // own row of the per-level arrays
+#define OW(q) ow[((size_t)(q) * LC + li) * DoF + ID]
+  double rho = 1, u = 0, v = 0, wl = 0, wh = 0, M0 = 1, M1 = 0, MC = 1, Js = 1, J0 = 0, J1 = 0;
   double e310 = 0, e311 = 0, e320 = 0, e321 = 0, e330 = 1, e331 = 1;
-  const double *mt = mte + (size_t)ID * nz;
   if (act) {
-    g = P.glob[IF * DoF + ID];
-    d110 = mt[C_D11_0 * cs + lv]; d111 = mt[C_D11_1 * cs + lv];
-    d120 = mt[C_D12_0 * cs + lv]; d121 = mt[C_D12_1 * cs + lv];
-    d210 = mt[C_D21_0 * cs + lv]; d211 = mt[C_D21_1 * cs + lv];
-    d220 = mt[C_D22_0 * cs + lv]; d221 = mt[C_D22_1 * cs + lv];
-    J1 = mt[C_J1 * cs + lv];
-    fc = mt[C_FCOR * cs + lv];
+    J1 = OW(O_J1);
     rho = PW(Q_RHO, p0, ID); u = PW(Q_U, p0, ID); v = PW(Q_V, p0, ID); wh = PW(Q_W, p0, ID);
     e310 = PW(Q_D310, p0, ID); e311 = PW(Q_D311, p0, ID); e320 = PW(Q_D320, p0, ID);
     e321 = PW(Q_D321, p0, ID); e330 = PW(Q_D330, p0, ID); e331 = PW(Q_D331, p0, ID);
     J0 = PW(Q_J0, p0, ID);
     M0 = PW(Q_M0, p0, ID); M1 = PW(Q_M1, p0, ID);
-    d11 = d110 + d111; d12 = d120 + d121; d21 = d210 + d211; d22 = d220 + d221;
     Js = J0 + J1;
     MC = M0 + M1;
     // surface w from no normal flow (MomentumKernel.jl:35-36)
@@ -140,23 +188,28 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
   }
   const double rJs = 1.0 / Js, rMC = 1.0 / MC;
   (void)rJs; (void)rMC;
-  const size_t ob = (size_t)nz * g + lv;   // (lv, g) in the column-major state layout
+  // the horizontal metric of the own level, re-read from shared memory where used
+#define D11 (OW(O_D110) + OW(O_D111))
+#define D12 (OW(O_D120) + OW(O_D121))
+#define D21 (OW(O_D210) + OW(O_D211))
+#define D22 (OW(O_D220) + OW(O_D221))
 
   // ---- round 1: first derivatives of the DSS'd hyperviscosity cache ----
   if (act) {
-    const double *T = T1 + ob;
-    const double c1 = T[0], c2 = T[fs], c3 = T[2 * fs], c4 = T[3 * fs], c5 = T[4 * fs];
+    const double d11 = D11, d12 = D12, d21 = D21, d22 = D22;
+    const double c1 = OW(O_T1), c2 = OW(O_T1 + 1), c3 = OW(O_T1 + 2), c4 = OW(O_T1 + 3), c5 = OW(O_T1 + 4);
     SC(0, ID) = d11 * c2 - d12 * c1;       // Curl12(Cache1, Cache2)
     SC(1, ID) = d21 * c2 - d22 * c1;
     SC(2, ID) = d11 * c3 + d12 * c4;       // Contra12(Cache3, Cache4)
     SC(3, ID) = d21 * c3 + d22 * c4;
     SC(4, ID) = c5;
-    for (int q = 0; q < NT; ++q) SC(5 + q, ID) = T[(5 + q) * fs];
+    for (int q = 0; q < NT; ++q) SC(5 + q, ID) = OW(O_T1 + 5 + q);
   }
   __syncwarp();
   double b1 = 0, b2 = 0, b3 = 0, b4 = 0;
-  double e3t[MAXTR], e4t[MAXTR];
+  double e3t[NT > 0 ? NT : 1], e4t[NT > 0 ? NT : 1];
   if (act) {
+    const double d11 = D11, d12 = D12, d21 = D21, d22 = D22;
     {
       double Dxc = DI[0] * SC(4, N * Jn), Dyc = DJ[0] * SC(4, I);
       double cu = DI[0] * SC(0, N * Jn) + DJ[0] * SC(1, I);
@@ -176,8 +229,8 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
       b4 = rho * (d21 * GradDx + d22 * GradDy);
     }
 #pragma unroll
-    for (int q = 0; q < MAXTR; ++q) {
-      if (q < NT) {
+    for (int q = 0; q < NT; ++q) {
+      {
         double Dxc = DI[0] * SC(5 + q, N * Jn), Dyc = DJ[0] * SC(5 + q, I);
 #pragma unroll
         for (int k = 1; k < N; ++k) {
@@ -196,15 +249,14 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
   if (act) {
     SC(0, ID) = b1; SC(1, ID) = b2; SC(2, ID) = b3; SC(3, ID) = b4;
 #pragma unroll
-    for (int q = 0; q < MAXTR; ++q)
-      if (q < NT) { SC(4 + 2 * q, ID) = e3t[q]; SC(5 + 2 * q, ID) = e4t[q]; }
+    for (int q = 0; q < NT; ++q) { SC(4 + 2 * q, ID) = e3t[q]; SC(5 + 2 * q, ID) = e4t[q]; }
   }
   __syncwarp();
   // The element-node contributions are accumulated in the restatement's order
   // (rho: flux top, flux bottom, horizontal divergence; u, v: hyperviscosity,
   // momentum, gradient; rho*theta and tracers: hyperviscosity, flux top, flux
   // bottom, horizontal divergence) as soon as each term is available.
-  double acc_r = 0.0, acc_u = 0.0, acc_v = 0.0, acc_th = 0.0, acc_tr[MAXTR];
+  double acc_r = 0.0, acc_u = 0.0, acc_v = 0.0, acc_th = 0.0, acc_tr[NT > 0 ? NT : 1];
   if (act) {
     double WI[N], WJ[N];
 #pragma unroll
@@ -223,6 +275,7 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
       DyDiv += WJ[k] * SC(1, I + N * k);
       DivTh += WI[k] * SC(2, k + N * Jn) + WJ[k] * SC(3, I + N * k);
     }
+    const double d11 = D11, d12 = D12, d21 = D21, d22 = D22;
     const double FuC = d12 * DxCurl + d22 * DyCurl;
     const double FvC = -d11 * DxCurl - d21 * DyCurl;
     const double FuD = d11 * DxDiv + d21 * DyDiv;
@@ -231,8 +284,8 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
     acc_v += CGD_DIVM(-(-P.nuCurl * FvC + P.nuGrad * FvD));
     acc_th += CGD_DIVM(-P.nuDiv * DivTh);
 #pragma unroll
-    for (int q = 0; q < MAXTR; ++q) {
-      if (q < NT) {
+    for (int q = 0; q < NT; ++q) {
+      {
         double DivTr = WI[0] * SC(4 + 2 * q, N * Jn) + WJ[0] * SC(5 + 2 * q, I);
 #pragma unroll
         for (int k = 1; k < N; ++k) DivTr += WI[k] * SC(4 + 2 * q, k + N * Jn) + WJ[k] * SC(5 + 2 * q, I + N * k);
@@ -243,49 +296,24 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
   }
   __syncwarp();
   const bool top = act && lv < nz - 1, bot = act && lv > 0;
-  // ---- vertical fluxes of both interfaces of the level: wCon and the limited
-  // upwind fluxes (RecU4, OperatorKernel.jl:1044-1059, J-only coefficients
-  // precomputed) of the interface il between planes pl and pl+1
-  auto wcon_at = [&](int pl) {
-    const double wI = PW(Q_W, pl, ID);
-    return PW(Q_RHO, pl, ID) * (PW(Q_D311, pl, ID) * PW(Q_U, pl, ID) + PW(Q_D321, pl, ID) * PW(Q_V, pl, ID) +
-                                PW(Q_D331, pl, ID) * wI) +
-           PW(Q_RHO, pl + 1, ID) * (PW(Q_D310, pl + 1, ID) * PW(Q_U, pl + 1, ID) +
-                                    PW(Q_D320, pl + 1, ID) * PW(Q_V, pl + 1, ID) + PW(Q_D330, pl + 1, ID) * wI);
-  };
-  auto upwind = [&](int q, int il, int pl, double wCon, double kR1, double kL1, double kL2, double kR2) {
-    const int pm = il > 0 ? pl - 1 : pl, pp2 = il + 2 < nz ? pl + 2 : pl + 1;
-    const double cLL = PW(q, pm, ID), cL = PW(q, pl, ID), cR = PW(q, pl + 1, ID), cRR = PW(q, pp2, ID);
-    const double aw = fabs(wCon);
-    double r = (cL - cLL) / (cR - cL + 1.e-20);
-    const double cFL = cL + cgd_max(0.0, cgd_min(r, cgd_min(kL1 * r + kR1, 1.0))) * (cR - cL);
-    r = (cR - cRR) / (cL - cR + 1.e-20);
-    const double cFR = cR + cgd_max(0.0, cgd_min(r, cgd_min(kR2 * r + kL2, 1.0))) * (cL - cR);
-    return 0.25 * ((aw + wCon) * cFL + (-aw + wCon) * cFR);
-  };
+  // ---- vertical fluxes of the two interfaces of the level
+#define FX(k, il) fx[((size_t)(k) * (LC + 1) + (il) - (L0 - 1)) * DoF + ID]
   if (top) {
-    const double wc = wcon_at(p0);
-    const double kR1 = mt[C_RK0 * cs + lv], kL1 = mt[C_RK1 * cs + lv];
-    const double kL2 = mt[C_RK2 * cs + lv], kR2 = mt[C_RK3 * cs + lv];
-    acc_r += CGD_DIVM(-(0.5 * wc));
-    acc_th += CGD_DIVM(-upwind(Q_CTH, lv, p0, wc, kR1, kL1, kL2, kR2));
+    acc_r += CGD_DIVM(-(0.5 * FX(0, lv)));
+    acc_th += CGD_DIVM(-FX(1, lv));
 #pragma unroll
-    for (int q = 0; q < MAXTR; ++q)
-      if (q < NT) acc_tr[q] += CGD_DIVM(-upwind(Q_TR0 + q, lv, p0, wc, kR1, kL1, kL2, kR2));
+    for (int q = 0; q < NT; ++q) acc_tr[q] += CGD_DIVM(-FX(2 + q, lv));
   }
   if (bot) {
-    const double wc = wcon_at(p0 - 1);
-    const int il = lv - 1;
-    const double kR1 = mt[C_RK0 * cs + il], kL1 = mt[C_RK1 * cs + il];
-    const double kL2 = mt[C_RK2 * cs + il], kR2 = mt[C_RK3 * cs + il];
-    acc_r += CGD_DIVM(0.5 * wc);
-    acc_th += CGD_DIVM(upwind(Q_CTH, il, p0 - 1, wc, kR1, kL1, kL2, kR2));
+    acc_r += CGD_DIVM(0.5 * FX(0, lv - 1));
+    acc_th += CGD_DIVM(FX(1, lv - 1));
 #pragma unroll
-    for (int q = 0; q < MAXTR; ++q)
-      if (q < NT) acc_tr[q] += CGD_DIVM(upwind(Q_TR0 + q, il, p0 - 1, wc, kR1, kL1, kL2, kR2));
+    for (int q = 0; q < NT; ++q) acc_tr[q] += CGD_DIVM(FX(2 + q, lv - 1));
   }
   // ---- round 3: vector-invariant momentum ----
   if (act) {
+    const double d110 = OW(O_D110), d111 = OW(O_D111), d120 = OW(O_D120), d121 = OW(O_D121);
+    const double d210 = OW(O_D210), d211 = OW(O_D211), d220 = OW(O_D220), d221 = OW(O_D221);
     SC(0, ID) = -d120 * wl;  SC(1, ID) = -d121 * wh;    // tempuZ1
     SC(2, ID) = -d220 * wl;  SC(3, ID) = -d221 * wh;    // tempuZ2
     SC(4, ID) = -d110 * wl;  SC(5, ID) = -d111 * wh;    // tempvZ1
@@ -296,7 +324,14 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
     SC(11, ID) = d221 * u - d211 * v;
   }
   __syncwarp();
+  // the w denominators (rho_l M1_l + rho_l+1 M0_l+1 at the interface); the fast
+  // build multiplies by their reciprocals
   double mwhi = 0.0, mwlo = 0.0, den_hi = 1.0, den_lo = 1.0, rho1 = 0.0;
+#ifdef CGD_FAST
+#define CGD_DIVW(x, d) ((x) * (1.0 / (d)))
+#else
+#define CGD_DIVW(x, d) ((x) / (d))
+#endif
   if (act) {
     const double tu0 = e330 * v - e320 * wl, tu1 = e331 * v - e321 * wh;
     const double tv0 = e330 * u - e310 * wl, tv1 = e331 * u - e311 * wh;
@@ -351,6 +386,7 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
       FW2 += (u * FluxVZt + v * FluxUZt);
       den_hi = rho1 * PW(Q_M0, pa, ID) + rho * M1;
     }
+    const double fc = OW(O_FC);
     const double FuCor = v * fc, FvCor = -u * fc, FwCor = 0.0;
     FU += FuCor * (J0 + J1);
     FV += FvCor * (J0 + J1);
@@ -358,14 +394,15 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
     FW2 += FwCor * J1;
     acc_u += CGD_DIVM(-v * W1 - wl * V1 - v * W2 - wh * V2 + FU);
     acc_v += CGD_DIVM(u * W1 - wl * U1 + u * W2 - wh * U2 + FV);
-    if (top) mwhi = rho * (u * V2 + v * U2 + FW2) / den_hi;
-    if (bot) mwlo = rho * (u * V1 + v * U1 + FW1) / den_lo;
+    if (top) mwhi = CGD_DIVW(rho * (u * V2 + v * U2 + FW2), den_hi);
+    if (bot) mwlo = CGD_DIVW(rho * (u * V1 + v * U1 + FW1), den_lo);
   }
   __syncwarp();
   // ---- round 4: kinetic-energy and pressure gradients, flux divergences ----
   const double K1s = 0.5 * (u * u + v * v) + 0.5 * (wl * wl);   // K on the bottom node
   const double K2s = 0.5 * (u * u + v * v) + 0.5 * (wh * wh);   // K on the top node
   if (act) {
+    const double d11 = D11, d12 = D12, d21 = D21, d22 = D22;
     SC(0, ID) = K1s;
     SC(1, ID) = K2s;
     SC(2, ID) = -rho * (d11 * u + d12 * v);                // Contra12(-Rho, u, v)
@@ -394,6 +431,9 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
       DXp += DI[k] * pa[k + N * Jn];
       DYp += DJ[k] * pa[I + N * k];
     }
+    const double d110 = OW(O_D110), d111 = OW(O_D111), d120 = OW(O_D120), d121 = OW(O_D121);
+    const double d210 = OW(O_D210), d211 = OW(O_D211), d220 = OW(O_D220), d221 = OW(O_D221);
+    const double d11 = d110 + d111, d12 = d120 + d121, d21 = d210 + d211, d22 = d220 + d221;
     double GuF1 = -(d110 * DXK1 + d210 * DYK1);
     double GvF1 = -(d120 * DXK1 + d220 * DYK1);
     double GuF2 = -(d111 * DXK2 + d211 * DYK2);
@@ -436,7 +476,7 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
       GZ = 0.5 * (PW(Q_P, pa1, ID) - PW(Q_P, p0, ID));
       const double Gradw = GZ * (e331 + PW(Q_D330, pa1, ID));
       const double Gradp = -(Gradw + P.Grav * (rho * J1 + rho1 * PW(Q_J0, pa1, ID)));
-      whi = mwhi + (GwF2 + Gradp) / den_hi;
+      whi = mwhi + CGD_DIVW(GwF2 + Gradp, den_hi);
     }
     if (bot) {
       double GwF1 = 0.0;
@@ -444,7 +484,7 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
       GwF1 += -rho * GZa * e330;
       GZa = 0.5 * (K2s - K1s);
       GwF1 += -rho * GZa * e330;
-      wlo = mwlo + GwF1 / den_lo;
+      wlo = mwlo + CGD_DIVW(GwF1, den_lo);
     }
     // horizontal flux divergences
     const double *cc = &PW(Q_CTH, p0, 0);
@@ -458,8 +498,8 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
     acc_th += CGD_DIVM(DivRhoTr);
     acc_r += CGD_DIVM(DivRho);
 #pragma unroll
-    for (int q = 0; q < MAXTR; ++q) {
-      if (q < NT) {
+    for (int q = 0; q < NT; ++q) {
+      {
         const double *ct = &PW(Q_TR0 + q, p0, 0);
         double Dv = DI[0] * SC(2, N * Jn) * ct[N * Jn] + DJ[0] * SC(3, I) * ct[I];
 #pragma unroll
@@ -478,9 +518,15 @@ __global__ void __launch_bounds__(P2Cfg<N>::THREADS, 2)
   if (bot) out[(size_t)P.NV * cs - 1] = wlo;   // slot NV, one level down
   out[4 * cs] = acc_th;
 #pragma unroll
-  for (int q = 0; q < MAXTR; ++q)
-    if (q < NT) out[(5 + q) * cs] = acc_tr[q];
+  for (int q = 0; q < NT; ++q) out[(5 + q) * cs] = acc_tr[q];
 #undef CGD_DIVR
+#undef FX
+#undef CGD_DIVW
+#undef D11
+#undef D12
+#undef D21
+#undef D22
+#undef OW
 #undef SC
 #undef PW
 }
