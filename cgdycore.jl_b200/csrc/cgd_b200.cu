@@ -43,6 +43,7 @@ struct cgd_handle {
   long long *inv_off = nullptr;
   double *C = nullptr, *T1 = nullptr, *Vst = nullptr, *k1 = nullptr, *k2 = nullptr;
   double *Ubuf = nullptr, *Fbuf = nullptr, *bands = nullptr, *part = nullptr, *scal = nullptr;
+  double *jbg = nullptr;   // Jacobian bands of the current step, [8][NumG][nz-1]
   double *mmass = nullptr;
   int *flag = nullptr;
   GP gp{};
@@ -174,11 +175,11 @@ void gather(cgd_handle *h, const double *C, double *out, bool wsplit)
 template <int MODE>
 void column(cgd_handle *h, const ColArgs &a)
 {
-  size_t smem = (size_t)COL_WARPS * (h->NV + 12) * h->nz * sizeof(double);
+  size_t smem = (size_t)COL_WARPS * COL_ARR * h->nz * sizeof(double);
   static bool attr = false;
-  if (!attr) {   // up to 8 warps x (9 + 12) arrays x 64 levels
+  if (!attr) {   // up to 8 warps x 15 arrays x 64 levels
     cudaFuncSetAttribute(k_column<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         COL_WARPS * (MAXNV + 12) * 64 * (int)sizeof(double));
+                         COL_WARPS * COL_ARR * 64 * (int)sizeof(double));
     attr = true;
   }
   k_column<MODE><<<(h->NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, h->stream>>>(h->gp, a);
@@ -202,6 +203,7 @@ void enqueue_step(cgd_handle *h, double *U, double dt)
   a.fac = dt * h->rk.gamma;
   a.rk = h->rk;
   a.C = h->C;
+  a.jbg = h->jbg;
   int e = 0;
   rec(h, e++);
   for (int stage = 0; stage < 3; ++stage) {
@@ -392,6 +394,7 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
   TRY(dalloc(h, &h->Ubuf, S * NV));
   TRY(dalloc(h, &h->Fbuf, S * NV));
   TRY(dalloc(h, &h->bands, 8 * (size_t)(nz - 1) * NumG));
+  TRY(dalloc(h, &h->jbg, 8 * (size_t)(nz - 1) * NumG));
   TRY(dalloc(h, &h->part, 1024));
   TRY(dalloc(h, &h->scal, 4));
   TRY(dalloc(h, &h->mmass, S));
@@ -655,7 +658,7 @@ int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const do
       void *p = nullptr;
       CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
       CK(cudaFuncSetAttribute(k_column<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              COL_WARPS * (MAXNV + 12) * 64 * (int)sizeof(double)));
+                              COL_WARPS * COL_ARR * 64 * (int)sizeof(double)));
       g_noalloc_ptr[dev] = static_cast<double *>(p);
     }
     bands = g_noalloc_ptr[dev];
@@ -672,7 +675,7 @@ int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const do
   a.bands = bands;
   a.fac = fac;
   a.dt = fac;
-  const size_t smem = (size_t)COL_WARPS * (P.NV + 12) * P.nz * sizeof(double);
+  const size_t smem = (size_t)COL_WARPS * COL_ARR * P.nz * sizeof(double);
   k_column<3><<<(P.NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, st>>>(P, a);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(st));

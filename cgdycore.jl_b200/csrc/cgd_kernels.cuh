@@ -293,15 +293,18 @@ __global__ void __launch_bounds__(256) k_gather(const GP P, const double *__rest
 // ---------------------------------------------------------------------------
 // Column part of a Rosenbrock-W stage, fused (one warp per column, lanes over
 // levels): owner gather of the tendency, stage corrections
-// fV = F + sum_j c_ij/dt k_j, vertical acoustic Jacobian from the step's
+// fV = F + sum_j c_ij/dt k_j, the vertical acoustic Jacobian of the step's
 // initial state (JacSchurKernel!, src/DyCore/JacSchur.jl:29-75), the Schur
 // tridiagonal system (TriDiagKernel!, SchurSolveFKernel!, triSolve!,
 // SchurSolveBKernel!: src/Integration/SchurSolve.jl:1-114) and the stage
 // update of RosenbrockSchur! (src/Integration/RosenbrockSchur.jl:13-32).
-// MODE 0: stage 1 -> k1, Vst = Vn + a21 k1
+// MODE 0: stage 1 -> k1, Vst = Vn + a21 k1; the Jacobian bands are formed
+//         and kept (level fastest) for stages 2 and 3
 // MODE 1: stage 2 -> k2, Vst = (Vn + a31 k1) + a32 k2
 // MODE 2: stage 3 -> Vout = ((Vn + m1 k1) + m2 k2) + m3 k3   (Vout may alias Vn)
 // MODE 3: standalone Schur solve with stored bands: k, v updated (cgd_schur_solve)
+// Only rho, w and rho*theta enter the Schur system; every other field has
+// k = fac * fV and is finished right after its gather.
 // ---------------------------------------------------------------------------
 struct ColArgs {
   const double *C;       // contributions of phase 2 (MODE 0..2)
@@ -310,25 +313,31 @@ struct ColArgs {
   double *kout;          // MODE 0,1,3
   double *Vout;          // MODE 0,1 (stage state), 2 (new state)
   double *v;             // MODE 3: right-hand side (overwritten)
-  const double *bands;   // MODE 3: (2, nz-1, NumG) x 4
+  const double *bands;   // MODE 3: (2, nz-1, NumG) x 4, the reference layout
+  double *jbg;           // MODE 0 writes, 1-2 read: [8][NumG][nz-1] bands of the step
   double dt, fac;
   RK rk;
 };
 
 constexpr int COL_WARPS = 8;
-// per warp: fv[NV], 8 bands, tri[3], x; each nz long
+// per warp: fv of rho, w, rho*theta, 8 bands, tri[3], x; each nz long
+constexpr int COL_ARR = 15;
 
-__device__ __forceinline__ void jac_at(const GP &P, double RhoL, double RhoR, double RhoThL0, double RhoThR0,
-                                       double dzL, double dzR, double *jb)
+// dPresdRhoTh (src/Models/Equation.jl:33-36) of one level
+__device__ __forceinline__ double dpdrhoth(const GP &P, double RhoTh0)
+{
+  const double RhoTh = RhoTh0 + 0.0;
+  return P.Rd * cgd_pow(P.Rd * RhoTh / P.p0, P.kappa / (1.0 - P.kappa));
+}
+
+__device__ __forceinline__ void jac_bands(const GP &P, double RhoL, double RhoR, double RhoThL0, double RhoThR0,
+                                          double dPdThL, double dPdThR, double dzL, double dzR, double *jb)
 {
   // JacSchurKernel! (src/DyCore/JacSchur.jl:40-73); AuxG[:,:,4] == 0 for Dry
   double RhoThL = RhoThL0 + 0.0, RhoThR = RhoThR0 + 0.0;
   double RhoF = (RhoL * dzL + RhoR * dzR) / (dzL + dzR);
   jb[0] = -RhoF / dzL;             // JRhoW[1]
   jb[1] = RhoF / dzR;              // JRhoW[2]
-  double expo = P.kappa / (1.0 - P.kappa);
-  double dPdThL = P.Rd * cgd_pow(P.Rd * RhoThL / P.p0, expo);
-  double dPdThR = P.Rd * cgd_pow(P.Rd * RhoThR / P.p0, expo);
   jb[4] = -dPdThR / RhoF / (0.5 * (dzL + dzR));   // JWRhoTh[1]
   jb[5] = dPdThL / RhoF / (0.5 * (dzL + dzR));    // JWRhoTh[2]
   jb[2] = -P.Grav * dzR / RhoF / (dzL + dzR);     // JWRho[1]
@@ -336,6 +345,12 @@ __device__ __forceinline__ void jac_at(const GP &P, double RhoL, double RhoR, do
   double RhoThF = (RhoThL * dzL + RhoThR * dzR) / (dzL + dzR);
   jb[6] = -RhoThF / dzL;           // JRhoThW[1]
   jb[7] = RhoThF / dzR;            // JRhoThW[2]
+}
+
+__device__ __forceinline__ void jac_at(const GP &P, double RhoL, double RhoR, double RhoThL0, double RhoThR0,
+                                       double dzL, double dzR, double *jb)
+{
+  jac_bands(P, RhoL, RhoR, RhoThL0, RhoThR0, dpdrhoth(P, RhoThL0), dpdrhoth(P, RhoThR0), dzL, dzR, jb);
 }
 
 template <int MODE>
@@ -348,16 +363,23 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
   const int nz = P.nz, n = nz - 1, NV = P.NV, NumG = P.NumG;
   const bool valid = g < NumG;   // no early return: the block synchronises below
   const int LS = nz;                    // per-warp arrays of nz entries
-  double *sw = csm + (size_t)warp * (NV + 12) * LS;
-  double *fv = sw;                      // [NV][nz]
-  double *jb = sw + NV * LS;            // [8][nz]
+  double *sw = csm + (size_t)warp * COL_ARR * LS;
+  double *fv = sw;                      // [3][nz]: rho, w, rho*theta
+  double *jb = sw + 3 * LS;             // [8][nz]
   double *tri = jb + 8 * LS;            // [3][nz]
   double *xs = tri + 3 * LS;            // [nz]
   const size_t fs = (size_t)nz * NumG;
   const double fac = A.fac;
+  // k1, k2 of the Schur fields (rho, w, rho*theta), kept for the update
+  double s1[2][3], s2[2][3];
 
-  // 1. tendency (owner gather) + stage corrections ; bands
-  for (int l = lane; valid && l < nz; l += 32) {
+  // 1. tendency (owner gather) + stage corrections; fields outside the Schur
+  //    system finished here; bands
+#pragma unroll
+  for (int it = 0; it < 2; ++it) {
+    const int l = lane + 32 * it;
+    if (!valid || l >= nz) continue;
+    const size_t o0 = l + (size_t)nz * g;
     if (MODE <= 2) {
       const size_t fstr = (size_t)P.DoF * nz;
       double gacc[MAXNV];
@@ -365,20 +387,46 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
 #pragma unroll
       for (int f = 0; f < MAXNV; ++f) {
         if (f >= NV) break;
+        const size_t o = o0 + f * fs;
         double x = gacc[f];
-        if (MODE >= 1) x = x + A.rk.c[MODE][0] / A.dt * A.k1[l + (size_t)nz * g + f * fs];
-        if (MODE >= 2) x = x + A.rk.c[MODE][1] / A.dt * A.k2[l + (size_t)nz * g + f * fs];
-        fv[f * LS + l] = x;
+        double x1 = 0.0, x2 = 0.0;
+        if (MODE >= 1) {
+          x1 = A.k1[o];
+          x = x + A.rk.c[MODE][0] / A.dt * x1;
+        }
+        if (MODE >= 2) {
+          x2 = A.k2[o];
+          x = x + A.rk.c[MODE][1] / A.dt * x2;
+        }
+        if (f == 0 || f == 3 || f == 4) {
+          const int sf = f == 0 ? 0 : f - 2;   // 0, 1, 2
+          fv[sf * LS + l] = x;
+          s1[it][sf] = x1;
+          s2[it][sf] = x2;
+        } else {
+          const double k = fac * x;
+          const double vn = A.Vn[o];
+          if (MODE == 0) {
+            A.kout[o] = k;
+            A.Vout[o] = vn + A.rk.a[1][0] * k;
+          } else if (MODE == 1) {
+            A.kout[o] = k;
+            A.Vout[o] = vn + A.rk.a[2][0] * x1 + A.rk.a[2][1] * k;
+          } else {
+            A.Vout[o] = vn + A.rk.m[0] * x1 + A.rk.m[1] * x2 + A.rk.m[2] * k;
+          }
+        }
       }
-      if (l < n) {
-        double b[8];
-        const double *V0 = A.Vn + (size_t)nz * g;
-        jac_at(P, V0[l], V0[l + 1], V0[l + 4 * fs], V0[l + 1 + 4 * fs],
-               P.dz[l + (size_t)nz * g], P.dz[l + 1 + (size_t)nz * g], b);
-        for (int r = 0; r < 8; ++r) jb[r * LS + l] = b[r];
+      if (MODE == 0) {
+        // dPresdRhoTh once per level, shared with the interface below
+        xs[l] = dpdrhoth(P, A.Vn[o0 + 4 * fs]);
       }
     } else {
-      for (int f = 0; f < NV; ++f) fv[f * LS + l] = A.v[l + (size_t)nz * g + f * fs];
+      fv[l] = A.v[o0];
+      fv[LS + l] = A.v[o0 + 3 * fs];
+      fv[2 * LS + l] = A.v[o0 + 4 * fs];
+      for (int f = 1; f < NV; ++f)
+        if (f != 3 && f != 4) A.kout[o0 + f * fs] = fac * A.v[o0 + f * fs];
       if (l < n) {
         const size_t bs = (size_t)2 * n * NumG;
         for (int arr = 0; arr < 4; ++arr)
@@ -386,9 +434,36 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
       }
     }
   }
+  if (MODE <= 2) {
+    if (MODE == 0) __syncwarp();
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+      const int l = lane + 32 * it;
+      if (!valid || l >= n) continue;
+      double *jg = A.jbg + (size_t)g * n + l;
+      const size_t js = (size_t)NumG * n;
+      if (MODE == 0) {
+        double b[8];
+        const double *V0 = A.Vn + (size_t)nz * g;
+        jac_bands(P, V0[l], V0[l + 1], V0[l + 4 * fs], V0[l + 1 + 4 * fs], xs[l], xs[l + 1],
+                  P.dz[l + (size_t)nz * g], P.dz[l + 1 + (size_t)nz * g], b);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          jb[r * LS + l] = b[r];
+          jg[r * js] = b[r];
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) jb[r * LS + l] = jg[r * js];
+      }
+    }
+  }
   __syncwarp();
   // jb rows: 0,1 JRhoW ; 2,3 JWRho ; 4,5 JWRhoTh ; 6,7 JRhoThW  (row r = Julia index r%2+1)
 #define JB(arr, r, i) jb[((arr) * 2 + (r)) * LS + (i)]
+#define FV0(i) fv[(i)]
+#define FV3(i) fv[LS + (i)]
+#define FV4(i) fv[2 * LS + (i)]
   const double invfac = 1.0 / fac;
   const double invfac2 = invfac / fac;
   double v3new[2] = {0.0, 0.0};
@@ -405,22 +480,22 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
       else t2 = -JB(1, 1, l + 1) * JB(0, 1, l) - JB(2, 1, l + 1) * JB(3, 1, l);
       tri[l] = t0; tri[LS + l] = t1; tri[2 * LS + l] = t2;
       // SchurSolveFKernel!
-      v3new[it] = fv[3 * LS + l] / fac + JB(1, 1, l) * fv[l] + JB(1, 0, l) * fv[l + 1] +
-                  JB(2, 1, l) * fv[4 * LS + l] + JB(2, 0, l) * fv[4 * LS + l + 1];
+      v3new[it] = FV3(l) / fac + JB(1, 1, l) * FV0(l) + JB(1, 0, l) * FV0(l + 1) +
+                  JB(2, 1, l) * FV4(l) + JB(2, 0, l) * FV4(l + 1);
     }
   }
   __syncwarp();
 #pragma unroll
   for (int it = 0; it < 2; ++it)
-    if (valid && lane + 32 * it < n) fv[3 * LS + lane + 32 * it] = v3new[it];
+    if (valid && lane + 32 * it < n) FV3(lane + 32 * it) = v3new[it];
   __syncthreads();
-  // triSolve! (Thomas), b = fv[3], x = xs: the serial sweeps of the block's
+  // triSolve! (Thomas), b = FV3, x = xs: the serial sweeps of the block's
   // columns run concurrently, one per lane of the first warp
   if (threadIdx.x < COL_WARPS && g0 + (int)threadIdx.x < NumG) {
-    double *sc = csm + (size_t)threadIdx.x * (NV + 12) * LS;
-    double *b = sc + 3 * LS;
-    const double *tr = sc + (NV + 8) * LS;
-    double *x = sc + (NV + 11) * LS;
+    double *sc = csm + (size_t)threadIdx.x * COL_ARR * LS;
+    double *b = sc + LS;
+    const double *tr = sc + 11 * LS;
+    double *x = sc + 14 * LS;
     x[0] = tr[LS + 0];
     for (int i = 0; i < n - 1; ++i) {
       const double m = tr[2 * LS + i] / x[i];   // the reference's tri[3,i]/x[i], used twice
@@ -432,14 +507,14 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
   }
   __syncthreads();
   if (!valid) return;
-  // SchurSolveBKernel! and the stage update; each lane owns levels lane and
-  // lane + 32 (compile-time unrolled so nothing is kept in local memory)
+  // SchurSolveBKernel! and the stage update of rho, w, rho*theta; each lane
+  // owns levels lane and lane + 32
 #pragma unroll
   for (int it = 0; it < 2; ++it) {
     const int l = lane + 32 * it;
     if (l >= nz) continue;
     const double kw = l < n ? xs[l] : 0.0;
-    double v0 = fv[l], v4 = fv[4 * LS + l];
+    double v0 = FV0(l), v4 = FV4(l);
     if (l == 0) {
       v0 += JB(0, 0, l) * xs[l];
       v4 += JB(3, 0, l) * xs[l];
@@ -450,50 +525,41 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
       v0 += JB(0, 0, l) * xs[l] + JB(0, 1, l - 1) * xs[l - 1];
       v4 += JB(3, 0, l) * xs[l] + JB(3, 1, l - 1) * xs[l - 1];
     }
+    const size_t o0 = l + (size_t)nz * g;
     if (MODE == 3) {
       // v after SchurSolveF/B (the Thomas sweep works on a copy, as in
       // SchurSolveTriKernel!'s shared-memory vCol)
-      A.v[l + (size_t)nz * g] = v0;
-      A.v[l + (size_t)nz * g + 4 * fs] = v4;
-      if (l < n) A.v[l + (size_t)nz * g + 3 * fs] = it == 0 ? v3new[0] : v3new[1];
+      A.v[o0] = v0;
+      A.v[o0 + 4 * fs] = v4;
+      if (l < n) A.v[o0 + 3 * fs] = it == 0 ? v3new[0] : v3new[1];
     }
-    // all loads of this level first (Vout may alias Vn), then the stores
-    double kk[MAXNV], vn[MAXNV], x1[MAXNV], x2[MAXNV];
+    const double kk[3] = {fac * v0, kw, fac * v4};
 #pragma unroll
-    for (int f = 0; f < MAXNV; ++f) {
-      if (f < NV) {
-        if (f == 3) kk[f] = kw;
-        else if (f == 0) kk[f] = fac * v0;
-        else if (f == 4) kk[f] = fac * v4;
-        else kk[f] = fac * fv[f * LS + l];
-        const size_t o = l + (size_t)nz * g + f * fs;
-        if (MODE <= 2) vn[f] = A.Vn[o];
-        if (MODE >= 1 && MODE <= 2) x1[f] = A.k1[o];
-        if (MODE == 2) x2[f] = A.k2[o];
-      }
-    }
-#pragma unroll
-    for (int f = 0; f < MAXNV; ++f) {
-      if (f < NV) {
-        const size_t o = l + (size_t)nz * g + f * fs;
-        const double k = kk[f];
-        if (MODE == 0) {
-          A.kout[o] = k;
-          A.Vout[o] = vn[f] + A.rk.a[1][0] * k;
-        } else if (MODE == 1) {
-          A.kout[o] = k;
-          A.Vout[o] = vn[f] + A.rk.a[2][0] * x1[f] + A.rk.a[2][1] * k;
-        } else if (MODE == 2) {
-          // Vout may alias Vn: this lane alone reads and writes index o, and all
-          // lanes finished reading Vn for the bands before the block barrier above
-          A.Vout[o] = vn[f] + A.rk.m[0] * x1[f] + A.rk.m[1] * x2[f] + A.rk.m[2] * k;
-        } else {
-          A.kout[o] = k;
-        }
+    for (int sf = 0; sf < 3; ++sf) {
+      const int f = sf == 0 ? 0 : sf + 2;
+      const size_t o = o0 + f * fs;
+      const double k = kk[sf];
+      if (MODE == 0) {
+        const double vn = A.Vn[o];
+        A.kout[o] = k;
+        A.Vout[o] = vn + A.rk.a[1][0] * k;
+      } else if (MODE == 1) {
+        const double vn = A.Vn[o];
+        A.kout[o] = k;
+        A.Vout[o] = vn + A.rk.a[2][0] * s1[it][sf] + A.rk.a[2][1] * k;
+      } else if (MODE == 2) {
+        // Vout may alias Vn: this lane alone reads and writes index o
+        const double vn = A.Vn[o];
+        A.Vout[o] = vn + A.rk.m[0] * s1[it][sf] + A.rk.m[1] * s2[it][sf] + A.rk.m[2] * k;
+      } else {
+        A.kout[o] = k;
       }
     }
   }
 #undef JB
+#undef FV0
+#undef FV3
+#undef FV4
 }
 
 // Jacobian bands into memory (cgd_jac): one thread per (interface, column)
