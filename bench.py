@@ -231,12 +231,15 @@ def step_bytes(cfg):
 
 
 def ncu_traffic():
-    """Per-launch DRAM bytes of the phase-2 kernel from the committed ncu summary."""
+    """Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of
+    the phase-2 kernel from the committed ncu summary of the drop-in workload."""
     try:
-        d = json.load(open(os.path.join(ROOT, "profiles", "phase2_dram.json")))
-        return float(d["dram_bytes_per_launch"])
-    except (OSError, KeyError, ValueError):
-        return None
+        for line in open(os.path.join(ROOT, "profiles", "k_phase2_dropin_n30_p4_nz45.md")):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except (OSError, ValueError):
+        pass
+    return None
 
 
 # ---------------------------------------------------------------------------
