@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision sub-measurement")
+    ap.add_argument("--mixed-days", type=float, default=1.0, help="simulated days of the mixed accuracy run")
     return ap.parse_args()
 
 
@@ -261,6 +263,50 @@ def run_reference(args, cfg, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_mixed(args, cfg, rank, ranks, U0, fp64_value, torch):
+    """The mixed form on the same workload: device-resident steps/s (timed
+    like the FP64 line) and, over args.mixed_days simulated days from the same
+    initial state, the lowest-level pressure error against the FP64 path
+    and the mass drift of both."""
+    from cgd_b200 import setup
+    dm, _, mcfg = setup(member_config(cfg, rank), precision="mixed")
+    stream = torch.cuda.ExternalStream(dm.stream())
+    Ut = torch.from_numpy(np.ascontiguousarray(U0.transpose(2, 1, 0))).cuda()
+    dm.time_stepper(Ut, cfg.dt, args.warmup)
+    ranks.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    dm.time_stepper(Ut, cfg.dt, args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    t = ranks.max(e0.elapsed_time(e1) / 1e3)
+    value = aggregate(ranks.world, args.steps, t)
+    ktimes = dm.kernel_times()
+    dm.close()
+    # accuracy: the same initial state through both paths
+    nsteps = max(1, int(round(args.mixed_days * 86400.0 / cfg.dt)))
+    out = {}
+    for prec in ("fp64", "mixed"):
+        d, _, _ = setup(member_config(cfg, rank), precision=prec)
+        V = torch.from_numpy(np.ascontiguousarray(U0.transpose(2, 1, 0))).cuda()
+        m0 = d.mass_integral(V)
+        d.time_stepper(V, cfg.dt, nsteps)
+        torch.cuda.synchronize()
+        out[prec] = (np.asarray(d.fcn_prepare(V))[0].copy(), (d.mass_integral(V) - m0) / m0)
+        d.close()
+    p64, pm = out["fp64"][0], out["mixed"][0]
+    return {"value": value, "unit": UNIT, "ms_per_step": t / args.steps * 1e3, "speedup_vs_fp64": value / fp64_value,
+            "kernel_ms_last_step": {k: round(v, 4) for k, v in ktimes[:4]},
+            "accuracy": {"simulated_days": nsteps * cfg.dt / 86400.0, "steps": nsteps,
+                         "p1_rel_l2": float(np.sqrt(np.sum((pm - p64) ** 2) / np.sum(p64 ** 2))),
+                         "p1_rel_linf": float(np.abs(pm - p64).max() / np.abs(p64).max()),
+                         "mass_drift_mixed": float(out["mixed"][1]), "mass_drift_fp64": float(out["fp64"][1]),
+                         "p1": "pressure of the lowest layer (surface-pressure proxy), against the FP64 path"},
+            "form": "FP32 horizontal derivative sums on perturbations from an FP64 per-level reference "
+                    "profile; FP64 vertical terms, column Jacobian/Schur solve and reductions"}
+
+
 def run_ours(args, cfg, rank, world, local):
     import torch
     torch.cuda.set_device(local)
@@ -311,6 +357,10 @@ def run_ours(args, cfg, rank, world, local):
            "d2h_bytes_per_step": state_bytes, "steps": Ke,
            "call": "cgd_ros_step(h, host_state, dt, 1) per step (pinned host buffer)"}
 
+    mixed = None
+    if args.precision == "fp64" and not args.no_mixed:
+        mixed = run_mixed(args, cfg, rank, ranks, U0, value, torch)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -348,6 +398,7 @@ def run_ours(args, cfg, rank, world, local):
             "kernel_ms_last_step": {k: [round(x, 4) for x in v] for k, v in fam.items()},
             "kernel_share": shares,
             "e2e": e2e,
+            "mixed": mixed,
             "gpu_launches": 12 * args.steps,
             "cpu_baseline": cpu,
             "clocks": clk,

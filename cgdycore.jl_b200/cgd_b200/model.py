@@ -159,21 +159,37 @@ class Dycore:
         return list(zip(names.value.decode().split(";"), list(ms)[:n]))
 
 
+_SETUP_CACHE = {}
+
+
+def _grid_and_state(cfg):
+    """Grid and seeded initial state of a configuration, built once per
+    process (the arrays are read-only inputs of the library)."""
+    from . import grid as G
+    from . import physics as Ph
+    key = (cfg.nPanel, cfg.OrdPoly, cfg.nz, cfg.stretch, cfg.H, cfg.NumTr, cfg.Up, cfg.theta_noise,
+           cfg.seed_theta, cfg.seed_tracer)
+    if key not in _SETUP_CACHE:
+        phys = Ph.PhysParameters()
+        grid = G.init_grid_sphere(cfg.nPanel, cfg.OrdPoly, cfg.levels(), cfg.H, phys.RadEarth)
+        tl = Ph.tracer_centres(cfg.NumTr, cfg.seed_tracer) if cfg.NumTr else None
+        U = Ph.initial_state(grid, phys, cfg.NumTr, tl, cfg.Up)
+        Ph.theta_noise(U, cfg.theta_noise, cfg.seed_theta)
+        _SETUP_CACHE.clear()
+        _SETUP_CACHE[key] = (grid, U)
+    return _SETUP_CACHE[key]
+
+
 def setup(cfg_name_or_cfg, precision="fp64", check_finite=False, nz=None, nPanel=None, exact=False):
     """Grid + initial state + Dycore for a named configuration
-    (physics.CONFIGS).  Returns (dycore, U0, config)."""
-    from . import grid as G
+    (physics.CONFIGS).  Returns (dycore, U0, config); U0 is a fresh copy."""
     from . import physics as Ph
     cfg = Ph.CONFIGS[cfg_name_or_cfg] if isinstance(cfg_name_or_cfg, str) else cfg_name_or_cfg
     if nz is not None or nPanel is not None:
         import dataclasses
         cfg = dataclasses.replace(cfg, nz=nz or cfg.nz, nPanel=nPanel or cfg.nPanel)
     phys = Ph.PhysParameters()
-    z = cfg.levels()
-    grid = G.init_grid_sphere(cfg.nPanel, cfg.OrdPoly, z, cfg.H, phys.RadEarth)
-    tl = Ph.tracer_centres(cfg.NumTr, cfg.seed_tracer) if cfg.NumTr else None
-    U = Ph.initial_state(grid, phys, cfg.NumTr, tl, cfg.Up)
-    Ph.theta_noise(U, cfg.theta_noise, cfg.seed_theta)
+    grid, U = _grid_and_state(cfg)
     nu = Ph.hyperdiffusion(cfg.nPanel, cfg.OrdPoly)
     dyc = Dycore(grid, cfg.NumTr, nu, phys, precision=precision, check_finite=check_finite, exact=exact)
-    return dyc, U, cfg
+    return dyc, U.copy(order="F"), cfg

@@ -8,7 +8,6 @@
 #include "../../include/cgd_b200.h"
 #include "cgd_kernels.cuh"
 #include "cgd_phase2.cuh"
-#include "cgd_mixed.cuh"
 
 #include <cuda_runtime.h>
 #include <cmath>
@@ -58,8 +57,10 @@ struct cgd_handle {
   bool profile = false;
   bool capturing = false;
   cudaEvent_t ev[NPROF + 1] = {};
-  // mixed precision form
-  MixedState *mixed = nullptr;
+  // mixed form: FP32 horizontal derivative sums around an FP64 reference
+  // profile (the horizontal mean of the first state the handle sees)
+  bool mix = false, have_ref = false;
+  double *pref = nullptr, *thref = nullptr;
   std::string last_error;
 };
 
@@ -117,20 +118,28 @@ void launch_hv1(cgd_handle *h, const double *U, double *C)
 {
   constexpr int LT = 256 / (N * N);
   dim3 grid((h->nz + LT - 1) / LT, h->NF);   // the level tiles of one element run back to back
-  k_hypervisc1<N><<<grid, 256, 0, h->stream>>>(h->gp, U, C);
+  if (h->mix) k_hypervisc1<N, float><<<grid, 256, 0, h->stream>>>(h->gp, U, C);
+  else k_hypervisc1<N, double><<<grid, 256, 0, h->stream>>>(h->gp, U, C);
+}
+
+template <int N, int NT, typename R>
+void launch_p2r(cgd_handle *h, const double *U, const double *T1, double *C)
+{
+  using CF = P2Cfg<N, NT, R>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_phase2<N, NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
+    attr = true;
+  }
+  dim3 grid((h->nz + CF::LC - 1) / CF::LC, h->NF);
+  k_phase2<N, NT, R><<<grid, CF::THREADS, CF::SMEM, h->stream>>>(h->gp, U, T1, C);
 }
 
 template <int N, int NT>
 void launch_p2(cgd_handle *h, const double *U, const double *T1, double *C)
 {
-  using CF = P2Cfg<N, NT>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_phase2<N, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
-    attr = true;
-  }
-  dim3 grid((h->nz + CF::LC - 1) / CF::LC, h->NF);
-  k_phase2<N, NT><<<grid, CF::THREADS, CF::SMEM, h->stream>>>(h->gp, U, T1, C);
+  if (h->mix) launch_p2r<N, NT, float>(h, U, T1, C);
+  else launch_p2r<N, NT, double>(h, U, T1, C);
 }
 
 template <int N>
@@ -226,6 +235,14 @@ void enqueue_step(cgd_handle *h, double *U, double dt)
     }
     rec(h, e++);
   }
+}
+
+// Mixed form: the reference profile from the first state (before any capture).
+void ensure_ref(cgd_handle *h, const double *Ud)
+{
+  if (!h->mix || h->have_ref) return;
+  k_refprof<<<h->nz, 256, 0, h->stream>>>(h->gp, Ud, h->pref, h->thref);
+  h->have_ref = true;
 }
 
 void free_graph(cgd_handle *h)
@@ -395,6 +412,9 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
   TRY(dalloc(h, &h->Fbuf, S * NV));
   TRY(dalloc(h, &h->bands, 8 * (size_t)(nz - 1) * NumG));
   TRY(dalloc(h, &h->jbg, 8 * (size_t)(nz - 1) * NumG));
+  h->mix = cfg->precision == CGD_PREC_MIXED;
+  TRY(dalloc(h, &h->pref, nz));
+  TRY(dalloc(h, &h->thref, nz));
   TRY(dalloc(h, &h->part, 1024));
   TRY(dalloc(h, &h->scal, 4));
   TRY(dalloc(h, &h->mmass, S));
@@ -419,6 +439,7 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
   GP &P = h->gp;
   P.N = N; P.DoF = DoF; P.nz = nz; P.NF = NF; P.NumG = NumG; P.NumTr = h->NumTr; P.NV = NV; P.NC = NV + 1;
   P.met = h->met; P.M = h->M; P.dz = h->dz; P.glob = h->glob; P.inv_ptr = h->inv_ptr; P.inv_off = h->inv_off;
+  P.pref = h->pref; P.thref = h->thref;
   for (int i = 0; i < 25; ++i) { P.D[i] = 0.0; P.DW[i] = 0.0; }
   for (int i = 0; i < N * N; ++i) { P.D[i] = DS[i]; P.DW[i] = DW[i]; }
   P.Grav = cfg->Grav; P.Rd = cfg->Rd; P.p0 = cfg->p0; P.kappa = cfg->Rd / cfg->Cpd;
@@ -440,10 +461,6 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
   if (h->profile)
     for (int i = 0; i <= NPROF; ++i) cudaEventCreate(&h->ev[i]);
 
-  if (cfg->precision == CGD_PREC_MIXED) {
-    int mrc = mixed_create(h->mixed, P, h->stream, X, dz);
-    if (mrc) { cgd_destroy(h); return mrc; }
-  }
 #undef TRY
   *out = h;
   return CGD_OK;
@@ -454,7 +471,6 @@ void cgd_destroy(cgd_handle *h)
   if (!h) return;
   if (h->stream) cudaStreamSynchronize(h->stream);
   free_graph(h);
-  if (h->mixed) mixed_destroy(h->mixed);
   for (auto &b : h->bufs) cudaFree(b.p);
   for (int i = 0; i <= NPROF; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
@@ -504,6 +520,7 @@ int cgd_hypervisc_phase1(cgd_handle *h, const double *U, double *Temp1)
   if (rc) return rc;
   bool tdev = is_device_ptr(Temp1);
   double *td = tdev ? Temp1 : h->Fbuf;
+  ensure_ref(h, Ud);
   hv1(h, Ud, h->C);
   gather(h, h->C, td, false);
   if (!tdev)
@@ -514,10 +531,10 @@ int cgd_hypervisc_phase1(cgd_handle *h, const double *U, double *Temp1)
 int cgd_rhs(cgd_handle *h, const double *U, double *F)
 {
   if (!h || !U || !F) return CGD_ERR_INVALID_ARG;
-  if (h->mixed) return mixed_rhs(h->mixed, h->gp, U, F, h->Ubuf, h->Fbuf) ? CGD_ERR_CUDA : CGD_OK;
   double *Ud;
   int rc = stage_in(h, U, h->Ubuf, true, &Ud);
   if (rc) return rc;
+  ensure_ref(h, Ud);
   bool fdev = is_device_ptr(F);
   double *fd = fdev ? F : h->Fbuf;
   hv1(h, Ud, h->C);
@@ -571,10 +588,10 @@ int cgd_schur_solve(cgd_handle *h, double *k, double *v, double fac)
 int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps)
 {
   if (!h || !U || !(dt > 0) || nsteps < 0) return CGD_ERR_INVALID_ARG;
-  if (h->mixed) return mixed_ros_step(h->mixed, h->gp, U, dt, nsteps, h->Ubuf);
   double *Ud;
   int rc = stage_in(h, U, h->Ubuf, true, &Ud);
   if (rc) return rc;
+  ensure_ref(h, Ud);
   if (!h->gexec || h->graph_U != Ud || h->graph_dt != dt) {
     free_graph(h);
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));

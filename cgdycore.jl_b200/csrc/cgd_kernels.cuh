@@ -42,6 +42,21 @@
 
 namespace cgd {
 
+// Arithmetic of the horizontal derivative sums, generic in the compute type R.
+// For R = double the expressions are the reference's, unfused, in its order
+// (acc + c*x; acc + (c1*x1 + c2*x2)); for R = float (the mixed form) they are
+// fused multiply-adds.
+__device__ __forceinline__ double rsum1(double acc, double c, double x) { return acc + c * x; }
+__device__ __forceinline__ double rsum2(double acc, double c1, double x1, double c2, double x2)
+{
+  return acc + (c1 * x1 + c2 * x2);
+}
+__device__ __forceinline__ float rsum1(float acc, float c, float x) { return __fmaf_rn(c, x, acc); }
+__device__ __forceinline__ float rsum2(float acc, float c1, float x1, float c2, float x2)
+{
+  return __fmaf_rn(c1, x1, __fmaf_rn(c2, x2, acc));
+}
+
 constexpr int NCOMP = 21;
 enum {
   C_D11_0 = 0, C_D11_1, C_D12_0, C_D12_1, C_D21_0, C_D21_1, C_D22_0, C_D22_1,
@@ -64,6 +79,8 @@ struct GP {
   const int *inv_ptr;       // NumG + 1
   const long long *inv_off; // (IF*NC*DoF + ID)*nz for every contributor
   double D[25], DW[25];     // D[i + N*j] = DS[i,j]
+  const double *pref;       // mixed form: per-level FP64 reference pressure and theta
+  const double *thref;
   double Grav, Rd, p0, kappa, nuCurl, nuGrad, nuDiv;
 };
 
@@ -96,14 +113,18 @@ __device__ __forceinline__ void recu4(double cLL, double cL, double cR, double c
 // Phase 1: HyperViscKernel! + HyperViscTracerKernel!
 // (src/GPU/ViscKernel.jl:1-84,169-218).  One CTA per (element, tile of LT
 // levels); thread (node, level).  Purely horizontal: no vertical halo.
+// R is the compute type of the derivative sums: double, or float for the
+// mixed form, where theta enters as its perturbation from the level's FP64
+// reference value.
 // ---------------------------------------------------------------------------
-template <int N>
-__global__ void __launch_bounds__(256) k_hypervisc1(const GP P, const double *__restrict__ U,
+template <int N, typename R>
+__global__ void __launch_bounds__(256, 4) k_hypervisc1(const GP P, const double *__restrict__ U,
                                                     double *__restrict__ C)
 {
+  constexpr bool MIX = sizeof(R) == sizeof(float);
   constexpr int DoF = N * N;
   constexpr int LT = 256 / DoF;
-  __shared__ double s[9][LT * DoF];
+  __shared__ R s[9][LT * DoF];
   const int IF = blockIdx.y;
   const int t = threadIdx.x;
   const int lvl = t % LT, ID = t / LT;
@@ -114,101 +135,116 @@ __global__ void __launch_bounds__(256) k_hypervisc1(const GP P, const double *__
   const int si = lvl * DoF + ID, row = lvl * DoF;
   const size_t cs = (size_t)DoF * nz;
   int g = 0;
-  double d11 = 0, d12 = 0, d21 = 0, d22 = 0, Js = 1, MC = 1;
+  R d11 = 0, d12 = 0, d21 = 0, d22 = 0;
+  double JsD = 1, MCD = 1;
+  R DI[N], DJ[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    DI[k] = (R)P.D[I + N * k];
+    DJ[k] = (R)P.D[Jn + N * k];
+  }
   const double *mt = P.met + ((size_t)IF * NCOMP * DoF + ID) * nz + l;
   if (act) {
     g = P.glob[IF * DoF + ID];
-    d11 = mt[C_D11_0 * cs] + mt[C_D11_1 * cs];
-    d12 = mt[C_D12_0 * cs] + mt[C_D12_1 * cs];
-    d21 = mt[C_D21_0 * cs] + mt[C_D21_1 * cs];
-    d22 = mt[C_D22_0 * cs] + mt[C_D22_1 * cs];
-    Js = mt[C_J0 * cs] + mt[C_J1 * cs];
+    d11 = (R)(mt[C_D11_0 * cs] + mt[C_D11_1 * cs]);
+    d12 = (R)(mt[C_D12_0 * cs] + mt[C_D12_1 * cs]);
+    d21 = (R)(mt[C_D21_0 * cs] + mt[C_D21_1 * cs]);
+    d22 = (R)(mt[C_D22_0 * cs] + mt[C_D22_1 * cs]);
+    JsD = mt[C_J0 * cs] + mt[C_J1 * cs];
     const double *Ug = U + l + (size_t)nz * g;
     const size_t fs = (size_t)nz * NumG;
-    double u = Ug[1 * fs], v = Ug[2 * fs];
+    const R u = (R)Ug[1 * fs], v = (R)Ug[2 * fs];
     s[0][si] = d11 * v - d12 * u;   // Curl12
     s[1][si] = d21 * v - d22 * u;
     s[2][si] = d11 * u + d12 * v;   // Contra12
     s[3][si] = d21 * u + d22 * v;
-    s[4][si] = Ug[4 * fs] / Ug[0];
-    MC = P.M[l + (size_t)nz * g] + P.M[l + (size_t)nz * (g + (size_t)NumG)];
+    if (MIX) s[4][si] = (R)(Ug[4 * fs] / Ug[0] - P.thref[l]);
+    else s[4][si] = (R)(Ug[4 * fs] / Ug[0]);
+    MCD = P.M[l + (size_t)nz * g] + P.M[l + (size_t)nz * (g + (size_t)NumG)];
   }
-  const double rJs = 1.0 / Js, rMC = 1.0 / MC;
-  (void)rJs; (void)rMC;
+  const R Js = (R)JsD, MC = (R)MCD;
+  const R rJs = (R)(1.0 / JsD), rMC = (R)(1.0 / MCD);
+  (void)rJs; (void)rMC; (void)Js; (void)MC;
   __syncthreads();
   if (act) {
-    const double *uC = s[0] + row, *vC = s[1] + row, *uD = s[2] + row, *vD = s[3] + row, *Th = s[4] + row;
-    double Dxc = P.D[I] * Th[N * Jn];
-    double Dyc = P.D[Jn] * Th[I];
-    double cu = P.D[I] * uC[N * Jn] + P.D[Jn] * vC[I];
-    double dv = P.D[I] * uD[N * Jn] + P.D[Jn] * vD[I];
+    const R *uC = s[0] + row, *vC = s[1] + row, *uD = s[2] + row, *vD = s[3] + row, *Th = s[4] + row;
+    R Dxc = DI[0] * Th[N * Jn];
+    R Dyc = DJ[0] * Th[I];
+    R cu = DI[0] * uC[N * Jn] + DJ[0] * vC[I];
+    R dv = DI[0] * uD[N * Jn] + DJ[0] * vD[I];
 #pragma unroll
     for (int k = 1; k < N; ++k) {
-      Dxc += P.D[I + N * k] * Th[k + N * Jn];
-      Dyc += P.D[Jn + N * k] * Th[I + N * k];
-      cu += P.D[I + N * k] * uC[k + N * Jn] + P.D[Jn + N * k] * vC[I + N * k];
-      dv += P.D[I + N * k] * uD[k + N * Jn] + P.D[Jn + N * k] * vD[I + N * k];
+      Dxc = rsum1(Dxc, DI[k], Th[k + N * Jn]);
+      Dyc = rsum1(Dyc, DJ[k], Th[I + N * k]);
+      cu = rsum2(cu, DI[k], uC[k + N * Jn], DJ[k], vC[I + N * k]);
+      dv = rsum2(dv, DI[k], uD[k + N * Jn], DJ[k], vD[I + N * k]);
     }
     s[5][si] = CGD_DIVJ(cu);
     s[6][si] = CGD_DIVJ(dv);
-    double GradDx = CGD_DIVJ(d11 * Dxc + d21 * Dyc);   // Grad12 with J
-    double GradDy = CGD_DIVJ(d12 * Dxc + d22 * Dyc);
+    R GradDx = CGD_DIVJ(d11 * Dxc + d21 * Dyc);   // Grad12 with J
+    R GradDy = CGD_DIVJ(d12 * Dxc + d22 * Dyc);
     s[7][si] = d11 * GradDx + d12 * GradDy;         // Contra12
     s[8][si] = d21 * GradDx + d22 * GradDy;
   }
   __syncthreads();
   double *out = C + ((size_t)IF * P.NC * DoF + ID) * nz + l;
+  R WI[N], WJ[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    WI[k] = (R)P.DW[I + N * k];
+    WJ[k] = (R)P.DW[Jn + N * k];
+  }
   if (act) {
-    const double *Cu = s[5] + row, *Dv = s[6] + row, *Cx = s[7] + row, *Cy = s[8] + row;
-    double DxCurl = P.DW[I] * Cu[N * Jn], DyCurl = P.DW[Jn] * Cu[I];
-    double DxDiv = P.DW[I] * Dv[N * Jn], DyDiv = P.DW[Jn] * Dv[I];
-    double DivTh = P.DW[I] * Cx[N * Jn] + P.DW[Jn] * Cy[I];
+    const R *Cu = s[5] + row, *Dv = s[6] + row, *Cx = s[7] + row, *Cy = s[8] + row;
+    R DxCurl = WI[0] * Cu[N * Jn], DyCurl = WJ[0] * Cu[I];
+    R DxDiv = WI[0] * Dv[N * Jn], DyDiv = WJ[0] * Dv[I];
+    R DivTh = WI[0] * Cx[N * Jn] + WJ[0] * Cy[I];
 #pragma unroll
     for (int k = 1; k < N; ++k) {
-      DxCurl += P.DW[I + N * k] * Cu[k + N * Jn];
-      DyCurl += P.DW[Jn + N * k] * Cu[I + N * k];
-      DxDiv += P.DW[I + N * k] * Dv[k + N * Jn];
-      DyDiv += P.DW[Jn + N * k] * Dv[I + N * k];
-      DivTh += P.DW[I + N * k] * Cx[k + N * Jn] + P.DW[Jn + N * k] * Cy[I + N * k];
+      DxCurl = rsum1(DxCurl, WI[k], Cu[k + N * Jn]);
+      DyCurl = rsum1(DyCurl, WJ[k], Cu[I + N * k]);
+      DxDiv = rsum1(DxDiv, WI[k], Dv[k + N * Jn]);
+      DyDiv = rsum1(DyDiv, WJ[k], Dv[I + N * k]);
+      DivTh = rsum2(DivTh, WI[k], Cx[k + N * Jn], WJ[k], Cy[I + N * k]);
     }
-    double FuC = d12 * DxCurl + d22 * DyCurl;       // Rot12
-    double FvC = -d11 * DxCurl - d21 * DyCurl;
-    double FuD = d11 * DxDiv + d21 * DyDiv;         // Grad12
-    double FvD = d12 * DxDiv + d22 * DyDiv;
-    out[0 * cs] = CGD_DIVM(-FuC);
-    out[1 * cs] = CGD_DIVM(-FvC);
-    out[2 * cs] = CGD_DIVM(FuD);
-    out[3 * cs] = CGD_DIVM(FvD);
-    out[4 * cs] = CGD_DIVM(DivTh);
+    R FuC = d12 * DxCurl + d22 * DyCurl;       // Rot12
+    R FvC = -d11 * DxCurl - d21 * DyCurl;
+    R FuD = d11 * DxDiv + d21 * DyDiv;         // Grad12
+    R FvD = d12 * DxDiv + d22 * DyDiv;
+    out[0 * cs] = (double)CGD_DIVM(-FuC);
+    out[1 * cs] = (double)CGD_DIVM(-FvC);
+    out[2 * cs] = (double)CGD_DIVM(FuD);
+    out[3 * cs] = (double)CGD_DIVM(FvD);
+    out[4 * cs] = (double)CGD_DIVM(DivTh);
   }
   for (int iT = 0; iT < P.NumTr; ++iT) {
     if (act) {
       const size_t fs = (size_t)nz * NumG;
       const double *Ug = U + l + (size_t)nz * g;
-      s[4][si] = Ug[(5 + iT) * fs] / Ug[0];
+      s[4][si] = (R)(Ug[(5 + iT) * fs] / Ug[0]);
     }
     __syncthreads();
     if (act) {
-      const double *Tr = s[4] + row;
-      double Dxc = P.D[I] * Tr[N * Jn];
-      double Dyc = P.D[Jn] * Tr[I];
+      const R *Tr = s[4] + row;
+      R Dxc = DI[0] * Tr[N * Jn];
+      R Dyc = DJ[0] * Tr[I];
 #pragma unroll
       for (int k = 1; k < N; ++k) {
-        Dxc += P.D[I + N * k] * Tr[k + N * Jn];
-        Dyc += P.D[Jn + N * k] * Tr[I + N * k];
+        Dxc = rsum1(Dxc, DI[k], Tr[k + N * Jn]);
+        Dyc = rsum1(Dyc, DJ[k], Tr[I + N * k]);
       }
-      double GradDx = CGD_DIVJ(d11 * Dxc + d21 * Dyc);
-      double GradDy = CGD_DIVJ(d12 * Dxc + d22 * Dyc);
+      R GradDx = CGD_DIVJ(d11 * Dxc + d21 * Dyc);
+      R GradDy = CGD_DIVJ(d12 * Dxc + d22 * Dyc);
       s[7][si] = d11 * GradDx + d12 * GradDy;
       s[8][si] = d21 * GradDx + d22 * GradDy;
     }
     __syncthreads();
     if (act) {
-      const double *Cx = s[7] + row, *Cy = s[8] + row;
-      double DivTr = P.DW[I] * Cx[N * Jn] + P.DW[Jn] * Cy[I];
+      const R *Cx = s[7] + row, *Cy = s[8] + row;
+      R DivTr = WI[0] * Cx[N * Jn] + WJ[0] * Cy[I];
 #pragma unroll
-      for (int k = 1; k < N; ++k) DivTr += P.DW[I + N * k] * Cx[k + N * Jn] + P.DW[Jn + N * k] * Cy[I + N * k];
-      out[(5 + iT) * cs] = CGD_DIVM(DivTr);
+      for (int k = 1; k < N; ++k) DivTr = rsum2(DivTr, WI[k], Cx[k + N * Jn], WJ[k], Cy[I + N * k]);
+      out[(5 + iT) * cs] = (double)CGD_DIVM(DivTr);
     }
     __syncthreads();
   }
@@ -560,6 +596,37 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
 #undef FV0
 #undef FV3
 #undef FV4
+}
+
+// Mixed form: the FP64 reference profile of pressure and theta, the
+// horizontal mean of each level of a state (one CTA per level, fixed-order
+// tree reduction, so the profile is reproducible).
+__global__ void __launch_bounds__(256) k_refprof(const GP P, const double *__restrict__ U, double *__restrict__ pref,
+                                                 double *__restrict__ thref)
+{
+  __shared__ double sp[256], st[256];
+  const int l = blockIdx.x, nz = P.nz, NumG = P.NumG;
+  const size_t fs = (size_t)nz * NumG;
+  double a = 0.0, b = 0.0;
+  for (int g = threadIdx.x; g < NumG; g += blockDim.x) {
+    const double rho = U[l + (size_t)nz * g], rth = U[l + (size_t)nz * g + 4 * fs];
+    a += pressure_dry(P, rth);
+    b += rth / rho;
+  }
+  sp[threadIdx.x] = a;
+  st[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      sp[threadIdx.x] += sp[threadIdx.x + w];
+      st[threadIdx.x] += st[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    pref[l] = sp[0] / NumG;
+    thref[l] = st[0] / NumG;
+  }
 }
 
 // Jacobian bands into memory (cgd_jac): one thread per (interface, column)

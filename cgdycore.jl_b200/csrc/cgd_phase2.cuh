@@ -47,41 +47,42 @@ enum {
 constexpr int P2_WARPS = 8;
 constexpr int P2_NSCR = 12;   // scratch quantities per warp (the largest derivative round)
 
-template <int N, int NT>
+template <int N, int NT, typename R>
 struct P2Cfg {
   static constexpr int DoF = N * N;
   static constexpr int LPW = 32 / DoF;           // levels per warp
   static constexpr int LC = P2_WARPS * LPW;      // levels per CTA
-  static constexpr int R = LC + 4;               // staged planes
+  static constexpr int RP = LC + 4;              // staged planes
   static constexpr int THREADS = 32 * P2_WARPS;
-  static constexpr size_t SMEM = ((size_t)(Q_TR0 + NT) * R * DoF + (size_t)(O_T1 + 5 + NT) * LC * DoF +
-                                   (size_t)(2 + NT) * (LC + 1) * DoF + (size_t)P2_WARPS * P2_NSCR * 32) *
-                                  sizeof(double);
+  static constexpr size_t SMEM = ((size_t)(Q_TR0 + NT) * RP * DoF + (size_t)(O_T1 + 5 + NT) * LC * DoF +
+                                   (size_t)(2 + NT) * (LC + 1) * DoF) * sizeof(double) +
+                                  (size_t)P2_WARPS * P2_NSCR * 32 * sizeof(R);
 };
 
-template <int N, int NT>
-__global__ void __launch_bounds__(P2Cfg<N, NT>::THREADS, 2)
+template <int N, int NT, typename R>
+__global__ void __launch_bounds__(P2Cfg<N, NT, R>::THREADS, 2)
     k_phase2(const GP P, const double *__restrict__ U, const double *__restrict__ T1, double *__restrict__ C)
 {
-  using CF = P2Cfg<N, NT>;
-  constexpr int DoF = CF::DoF, LPW = CF::LPW, LC = CF::LC, R = CF::R;
+  using CF = P2Cfg<N, NT, R>;
+  constexpr bool MIX = sizeof(R) == sizeof(float);
+  constexpr int DoF = CF::DoF, LPW = CF::LPW, LC = CF::LC, RP = CF::RP;
   extern __shared__ double sm[];
   const int nz = P.nz, NumG = P.NumG;
   const int IF = blockIdx.y;
   const int L0 = blockIdx.x * LC;
   const size_t cs = (size_t)DoF * nz, fs = (size_t)nz * NumG;
   double *pw = sm;                                             // [Q][R][DoF]
-  double *ow = pw + (size_t)(Q_TR0 + NT) * R * DoF;             // [O][LC][DoF]
+  double *ow = pw + (size_t)(Q_TR0 + NT) * RP * DoF;             // [O][LC][DoF]
   double *fx = ow + (size_t)(O_T1 + 5 + NT) * LC * DoF;         // [2+NT][LC+1][DoF] interface fluxes
-  double *scr = fx + (size_t)(2 + NT) * (LC + 1) * DoF;         // [warp][P2_NSCR][32]
+  R *scr = (R *)(fx + (size_t)(2 + NT) * (LC + 1) * DoF);      // [warp][P2_NSCR][32]
   const double *mte = P.met + (size_t)IF * NCOMP * cs;
-#define PW(q, p, id) pw[((size_t)(q) * R + (p)) * DoF + (id)]
+#define PW(q, p, id) pw[((size_t)(q) * RP + (p)) * DoF + (id)]
 
   // ---------------- 1. stage the pointwise planes L0-2 .. L0+LC+1 ----------------
   // (level fastest: every load is a run of consecutive levels of one column
   // or one metric row) and the own levels' metric and cache
-  for (int s = threadIdx.x; s < DoF * R; s += CF::THREADS) {
-    const int ID = s / R, p = s % R;
+  for (int s = threadIdx.x; s < DoF * RP; s += CF::THREADS) {
+    const int ID = s / RP, p = s % RP;
     const int lev = L0 - 2 + p;
     if (lev < 0 || lev >= nz) continue;
     const int g = P.glob[IF * DoF + ID];
@@ -103,7 +104,7 @@ __global__ void __launch_bounds__(P2Cfg<N, NT>::THREADS, 2)
     PW(Q_RHO, p, ID) = rho;
     PW(Q_CTH, p, ID) = rth / rho;
     for (int q = 0; q < NT; ++q) PW(Q_TR0 + q, p, ID) = Ug[(5 + q) * fs] / rho;
-    if (p == 0 || p == R - 1) continue;   // the outer halo planes feed the upwind stencil only
+    if (p == 0 || p == RP - 1) continue;   // the outer halo planes feed the upwind stencil only
     PW(Q_U, p, ID) = Ug[fs];
     PW(Q_V, p, ID) = Ug[2 * fs];
     PW(Q_W, p, ID) = Ug[3 * fs];
@@ -159,15 +160,15 @@ __global__ void __launch_bounds__(P2Cfg<N, NT>::THREADS, 2)
   const bool act = sub < LPW && lv < nz;
   const int I = ID % N, Jn = ID / N;
   const int p0 = lv - (L0 - 2);          // own plane
-  double *sw = scr + (size_t)warp * P2_NSCR * 32 + sub * DoF;   // this level's scratch row base
+  R *sw = scr + (size_t)warp * P2_NSCR * 32 + sub * DoF;        // this level's scratch row base
 #define SC(q, id) sw[(q) * 32 + (id)]
 
   // derivative coefficients of this node
-  double DI[N], DJ[N];
+  R DI[N], DJ[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) {
-    DI[k] = P.D[I + N * k];
-    DJ[k] = P.D[Jn + N * k];
+    DI[k] = (R)P.D[I + N * k];
+    DJ[k] = (R)P.D[Jn + N * k];
   }
   // own quantities
   const int li = lv - L0;                // own row of the per-level arrays
@@ -196,49 +197,49 @@ __global__ void __launch_bounds__(P2Cfg<N, NT>::THREADS, 2)
 
   // ---- round 1: first derivatives of the DSS'd hyperviscosity cache ----
   if (act) {
-    const double d11 = D11, d12 = D12, d21 = D21, d22 = D22;
-    const double c1 = OW(O_T1), c2 = OW(O_T1 + 1), c3 = OW(O_T1 + 2), c4 = OW(O_T1 + 3), c5 = OW(O_T1 + 4);
+    const R d11 = (R)(D11), d12 = (R)(D12), d21 = (R)(D21), d22 = (R)(D22);
+    const R c1 = (R)OW(O_T1), c2 = (R)OW(O_T1 + 1), c3 = (R)OW(O_T1 + 2), c4 = (R)OW(O_T1 + 3), c5 = (R)OW(O_T1 + 4);
     SC(0, ID) = d11 * c2 - d12 * c1;       // Curl12(Cache1, Cache2)
     SC(1, ID) = d21 * c2 - d22 * c1;
     SC(2, ID) = d11 * c3 + d12 * c4;       // Contra12(Cache3, Cache4)
     SC(3, ID) = d21 * c3 + d22 * c4;
     SC(4, ID) = c5;
-    for (int q = 0; q < NT; ++q) SC(5 + q, ID) = OW(O_T1 + 5 + q);
+    for (int q = 0; q < NT; ++q) SC(5 + q, ID) = (R)OW(O_T1 + 5 + q);
   }
   __syncwarp();
-  double b1 = 0, b2 = 0, b3 = 0, b4 = 0;
-  double e3t[NT > 0 ? NT : 1], e4t[NT > 0 ? NT : 1];
+  R b1 = 0, b2 = 0, b3 = 0, b4 = 0;
+  R e3t[NT > 0 ? NT : 1], e4t[NT > 0 ? NT : 1];
   if (act) {
-    const double d11 = D11, d12 = D12, d21 = D21, d22 = D22;
+    const R d11 = (R)(D11), d12 = (R)(D12), d21 = (R)(D21), d22 = (R)(D22);
     {
-      double Dxc = DI[0] * SC(4, N * Jn), Dyc = DJ[0] * SC(4, I);
-      double cu = DI[0] * SC(0, N * Jn) + DJ[0] * SC(1, I);
-      double dv = DI[0] * SC(2, N * Jn) + DJ[0] * SC(3, I);
+      R Dxc = DI[0] * SC(4, N * Jn), Dyc = DJ[0] * SC(4, I);
+      R cu = DI[0] * SC(0, N * Jn) + DJ[0] * SC(1, I);
+      R dv = DI[0] * SC(2, N * Jn) + DJ[0] * SC(3, I);
 #pragma unroll
       for (int k = 1; k < N; ++k) {
-        Dxc += DI[k] * SC(4, k + N * Jn);
-        Dyc += DJ[k] * SC(4, I + N * k);
-        cu += DI[k] * SC(0, k + N * Jn) + DJ[k] * SC(1, I + N * k);
-        dv += DI[k] * SC(2, k + N * Jn) + DJ[k] * SC(3, I + N * k);
+        Dxc = rsum1(Dxc, DI[k], SC(4, k + N * Jn));
+        Dyc = rsum1(Dyc, DJ[k], SC(4, I + N * k));
+        cu = rsum2(cu, DI[k], SC(0, k + N * Jn), DJ[k], SC(1, I + N * k));
+        dv = rsum2(dv, DI[k], SC(2, k + N * Jn), DJ[k], SC(3, I + N * k));
       }
       b1 = CGD_DIVJ(cu);
       b2 = CGD_DIVJ(dv);
-      const double GradDx = CGD_DIVJ(d11 * Dxc + d21 * Dyc);
-      const double GradDy = CGD_DIVJ(d12 * Dxc + d22 * Dyc);
+      const R GradDx = CGD_DIVJ(d11 * Dxc + d21 * Dyc);
+      const R GradDy = CGD_DIVJ(d12 * Dxc + d22 * Dyc);
       b3 = rho * (d11 * GradDx + d12 * GradDy);
       b4 = rho * (d21 * GradDx + d22 * GradDy);
     }
 #pragma unroll
     for (int q = 0; q < NT; ++q) {
       {
-        double Dxc = DI[0] * SC(5 + q, N * Jn), Dyc = DJ[0] * SC(5 + q, I);
+        R Dxc = DI[0] * SC(5 + q, N * Jn), Dyc = DJ[0] * SC(5 + q, I);
 #pragma unroll
         for (int k = 1; k < N; ++k) {
-          Dxc += DI[k] * SC(5 + q, k + N * Jn);
-          Dyc += DJ[k] * SC(5 + q, I + N * k);
+          Dxc = rsum1(Dxc, DI[k], SC(5 + q, k + N * Jn));
+          Dyc = rsum1(Dyc, DJ[k], SC(5 + q, I + N * k));
         }
-        const double GradDx = CGD_DIVJ(d11 * Dxc + d21 * Dyc);
-        const double GradDy = CGD_DIVJ(d12 * Dxc + d22 * Dyc);
+        const R GradDx = CGD_DIVJ(d11 * Dxc + d21 * Dyc);
+        const R GradDy = CGD_DIVJ(d12 * Dxc + d22 * Dyc);
         e3t[q] = rho * (d11 * GradDx + d12 * GradDy);
         e4t[q] = rho * (d21 * GradDx + d22 * GradDy);
       }
@@ -258,37 +259,38 @@ __global__ void __launch_bounds__(P2Cfg<N, NT>::THREADS, 2)
   // bottom, horizontal divergence) as soon as each term is available.
   double acc_r = 0.0, acc_u = 0.0, acc_v = 0.0, acc_th = 0.0, acc_tr[NT > 0 ? NT : 1];
   if (act) {
-    double WI[N], WJ[N];
+    R WI[N], WJ[N];
 #pragma unroll
     for (int k = 0; k < N; ++k) {
-      WI[k] = P.DW[I + N * k];
-      WJ[k] = P.DW[Jn + N * k];
+      WI[k] = (R)P.DW[I + N * k];
+      WJ[k] = (R)P.DW[Jn + N * k];
     }
-    double DxCurl = WI[0] * SC(0, N * Jn), DyCurl = WJ[0] * SC(0, I);
-    double DxDiv = WI[0] * SC(1, N * Jn), DyDiv = WJ[0] * SC(1, I);
-    double DivTh = WI[0] * SC(2, N * Jn) + WJ[0] * SC(3, I);
+    R DxCurl = WI[0] * SC(0, N * Jn), DyCurl = WJ[0] * SC(0, I);
+    R DxDiv = WI[0] * SC(1, N * Jn), DyDiv = WJ[0] * SC(1, I);
+    R DivTh = WI[0] * SC(2, N * Jn) + WJ[0] * SC(3, I);
 #pragma unroll
     for (int k = 1; k < N; ++k) {
-      DxCurl += WI[k] * SC(0, k + N * Jn);
-      DyCurl += WJ[k] * SC(0, I + N * k);
-      DxDiv += WI[k] * SC(1, k + N * Jn);
-      DyDiv += WJ[k] * SC(1, I + N * k);
-      DivTh += WI[k] * SC(2, k + N * Jn) + WJ[k] * SC(3, I + N * k);
+      DxCurl = rsum1(DxCurl, WI[k], SC(0, k + N * Jn));
+      DyCurl = rsum1(DyCurl, WJ[k], SC(0, I + N * k));
+      DxDiv = rsum1(DxDiv, WI[k], SC(1, k + N * Jn));
+      DyDiv = rsum1(DyDiv, WJ[k], SC(1, I + N * k));
+      DivTh = rsum2(DivTh, WI[k], SC(2, k + N * Jn), WJ[k], SC(3, I + N * k));
     }
-    const double d11 = D11, d12 = D12, d21 = D21, d22 = D22;
-    const double FuC = d12 * DxCurl + d22 * DyCurl;
-    const double FvC = -d11 * DxCurl - d21 * DyCurl;
-    const double FuD = d11 * DxDiv + d21 * DyDiv;
-    const double FvD = d12 * DxDiv + d22 * DyDiv;
+    const R d11 = (R)(D11), d12 = (R)(D12), d21 = (R)(D21), d22 = (R)(D22);
+    const R FuC = d12 * DxCurl + d22 * DyCurl;
+    const R FvC = -d11 * DxCurl - d21 * DyCurl;
+    const R FuD = d11 * DxDiv + d21 * DyDiv;
+    const R FvD = d12 * DxDiv + d22 * DyDiv;
     acc_u += CGD_DIVM(-(-P.nuCurl * FuC + P.nuGrad * FuD));
     acc_v += CGD_DIVM(-(-P.nuCurl * FvC + P.nuGrad * FvD));
     acc_th += CGD_DIVM(-P.nuDiv * DivTh);
 #pragma unroll
     for (int q = 0; q < NT; ++q) {
       {
-        double DivTr = WI[0] * SC(4 + 2 * q, N * Jn) + WJ[0] * SC(5 + 2 * q, I);
+        R DivTr = WI[0] * SC(4 + 2 * q, N * Jn) + WJ[0] * SC(5 + 2 * q, I);
 #pragma unroll
-        for (int k = 1; k < N; ++k) DivTr += WI[k] * SC(4 + 2 * q, k + N * Jn) + WJ[k] * SC(5 + 2 * q, I + N * k);
+        for (int k = 1; k < N; ++k)
+          DivTr = rsum2(DivTr, WI[k], SC(4 + 2 * q, k + N * Jn), WJ[k], SC(5 + 2 * q, I + N * k));
         acc_tr[q] = 0.0;
         acc_tr[q] += CGD_DIVM(-P.nuDiv * DivTr);
       }
@@ -312,16 +314,17 @@ __global__ void __launch_bounds__(P2Cfg<N, NT>::THREADS, 2)
   }
   // ---- round 3: vector-invariant momentum ----
   if (act) {
-    const double d110 = OW(O_D110), d111 = OW(O_D111), d120 = OW(O_D120), d121 = OW(O_D121);
-    const double d210 = OW(O_D210), d211 = OW(O_D211), d220 = OW(O_D220), d221 = OW(O_D221);
-    SC(0, ID) = -d120 * wl;  SC(1, ID) = -d121 * wh;    // tempuZ1
-    SC(2, ID) = -d220 * wl;  SC(3, ID) = -d221 * wh;    // tempuZ2
-    SC(4, ID) = -d110 * wl;  SC(5, ID) = -d111 * wh;    // tempvZ1
-    SC(6, ID) = -d210 * wl;  SC(7, ID) = -d211 * wh;    // tempvZ2
-    SC(8, ID) = d120 * u - d110 * v;                    // tempwZ1
-    SC(9, ID) = d121 * u - d111 * v;
-    SC(10, ID) = d220 * u - d210 * v;                   // tempwZ2
-    SC(11, ID) = d221 * u - d211 * v;
+    const R d110 = (R)OW(O_D110), d111 = (R)OW(O_D111), d120 = (R)OW(O_D120), d121 = (R)OW(O_D121);
+    const R d210 = (R)OW(O_D210), d211 = (R)OW(O_D211), d220 = (R)OW(O_D220), d221 = (R)OW(O_D221);
+    const R uR = (R)u, vR = (R)v, wlR = (R)wl, whR = (R)wh;
+    SC(0, ID) = -d120 * wlR;  SC(1, ID) = -d121 * whR;    // tempuZ1
+    SC(2, ID) = -d220 * wlR;  SC(3, ID) = -d221 * whR;    // tempuZ2
+    SC(4, ID) = -d110 * wlR;  SC(5, ID) = -d111 * whR;    // tempvZ1
+    SC(6, ID) = -d210 * wlR;  SC(7, ID) = -d211 * whR;    // tempvZ2
+    SC(8, ID) = d120 * uR - d110 * vR;                    // tempwZ1
+    SC(9, ID) = d121 * uR - d111 * vR;
+    SC(10, ID) = d220 * uR - d210 * vR;                   // tempwZ2
+    SC(11, ID) = d221 * uR - d211 * vR;
   }
   __syncwarp();
   // the w denominators (rho_l M1_l + rho_l+1 M0_l+1 at the interface); the fast
@@ -336,23 +339,17 @@ __global__ void __launch_bounds__(P2Cfg<N, NT>::THREADS, 2)
     const double tu0 = e330 * v - e320 * wl, tu1 = e331 * v - e321 * wh;
     const double tv0 = e330 * u - e310 * wl, tv1 = e331 * u - e311 * wh;
     const double tw0 = e320 * u - e310 * v, tw1 = e321 * u - e311 * v;
-    double U1 = 0.5 * (tu1 - tu0), U2 = U1;
-    double V1 = 0.5 * (tv1 - tv0), V2 = V1;
-    double W1 = 0.5 * (tw1 - tw0), W2 = W1;
-    U1 += DI[0] * SC(0, N * Jn) + DJ[0] * SC(2, I);
-    U2 += DI[0] * SC(1, N * Jn) + DJ[0] * SC(3, I);
-    V1 += DI[0] * SC(4, N * Jn) + DJ[0] * SC(6, I);
-    V2 += DI[0] * SC(5, N * Jn) + DJ[0] * SC(7, I);
-    W1 += DI[0] * SC(8, N * Jn) + DJ[0] * SC(10, I);
-    W2 += DI[0] * SC(9, N * Jn) + DJ[0] * SC(11, I);
+    R U1 = (R)(0.5 * (tu1 - tu0)), U2 = U1;
+    R V1 = (R)(0.5 * (tv1 - tv0)), V2 = V1;
+    R W1 = (R)(0.5 * (tw1 - tw0)), W2 = W1;
 #pragma unroll
-    for (int k = 1; k < N; ++k) {
-      U1 += DI[k] * SC(0, k + N * Jn) + DJ[k] * SC(2, I + N * k);
-      U2 += DI[k] * SC(1, k + N * Jn) + DJ[k] * SC(3, I + N * k);
-      V1 += DI[k] * SC(4, k + N * Jn) + DJ[k] * SC(6, I + N * k);
-      V2 += DI[k] * SC(5, k + N * Jn) + DJ[k] * SC(7, I + N * k);
-      W1 += DI[k] * SC(8, k + N * Jn) + DJ[k] * SC(10, I + N * k);
-      W2 += DI[k] * SC(9, k + N * Jn) + DJ[k] * SC(11, I + N * k);
+    for (int k = 0; k < N; ++k) {
+      U1 = rsum2(U1, DI[k], SC(0, k + N * Jn), DJ[k], SC(2, I + N * k));
+      U2 = rsum2(U2, DI[k], SC(1, k + N * Jn), DJ[k], SC(3, I + N * k));
+      V1 = rsum2(V1, DI[k], SC(4, k + N * Jn), DJ[k], SC(6, I + N * k));
+      V2 = rsum2(V2, DI[k], SC(5, k + N * Jn), DJ[k], SC(7, I + N * k));
+      W1 = rsum2(W1, DI[k], SC(8, k + N * Jn), DJ[k], SC(10, I + N * k));
+      W2 = rsum2(W2, DI[k], SC(9, k + N * Jn), DJ[k], SC(11, I + N * k));
     }
     // vertical parts from the neighbour levels
     double FU = 0.0, FV = 0.0, FW1 = 0.0, FW2 = 0.0;
@@ -403,10 +400,16 @@ __global__ void __launch_bounds__(P2Cfg<N, NT>::THREADS, 2)
   const double K2s = 0.5 * (u * u + v * v) + 0.5 * (wh * wh);   // K on the top node
   if (act) {
     const double d11 = D11, d12 = D12, d21 = D21, d22 = D22;
-    SC(0, ID) = K1s;
-    SC(1, ID) = K2s;
-    SC(2, ID) = -rho * (d11 * u + d12 * v);                // Contra12(-Rho, u, v)
-    SC(3, ID) = -rho * (d21 * u + d22 * v);
+    SC(0, ID) = (R)K1s;
+    SC(1, ID) = (R)K2s;
+    SC(2, ID) = (R)(-rho * (d11 * u + d12 * v));           // Contra12(-Rho, u, v)
+    SC(3, ID) = (R)(-rho * (d21 * u + d22 * v));
+    // pressure (the mixed form: its perturbation from the level's FP64
+    // reference), theta and the tracer ratios of the own plane
+    SC(4, ID) = (R)(PW(Q_P, p0, ID) - (MIX ? P.pref[lv] : 0.0));
+    SC(5, ID) = (R)PW(Q_CTH, p0, ID);
+#pragma unroll
+    for (int q = 0; q < NT; ++q) SC(6 + q, ID) = (R)PW(Q_TR0 + q, p0, ID);
   }
   __syncwarp();
   if (!act) return;   // no warp-level synchronisation below
@@ -418,18 +421,18 @@ __global__ void __launch_bounds__(P2Cfg<N, NT>::THREADS, 2)
 #endif
   double whi = 0.0, wlo = 0.0;
   {
-    const double *pa = &PW(Q_P, p0, 0);
-    double DXp = DI[0] * pa[N * Jn], DYp = DJ[0] * pa[I];
-    double DXK1 = DI[0] * SC(0, N * Jn), DYK1 = DJ[0] * SC(0, I);
-    double DXK2 = DI[0] * SC(1, N * Jn), DYK2 = DJ[0] * SC(1, I);
+    const R *pa = &SC(4, 0);
+    R DXp = DI[0] * pa[N * Jn], DYp = DJ[0] * pa[I];
+    R DXK1 = DI[0] * SC(0, N * Jn), DYK1 = DJ[0] * SC(0, I);
+    R DXK2 = DI[0] * SC(1, N * Jn), DYK2 = DJ[0] * SC(1, I);
 #pragma unroll
     for (int k = 1; k < N; ++k) {
-      DXK1 += DI[k] * SC(0, k + N * Jn);
-      DYK1 += DJ[k] * SC(0, I + N * k);
-      DXK2 += DI[k] * SC(1, k + N * Jn);
-      DYK2 += DJ[k] * SC(1, I + N * k);
-      DXp += DI[k] * pa[k + N * Jn];
-      DYp += DJ[k] * pa[I + N * k];
+      DXK1 = rsum1(DXK1, DI[k], SC(0, k + N * Jn));
+      DYK1 = rsum1(DYK1, DJ[k], SC(0, I + N * k));
+      DXK2 = rsum1(DXK2, DI[k], SC(1, k + N * Jn));
+      DYK2 = rsum1(DYK2, DJ[k], SC(1, I + N * k));
+      DXp = rsum1(DXp, DI[k], pa[k + N * Jn]);
+      DYp = rsum1(DYp, DJ[k], pa[I + N * k]);
     }
     const double d110 = OW(O_D110), d111 = OW(O_D111), d120 = OW(O_D120), d121 = OW(O_D121);
     const double d210 = OW(O_D210), d211 = OW(O_D211), d220 = OW(O_D220), d221 = OW(O_D221);
@@ -487,24 +490,24 @@ __global__ void __launch_bounds__(P2Cfg<N, NT>::THREADS, 2)
       wlo = mwlo + CGD_DIVW(GwF1, den_lo);
     }
     // horizontal flux divergences
-    const double *cc = &PW(Q_CTH, p0, 0);
-    double DivRhoTr = DI[0] * SC(2, N * Jn) * cc[N * Jn] + DJ[0] * SC(3, I) * cc[I];
-    double DivRho = DI[0] * SC(2, N * Jn) + DJ[0] * SC(3, I);
+    const R *cc = &SC(5, 0);
+    R DivRhoTr = DI[0] * SC(2, N * Jn) * cc[N * Jn] + DJ[0] * SC(3, I) * cc[I];
+    R DivRho = DI[0] * SC(2, N * Jn) + DJ[0] * SC(3, I);
 #pragma unroll
     for (int k = 1; k < N; ++k) {
-      DivRhoTr += DI[k] * SC(2, k + N * Jn) * cc[k + N * Jn] + DJ[k] * SC(3, I + N * k) * cc[I + N * k];
-      DivRho += DI[k] * SC(2, k + N * Jn) + DJ[k] * SC(3, I + N * k);
+      DivRhoTr = rsum2(DivRhoTr, DI[k] * SC(2, k + N * Jn), cc[k + N * Jn], DJ[k] * SC(3, I + N * k), cc[I + N * k]);
+      DivRho = rsum2(DivRho, DI[k], SC(2, k + N * Jn), DJ[k], SC(3, I + N * k));
     }
     acc_th += CGD_DIVM(DivRhoTr);
     acc_r += CGD_DIVM(DivRho);
 #pragma unroll
     for (int q = 0; q < NT; ++q) {
       {
-        const double *ct = &PW(Q_TR0 + q, p0, 0);
-        double Dv = DI[0] * SC(2, N * Jn) * ct[N * Jn] + DJ[0] * SC(3, I) * ct[I];
+        const R *ct = &SC(6 + q, 0);
+        R Dv = DI[0] * SC(2, N * Jn) * ct[N * Jn] + DJ[0] * SC(3, I) * ct[I];
 #pragma unroll
         for (int k = 1; k < N; ++k)
-          Dv += DI[k] * SC(2, k + N * Jn) * ct[k + N * Jn] + DJ[k] * SC(3, I + N * k) * ct[I + N * k];
+          Dv = rsum2(Dv, DI[k] * SC(2, k + N * Jn), ct[k + N * Jn], DJ[k] * SC(3, I + N * k), ct[I + N * k]);
         acc_tr[q] += CGD_DIVM(Dv);
       }
     }

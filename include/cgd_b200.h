@@ -46,6 +46,11 @@ extern "C" {
 
 #define CGD_PREC_FP64 0             /* everything in FP64 */
 #define CGD_PREC_MIXED 1            /* FP32 perturbations, FP64 reference/column */
+/* The mixed form evaluates the horizontal derivative sums of the tendency in
+ * FP32, on pressure and theta minus an FP64 per-level reference profile (the
+ * horizontal mean of each level of the first state the handle is given);
+ * the vertical terms, the column Jacobian and Schur solve, the stage
+ * updates and the reductions stay FP64.  No counterpart in the reference. */
 
 #define CGD_FLAG_CHECK_FINITE 1     /* cgd_ros_step scans the state for NaN/Inf */
 
