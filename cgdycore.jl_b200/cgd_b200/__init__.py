@@ -6,9 +6,9 @@ Host-side modules:
   grid     cubed-sphere topology, Glob numbering, GLL element, metric, mass
   physics  physical parameters, baroclinic-wave initial state, run configs
   model    Dycore: fcn / fcn_prepare / jac / schur_solve / rosenbrock_schur /
-           time_stepper over libcgd_b200.so
+           time_stepper over libcgd_b200.so; Ensemble: batched members
   build    compiles libcgd_b200.so for sm_100a
 """
 from . import grid, physics  # noqa: F401
 from ._lib import CgdError, lib  # noqa: F401
-from .model import Dycore, setup  # noqa: F401
+from .model import Dycore, Ensemble, setup  # noqa: F401

@@ -20,12 +20,14 @@ ERRORS = {
 PREC_FP64, PREC_MIXED = 0, 1
 NOALLOC_SCRATCH_DOUBLES = 4 * 1024 * 1024
 FLAG_CHECK_FINITE = 1
+BATCH_AUTOTUNE = 1
 
 # every symbol declared in include/cgd_b200.h
 EXPORTS = [
     "cgd_create", "cgd_destroy", "cgd_prepare", "cgd_hypervisc_phase1", "cgd_rhs", "cgd_jac",
     "cgd_schur_solve", "cgd_ros_step", "cgd_mass_integral", "cgd_jac_schur_solve_noalloc", "cgd_get_stream",
     "cgd_kernel_times", "cgd_strerror", "cgd_version",
+    "cgd_batch_create", "cgd_batch_step", "cgd_batch_tuning", "cgd_batch_get_stream", "cgd_batch_destroy",
 ]
 
 
@@ -73,6 +75,16 @@ def lib(exact=False):
         L.cgd_mass_integral.restype = ctypes.c_int
         L.cgd_jac_schur_solve_noalloc.argtypes = [ctypes.POINTER(CgdConfig), vp, vp, vp, vp, dbl, vp]
         L.cgd_jac_schur_solve_noalloc.restype = ctypes.c_int
+        L.cgd_batch_create.argtypes = [vp, i32, i32, ctypes.POINTER(vp)]
+        L.cgd_batch_create.restype = ctypes.c_int
+        L.cgd_batch_step.argtypes = [vp, vp, vp, i32]
+        L.cgd_batch_step.restype = ctypes.c_int
+        L.cgd_batch_tuning.argtypes = [vp, ctypes.c_char_p, i32]
+        L.cgd_batch_tuning.restype = ctypes.c_int
+        L.cgd_batch_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.cgd_batch_get_stream.restype = ctypes.c_int
+        L.cgd_batch_destroy.argtypes = [vp]
+        L.cgd_batch_destroy.restype = None
         L.cgd_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
         L.cgd_get_stream.restype = ctypes.c_int
         L.cgd_kernel_times.argtypes = [vp, ctypes.c_char_p, i32, vp, i32]

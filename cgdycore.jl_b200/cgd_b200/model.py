@@ -159,6 +159,51 @@ class Dycore:
         return list(zip(names.value.decode().split(";"), list(ms)[:n]))
 
 
+class Ensemble:
+    """Batched ensemble of Dycore members (same OrdPoly, NumTr and precision;
+    any nPanel and nz): one ensemble step is one CUDA graph of 12 launches over
+    flat work lists spanning every member (cgd_batch_step).  States are CUDA
+    torch tensors, one per member, stepped in place."""
+
+    def __init__(self, members, autotune=False):
+        self.members = list(members)
+        self._L = self.members[0]._L
+        arr = (ctypes.c_void_p * len(self.members))(*[m.h for m in self.members])
+        b = ctypes.c_void_p()
+        _lib.check(self._L.cgd_batch_create(arr, len(self.members), _lib.BATCH_AUTOTUNE if autotune else 0,
+                                            ctypes.byref(b)), "cgd_batch_create")
+        self.b = b
+
+    def step(self, states, dts, nsteps=1):
+        n = len(self.members)
+        if len(states) != n or len(dts) != n:
+            raise ValueError("one state and one dt per member")
+        ptrs = (ctypes.c_void_p * n)(*[_ptr(u, m.shape, True) for u, m in zip(states, self.members)])
+        dt = (ctypes.c_double * n)(*[float(x) for x in dts])
+        _lib.check(self._L.cgd_batch_step(self.b, ptrs, dt, int(nsteps)), "cgd_batch_step")
+
+    def tuning(self):
+        buf = ctypes.create_string_buffer(512)
+        _lib.check(self._L.cgd_batch_tuning(self.b, buf, 512), "cgd_batch_tuning")
+        return buf.value.decode()
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        _lib.check(self._L.cgd_batch_get_stream(self.b, ctypes.byref(s)), "cgd_batch_get_stream")
+        return s.value
+
+    def close(self):
+        if getattr(self, "b", None):
+            try:
+                self._L.cgd_batch_destroy(self.b)
+            except (TypeError, AttributeError):   # interpreter shutdown
+                pass
+            self.b = None
+
+    def __del__(self):
+        self.close()
+
+
 _SETUP_CACHE = {}
 
 

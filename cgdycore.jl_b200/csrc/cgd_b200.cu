@@ -8,12 +8,15 @@
 #include "../../include/cgd_b200.h"
 #include "cgd_kernels.cuh"
 #include "cgd_phase2.cuh"
+#include "cgd_batch.cuh"
 
 #include <cuda_runtime.h>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
+#include <chrono>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -729,6 +732,328 @@ int cgd_kernel_times(cgd_handle *h, char *names, int32_t names_len, double *ms, 
     names[names_len - 1] = 0;
   }
   return n;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batched ensemble (cgd_batch_*): the members' steps as one graph of 12
+// launches over flat work lists.
+// ===========================================================================
+struct cgd_batch {
+  std::vector<cgd_handle *> mem;
+  int N = 0, NT = 0, nzmax = 0;
+  bool mix = false;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // work lists, one set per candidate order; order[ci] names it
+  static constexpr int NORD = 3;
+  WItem *w[NORD][4] = {};
+  int n[4] = {};
+  cudaGraph_t graph[NORD] = {};
+  cudaGraphExec_t gexec[NORD] = {};
+  int chosen = 0;
+  bool tuned = false, autotune = false;
+  double tune_ms[NORD] = {};
+  std::vector<GP> gps;
+  std::vector<BMember> bms;
+  std::vector<void *> scratch;
+  std::string last_error;
+};
+
+namespace {
+
+const char *const ORDER_NAME[cgd_batch::NORD] = {"member-major", "largest-member-first", "members-interleaved"};
+
+int batch_fail(cgd_batch *b, cudaError_t e, const char *what)
+{
+  char buf[256];
+  snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+  g_last_error = buf;
+  if (b) b->last_error = buf;
+  return CGD_ERR_CUDA;
+}
+#define BCK(call)                                          \
+  do {                                                     \
+    cudaError_t e_ = (call);                               \
+    if (e_ != cudaSuccess) return batch_fail(b, e_, #call); \
+  } while (0)
+
+// Work items of every kernel of a stage for every member, in one of three
+// orders: members one after the other, the largest member first, or the
+// members' items interleaved one by one.
+void batch_lists(const cgd_batch *b, int order, std::vector<WItem> out[4])
+{
+  const int nm = (int)b->mem.size();
+  std::vector<std::vector<WItem>> per[4];
+  for (int k = 0; k < 4; ++k) per[k].resize(nm);
+  const int DoF = b->N * b->N;
+  const int LT = 256 / DoF;
+  int LC = 0;
+  switch (b->N) {
+    case 2: LC = P2Cfg<2, 0, double>::LC; break;
+    case 3: LC = P2Cfg<3, 0, double>::LC; break;
+    case 4: LC = P2Cfg<4, 0, double>::LC; break;
+    default: LC = P2Cfg<5, 0, double>::LC; break;
+  }
+  for (int m = 0; m < nm; ++m) {
+    const cgd_handle *h = b->mem[m];
+    for (int IF = 0; IF < h->NF; ++IF)
+      for (int t = 0; t < (h->nz + LT - 1) / LT; ++t) per[0][m].push_back({m, t, IF});
+    const long long ncl = (long long)h->nz * h->NumG;
+    for (long long t = 0; t < (ncl + 255) / 256; ++t) per[1][m].push_back({m, (int)t, 0});
+    for (int IF = 0; IF < h->NF; ++IF)
+      for (int c = 0; c < (h->nz + LC - 1) / LC; ++c) per[2][m].push_back({m, c, IF});
+    for (int c = 0; c < (h->NumG + COL_WARPS - 1) / COL_WARPS; ++c) per[3][m].push_back({m, c, 0});
+  }
+  std::vector<int> ord(nm);
+  for (int m = 0; m < nm; ++m) ord[m] = m;
+  if (order == 1)
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int c) {
+      return (long long)b->mem[a]->NF * b->mem[a]->nz > (long long)b->mem[c]->NF * b->mem[c]->nz;
+    });
+  for (int k = 0; k < 4; ++k) {
+    out[k].clear();
+    if (order == 2) {
+      size_t mx = 0;
+      for (int m = 0; m < nm; ++m) mx = std::max(mx, per[k][m].size());
+      for (size_t i = 0; i < mx; ++i)
+        for (int m = 0; m < nm; ++m)
+          if (i < per[k][m].size()) out[k].push_back(per[k][m][i]);
+    } else {
+      for (int m : ord) out[k].insert(out[k].end(), per[k][m].begin(), per[k][m].end());
+    }
+  }
+}
+
+template <int N, int NT, typename R>
+void batch_enqueue_t(cgd_batch *b, WItem *const *w)
+{
+  using CF = P2Cfg<N, NT, R>;
+  static bool attr = false;
+  const size_t csmem = (size_t)COL_WARPS * COL_ARR * b->nzmax * sizeof(double);
+  if (!attr) {
+    cudaFuncSetAttribute(kb_phase2<N, NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
+    for (auto f : {kb_column<0>, kb_column<1>, kb_column<2>})
+      cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, COL_WARPS * COL_ARR * 64 * (int)sizeof(double));
+    attr = true;
+  }
+  for (int stage = 0; stage < 3; ++stage) {
+    kb_hypervisc1<N, R><<<b->n[0], 256, 0, b->stream>>>(w[0], stage);
+    kb_gather<<<b->n[1], 256, 0, b->stream>>>(w[1]);
+    kb_phase2<N, NT, R><<<b->n[2], CF::THREADS, CF::SMEM, b->stream>>>(w[2], stage);
+    if (stage == 0) kb_column<0><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);
+    else if (stage == 1) kb_column<1><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);
+    else kb_column<2><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);
+  }
+}
+
+template <int N, typename R>
+void batch_enqueue_n(cgd_batch *b, WItem *const *w)
+{
+  switch (b->NT) {
+    case 0: batch_enqueue_t<N, 0, R>(b, w); break;
+    case 1: batch_enqueue_t<N, 1, R>(b, w); break;
+    case 2: batch_enqueue_t<N, 2, R>(b, w); break;
+    case 3: batch_enqueue_t<N, 3, R>(b, w); break;
+    default: batch_enqueue_t<N, 4, R>(b, w); break;
+  }
+}
+
+template <typename R>
+void batch_enqueue_r(cgd_batch *b, WItem *const *w)
+{
+  switch (b->N) {
+    case 2: batch_enqueue_n<2, R>(b, w); break;
+    case 3: batch_enqueue_n<3, R>(b, w); break;
+    case 4: batch_enqueue_n<4, R>(b, w); break;
+    default: batch_enqueue_n<5, R>(b, w); break;
+  }
+}
+
+void batch_enqueue(cgd_batch *b, int order)
+{
+  if (b->mix) batch_enqueue_r<float>(b, b->w[order]);
+  else batch_enqueue_r<double>(b, b->w[order]);
+}
+
+int batch_upload(cgd_batch *b)
+{
+  const size_t nm = b->mem.size();
+  BCK(cudaMemcpyToSymbolAsync(c_bgp, b->gps.data(), nm * sizeof(GP), 0, cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaMemcpyToSymbolAsync(c_bm, b->bms.data(), nm * sizeof(BMember), 0, cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaMemcpyToSymbolAsync(c_brk, &b->mem[0]->rk, sizeof(RK), 0, cudaMemcpyHostToDevice, b->stream));
+  return CGD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cgd_batch_create(cgd_handle *const *members, int32_t nmembers, int32_t flags, cgd_batch **out)
+{
+  cgd_batch *b = nullptr;
+  if (!members || !out || nmembers < 1) return CGD_ERR_INVALID_ARG;
+  if (nmembers > BMAX) return CGD_ERR_UNSUPPORTED;
+  for (int m = 0; m < nmembers; ++m) {
+    const cgd_handle *h = members[m];
+    if (!h) return CGD_ERR_INVALID_ARG;
+    if (h->N != members[0]->N || h->NumTr != members[0]->NumTr || h->mix != members[0]->mix ||
+        h->device != members[0]->device)
+      return CGD_ERR_SHAPE;
+  }
+  b = new cgd_batch;
+  b->mem.assign(members, members + nmembers);
+  b->N = members[0]->N;
+  b->NT = members[0]->NumTr;
+  b->mix = members[0]->mix;
+  b->device = members[0]->device;
+  b->autotune = (flags & CGD_BATCH_AUTOTUNE) != 0;
+  for (auto h : b->mem) b->nzmax = std::max(b->nzmax, h->nz);
+  int rc = CGD_OK;
+  do {
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { rc = batch_fail(b, e, "cgd_batch_create stream"); break; }
+    const int nord = b->autotune ? cgd_batch::NORD : 1;
+    for (int o = 0; o < nord && !rc; ++o) {
+      std::vector<WItem> lists[4];
+      batch_lists(b, o, lists);
+      for (int k = 0; k < 4; ++k) {
+        b->n[k] = (int)lists[k].size();
+        void *p = nullptr;
+        e = cudaMalloc(&p, lists[k].size() * sizeof(WItem));
+        if (e == cudaSuccess)
+          e = cudaMemcpy(p, lists[k].data(), lists[k].size() * sizeof(WItem), cudaMemcpyHostToDevice);
+        b->w[o][k] = static_cast<WItem *>(p);
+        if (e != cudaSuccess) { rc = batch_fail(b, e, "cgd_batch_create work lists"); break; }
+      }
+    }
+  } while (false);
+  if (rc) { cgd_batch_destroy(b); return rc; }
+  b->gps.resize(nmembers);
+  b->bms.resize(nmembers);
+  for (int m = 0; m < nmembers; ++m) b->gps[m] = members[m]->gp;
+  *out = b;
+  return CGD_OK;
+}
+
+void cgd_batch_destroy(cgd_batch *b)
+{
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (int o = 0; o < cgd_batch::NORD; ++o) {
+    if (b->gexec[o]) cudaGraphExecDestroy(b->gexec[o]);
+    if (b->graph[o]) cudaGraphDestroy(b->graph[o]);
+    for (int k = 0; k < 4; ++k)
+      if (b->w[o][k]) cudaFree(b->w[o][k]);
+  }
+  for (void *p : b->scratch) cudaFree(p);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nsteps)
+{
+  if (!b || !U || !dt || nsteps < 0) return CGD_ERR_INVALID_ARG;
+  const int nm = (int)b->mem.size();
+  for (int m = 0; m < nm; ++m) {
+    if (!U[m] || !(dt[m] > 0)) return CGD_ERR_INVALID_ARG;
+    if (!is_device_ptr(U[m])) return CGD_ERR_INVALID_ARG;
+  }
+  BCK(cudaSetDevice(b->device));
+  // mixed members: the reference profile from their first state
+  for (int m = 0; m < nm; ++m) {
+    cgd_handle *h = b->mem[m];
+    if (h->mix && !h->have_ref) {
+      ensure_ref(h, U[m]);
+      BCK(cudaStreamSynchronize(h->stream));
+    }
+  }
+  auto set_members = [&](double *const *state) {
+    for (int m = 0; m < nm; ++m) {
+      const cgd_handle *h = b->mem[m];
+      b->bms[m] = BMember{state[m], h->Vst, h->k1, h->k2, h->C, h->T1, h->jbg, dt[m]};
+    }
+  };
+  const int nord = b->autotune ? cgd_batch::NORD : 1;
+  for (int o = 0; o < nord; ++o) {
+    if (b->gexec[o]) continue;
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    batch_enqueue(b, o);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph[o]);
+    if (e != cudaSuccess) return batch_fail(b, e, "cgd_batch_step capture");
+    BCK(cudaGraphInstantiate(&b->gexec[o], b->graph[o], 0));
+  }
+  if (b->autotune && !b->tuned) {
+    // each candidate order advances copies of the states by one step after one
+    // warm-up step; the fastest is kept
+    std::vector<double *> copies(nm);
+    if (b->scratch.empty()) {
+      for (int m = 0; m < nm; ++m) {
+        void *p = nullptr;
+        BCK(cudaMalloc(&p, (size_t)b->mem[m]->nz * b->mem[m]->NumG * b->mem[m]->NV * sizeof(double)));
+        b->scratch.push_back(p);
+      }
+    }
+    for (int m = 0; m < nm; ++m) copies[m] = static_cast<double *>(b->scratch[m]);
+    cudaEvent_t e0, e1;
+    BCK(cudaEventCreate(&e0));
+    BCK(cudaEventCreate(&e1));
+    for (int o = 0; o < nord; ++o) {
+      for (int m = 0; m < nm; ++m) {
+        const cgd_handle *h = b->mem[m];
+        BCK(cudaMemcpyAsync(copies[m], U[m], (size_t)h->nz * h->NumG * h->NV * sizeof(double),
+                            cudaMemcpyDeviceToDevice, b->stream));
+      }
+      set_members(copies.data());
+      int rc = batch_upload(b);
+      if (rc) return rc;
+      BCK(cudaGraphLaunch(b->gexec[o], b->stream));
+      BCK(cudaEventRecord(e0, b->stream));
+      BCK(cudaGraphLaunch(b->gexec[o], b->stream));
+      BCK(cudaEventRecord(e1, b->stream));
+      BCK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      BCK(cudaEventElapsedTime(&ms, e0, e1));
+      b->tune_ms[o] = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->chosen = 0;
+    for (int o = 1; o < nord; ++o)
+      if (b->tune_ms[o] < b->tune_ms[b->chosen]) b->chosen = o;
+    b->tuned = true;
+  }
+  set_members(U);
+  int rc = batch_upload(b);
+  if (rc) return rc;
+  for (int s = 0; s < nsteps; ++s) BCK(cudaGraphLaunch(b->gexec[b->chosen], b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  BCK(cudaGetLastError());
+  return CGD_OK;
+}
+
+int cgd_batch_tuning(cgd_batch *b, char *desc, int32_t len)
+{
+  if (!b || !desc || len < 1) return CGD_ERR_INVALID_ARG;
+  std::string s = std::string("order=") + ORDER_NAME[b->chosen];
+  if (b->tuned) {
+    char buf[64];
+    for (int o = 0; o < cgd_batch::NORD; ++o) {
+      snprintf(buf, sizeof buf, ";%s=%.3fms", ORDER_NAME[o], b->tune_ms[o]);
+      s += buf;
+    }
+  }
+  snprintf(desc, (size_t)len, "%s", s.c_str());
+  return CGD_OK;
+}
+
+int cgd_batch_get_stream(cgd_batch *b, void **stream)
+{
+  if (!b || !stream) return CGD_ERR_INVALID_ARG;
+  *stream = b->stream;
+  return CGD_OK;
 }
 
 }  // extern "C"

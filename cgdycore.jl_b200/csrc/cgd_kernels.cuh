@@ -118,18 +118,17 @@ __device__ __forceinline__ void recu4(double cLL, double cL, double cR, double c
 // reference value.
 // ---------------------------------------------------------------------------
 template <int N, typename R>
-__global__ void __launch_bounds__(256, 4) k_hypervisc1(const GP P, const double *__restrict__ U,
-                                                    double *__restrict__ C)
+__device__ __forceinline__ void hypervisc1_body(const GP &P, const double *__restrict__ U, double *__restrict__ C,
+                                                const int tile, const int IF)
 {
   constexpr bool MIX = sizeof(R) == sizeof(float);
   constexpr int DoF = N * N;
   constexpr int LT = 256 / DoF;
   __shared__ R s[9][LT * DoF];
-  const int IF = blockIdx.y;
   const int t = threadIdx.x;
   const int lvl = t % LT, ID = t / LT;
   const int I = ID % N, Jn = ID / N;
-  const int l = blockIdx.x * LT + lvl;
+  const int l = tile * LT + lvl;
   const int nz = P.nz, NumG = P.NumG;
   const bool act = (ID < DoF) && (l < nz);
   const int si = lvl * DoF + ID, row = lvl * DoF;
@@ -250,6 +249,13 @@ __global__ void __launch_bounds__(256, 4) k_hypervisc1(const GP P, const double 
   }
 }
 
+template <int N, typename R>
+__global__ void __launch_bounds__(256, 4) k_hypervisc1(const GP P, const double *__restrict__ U,
+                                                      double *__restrict__ C)
+{
+  hypervisc1_body<N, R>(P, U, C, blockIdx.x, blockIdx.y);
+}
+
 // Sum the contributions of the element nodes sharing global DOF g at level l
 // (ascending element, node order) for every field.  Up to four contributors
 // (every cubed-sphere node) are loaded with independent loads.  WSPLIT (the
@@ -311,10 +317,9 @@ __device__ __forceinline__ void gather_node(const GP &P, const double *__restric
 // (element, node) order.  Thread per (g, l), level fastest.
 // ---------------------------------------------------------------------------
 template <bool WSPLIT>
-__global__ void __launch_bounds__(256) k_gather(const GP P, const double *__restrict__ C,
-                                                double *__restrict__ out)
+__device__ __forceinline__ void gather_body(const GP &P, const double *__restrict__ C, double *__restrict__ out,
+                                            const long long tid)
 {
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int nz = P.nz;
   if (tid >= (long long)nz * P.NumG) return;
   const int g = (int)(tid / nz), l = (int)(tid % nz);
@@ -324,6 +329,13 @@ __global__ void __launch_bounds__(256) k_gather(const GP P, const double *__rest
 #pragma unroll
   for (int f = 0; f < MAXNV; ++f)
     if (f < P.NV) out[l + (size_t)nz * (g + (size_t)P.NumG * f)] = acc[f];
+}
+
+template <bool WSPLIT>
+__global__ void __launch_bounds__(256) k_gather(const GP P, const double *__restrict__ C,
+                                                double *__restrict__ out)
+{
+  gather_body<WSPLIT>(P, C, out, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -390,11 +402,11 @@ __device__ __forceinline__ void jac_at(const GP &P, double RhoL, double RhoR, do
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const ColArgs A)
+__device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const int bx)
 {
   extern __shared__ double csm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g0 = blockIdx.x * COL_WARPS;
+  const int g0 = bx * COL_WARPS;
   const int g = g0 + warp;
   const int nz = P.nz, n = nz - 1, NV = P.NV, NumG = P.NumG;
   const bool valid = g < NumG;   // no early return: the block synchronises below
@@ -596,6 +608,12 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column(const GP P, const Col
 #undef FV0
 #undef FV3
 #undef FV4
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(32 * COL_WARPS, 3) k_column(const GP P, const ColArgs A)
+{
+  column_body<MODE>(P, A, blockIdx.x);
 }
 
 // Mixed form: the FP64 reference profile of pressure and theta, the

@@ -60,16 +60,15 @@ struct P2Cfg {
 };
 
 template <int N, int NT, typename R>
-__global__ void __launch_bounds__(P2Cfg<N, NT, R>::THREADS, 2)
-    k_phase2(const GP P, const double *__restrict__ U, const double *__restrict__ T1, double *__restrict__ C)
+__device__ __forceinline__ void phase2_body(const GP &P, const double *__restrict__ U, const double *__restrict__ T1,
+                                            double *__restrict__ C, const int chunk, const int IF)
 {
   using CF = P2Cfg<N, NT, R>;
   constexpr bool MIX = sizeof(R) == sizeof(float);
   constexpr int DoF = CF::DoF, LPW = CF::LPW, LC = CF::LC, RP = CF::RP;
   extern __shared__ double sm[];
   const int nz = P.nz, NumG = P.NumG;
-  const int IF = blockIdx.y;
-  const int L0 = blockIdx.x * LC;
+  const int L0 = chunk * LC;
   const size_t cs = (size_t)DoF * nz, fs = (size_t)nz * NumG;
   double *pw = sm;                                             // [Q][R][DoF]
   double *ow = pw + (size_t)(Q_TR0 + NT) * RP * DoF;             // [O][LC][DoF]
@@ -532,6 +531,13 @@ __global__ void __launch_bounds__(P2Cfg<N, NT, R>::THREADS, 2)
 #undef OW
 #undef SC
 #undef PW
+}
+
+template <int N, int NT, typename R>
+__global__ void __launch_bounds__(P2Cfg<N, NT, R>::THREADS, 2)
+    k_phase2(const GP P, const double *__restrict__ U, const double *__restrict__ T1, double *__restrict__ C)
+{
+  phase2_body<N, NT, R>(P, U, T1, C, blockIdx.x, blockIdx.y);
 }
 
 }  // namespace cgd

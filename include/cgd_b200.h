@@ -140,6 +140,28 @@ int cgd_mass_integral(cgd_handle *h, const double *U, const double *MMass, doubl
 int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const double *dz,
                                 double *k, double *v, double fac, void *stream);
 
+/* Batched ensemble.  Members are handles that share OrdPoly, NumTr, the
+ * precision and the device; their grids (nPanel, nz) may differ.  One
+ * ensemble step advances every member by one Rosenbrock-W step of its own
+ * dt, as one CUDA graph of 12 launches over flat work lists spanning all
+ * members (the kernels of one stage read each member's parameters from
+ * constant memory).  Calls on different batches must not run concurrently:
+ * they share those constant tables.  The member handles must stay alive and
+ * must not be stepped on their own while their batch steps.
+ * With CGD_BATCH_AUTOTUNE the first cgd_batch_step times the candidate
+ * work-list orders (member-major, largest member first, interleaved) on
+ * copies of the states and keeps the fastest; cgd_batch_tuning reports it.
+ * No counterpart in the reference, which runs one configuration per job. */
+#define CGD_BATCH_AUTOTUNE 1
+typedef struct cgd_batch cgd_batch;
+int cgd_batch_create(cgd_handle *const *members, int32_t nmembers, int32_t flags, cgd_batch **out);
+/* U[m] device pointers, dt[m] step sizes; nsteps ensemble steps, in place. */
+int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nsteps);
+/* The chosen work-list order and the timed candidates ("order=...;...=..ms"). */
+int cgd_batch_tuning(cgd_batch *b, char *desc, int32_t len);
+int cgd_batch_get_stream(cgd_batch *b, void **stream);
+void cgd_batch_destroy(cgd_batch *b);
+
 /* The handle's CUDA stream (cudaStream_t) so a caller can order its own
  * work or timing events with the library's.  No counterpart in the
  * reference (KernelAbstractions owns its queue). */
