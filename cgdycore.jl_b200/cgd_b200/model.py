@@ -150,7 +150,7 @@ class Dycore:
         _lib.check(self._L.cgd_get_stream(self.h, ctypes.byref(s)), "cgd_get_stream")
         return s.value or 0
 
-    def kernel_times(self, nmax=12):
+    def kernel_times(self, nmax=15):
         names = ctypes.create_string_buffer(512)
         ms = (ctypes.c_double * nmax)()
         n = self._L.cgd_kernel_times(self.h, names, 512, ms, nmax)
@@ -161,7 +161,7 @@ class Dycore:
 
 class Ensemble:
     """Batched ensemble of Dycore members (same OrdPoly, NumTr and precision;
-    any nPanel and nz): one ensemble step is one CUDA graph of 12 launches over
+    any nPanel and nz): one ensemble step is one CUDA graph of 15 launches over
     flat work lists spanning every member (cgd_batch_step).  States are CUDA
     torch tensors, one per member, stepped in place."""
 

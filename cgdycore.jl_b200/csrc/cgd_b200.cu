@@ -25,7 +25,7 @@ using namespace cgd;
 
 namespace {
 
-constexpr int NPROF = 12;   // kernels per step whose durations are recorded
+constexpr int NPROF = 15;   // kernels per step whose durations are recorded
 
 struct Buf {
   void *p = nullptr;
@@ -46,6 +46,7 @@ struct cgd_handle {
   double *C = nullptr, *T1 = nullptr, *Vst = nullptr, *k1 = nullptr, *k2 = nullptr;
   double *Ubuf = nullptr, *Fbuf = nullptr, *bands = nullptr, *part = nullptr, *scal = nullptr;
   double *jbg = nullptr;   // Jacobian bands of the current step, [8][NumG][nz-1]
+  double *pres = nullptr, *pres_st = nullptr;   // pressure of the state and of the stage state
   double *mmass = nullptr;
   int *flag = nullptr;
   GP gp{};
@@ -126,7 +127,7 @@ void launch_hv1(cgd_handle *h, const double *U, double *C)
 }
 
 template <int N, int NT, typename R>
-void launch_p2r(cgd_handle *h, const double *U, const double *T1, double *C)
+void launch_p2r(cgd_handle *h, const double *U, const double *Pr, const double *T1, double *C)
 {
   using CF = P2Cfg<N, NT, R>;
   static bool attr = false;
@@ -135,25 +136,25 @@ void launch_p2r(cgd_handle *h, const double *U, const double *T1, double *C)
     attr = true;
   }
   dim3 grid((h->nz + CF::LC - 1) / CF::LC, h->NF);
-  k_phase2<N, NT, R><<<grid, CF::THREADS, CF::SMEM, h->stream>>>(h->gp, U, T1, C);
+  k_phase2<N, NT, R><<<grid, CF::THREADS, CF::SMEM, h->stream>>>(h->gp, U, Pr, T1, C);
 }
 
 template <int N, int NT>
-void launch_p2(cgd_handle *h, const double *U, const double *T1, double *C)
+void launch_p2(cgd_handle *h, const double *U, const double *Pr, const double *T1, double *C)
 {
-  if (h->mix) launch_p2r<N, NT, float>(h, U, T1, C);
-  else launch_p2r<N, NT, double>(h, U, T1, C);
+  if (h->mix) launch_p2r<N, NT, float>(h, U, Pr, T1, C);
+  else launch_p2r<N, NT, double>(h, U, Pr, T1, C);
 }
 
 template <int N>
-void launch_p2(cgd_handle *h, const double *U, const double *T1, double *C)
+void launch_p2(cgd_handle *h, const double *U, const double *Pr, const double *T1, double *C)
 {
   switch (h->NumTr) {
-    case 0: launch_p2<N, 0>(h, U, T1, C); break;
-    case 1: launch_p2<N, 1>(h, U, T1, C); break;
-    case 2: launch_p2<N, 2>(h, U, T1, C); break;
-    case 3: launch_p2<N, 3>(h, U, T1, C); break;
-    default: launch_p2<N, 4>(h, U, T1, C); break;
+    case 0: launch_p2<N, 0>(h, U, Pr, T1, C); break;
+    case 1: launch_p2<N, 1>(h, U, Pr, T1, C); break;
+    case 2: launch_p2<N, 2>(h, U, Pr, T1, C); break;
+    case 3: launch_p2<N, 3>(h, U, Pr, T1, C); break;
+    default: launch_p2<N, 4>(h, U, Pr, T1, C); break;
   }
 }
 
@@ -167,14 +168,20 @@ void hv1(cgd_handle *h, const double *U, double *C)
   }
 }
 
-void phase2(cgd_handle *h, const double *U, const double *T1, double *C)
+void phase2(cgd_handle *h, const double *U, const double *Pr, const double *T1, double *C)
 {
   switch (h->N) {
-    case 2: launch_p2<2>(h, U, T1, C); break;
-    case 3: launch_p2<3>(h, U, T1, C); break;
-    case 4: launch_p2<4>(h, U, T1, C); break;
-    default: launch_p2<5>(h, U, T1, C); break;
+    case 2: launch_p2<2>(h, U, Pr, T1, C); break;
+    case 3: launch_p2<3>(h, U, Pr, T1, C); break;
+    case 4: launch_p2<4>(h, U, Pr, T1, C); break;
+    default: launch_p2<5>(h, U, Pr, T1, C); break;
   }
+}
+
+void pressure(cgd_handle *h, const double *U, double *p)
+{
+  const long long n = (long long)h->nz * h->NumG;
+  k_pressure<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->gp, U, p);
 }
 
 void gather(cgd_handle *h, const double *C, double *out, bool wsplit)
@@ -218,20 +225,26 @@ void enqueue_step(cgd_handle *h, double *U, double dt)
   a.jbg = h->jbg;
   int e = 0;
   rec(h, e++);
+  pressure(h, U, h->pres);
+  rec(h, e++);
   for (int stage = 0; stage < 3; ++stage) {
     const double *Vsrc = stage == 0 ? U : h->Vst;
     hv1(h, Vsrc, h->C);
     rec(h, e++);
     gather(h, h->C, h->T1, false);
     rec(h, e++);
-    phase2(h, Vsrc, h->T1, h->C);
+    phase2(h, Vsrc, stage == 0 ? h->pres : h->pres_st, h->T1, h->C);
     rec(h, e++);
     if (stage == 0) {
       a.kout = h->k1; a.Vout = h->Vst;
       column<0>(h, a);
+      rec(h, e++);
+      pressure(h, h->Vst, h->pres_st);
     } else if (stage == 1) {
       a.kout = h->k2; a.Vout = h->Vst;
       column<1>(h, a);
+      rec(h, e++);
+      pressure(h, h->Vst, h->pres_st);
     } else {
       a.kout = nullptr; a.Vout = U;
       column<2>(h, a);
@@ -415,6 +428,8 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
   TRY(dalloc(h, &h->Fbuf, S * NV));
   TRY(dalloc(h, &h->bands, 8 * (size_t)(nz - 1) * NumG));
   TRY(dalloc(h, &h->jbg, 8 * (size_t)(nz - 1) * NumG));
+  TRY(dalloc(h, &h->pres, S));
+  TRY(dalloc(h, &h->pres_st, S));
   h->mix = cfg->precision == CGD_PREC_MIXED;
   TRY(dalloc(h, &h->pref, nz));
   TRY(dalloc(h, &h->thref, nz));
@@ -542,7 +557,8 @@ int cgd_rhs(cgd_handle *h, const double *U, double *F)
   double *fd = fdev ? F : h->Fbuf;
   hv1(h, Ud, h->C);
   gather(h, h->C, h->T1, false);
-  phase2(h, Ud, h->T1, h->C);
+  pressure(h, Ud, h->pres);
+  phase2(h, Ud, h->pres, h->T1, h->C);
   gather(h, h->C, fd, true);
   if (!fdev) CK(cudaMemcpyAsync(F, fd, (size_t)h->nz * h->NumG * h->NV * 8, cudaMemcpyDeviceToHost, h->stream));
   return finish(h);
@@ -713,8 +729,9 @@ int cgd_kernel_times(cgd_handle *h, char *names, int32_t names_len, double *ms, 
 {
   if (!h || !ms) return CGD_ERR_INVALID_ARG;
   if (!h->profile) return CGD_ERR_UNSUPPORTED;
-  static const char *nm[NPROF] = {"hypervisc1", "gather", "phase2", "column", "hypervisc1", "gather",
-                                  "phase2", "column", "hypervisc1", "gather", "phase2", "column"};
+  static const char *nm[NPROF] = {"pressure", "hypervisc1", "gather", "phase2", "column", "pressure",
+                                  "hypervisc1", "gather", "phase2", "column", "pressure",
+                                  "hypervisc1", "gather", "phase2", "column"};
   std::string all;
   int n = nmax < NPROF ? nmax : NPROF;
   for (int i = 0; i < n; ++i) {
@@ -737,7 +754,7 @@ int cgd_kernel_times(cgd_handle *h, char *names, int32_t names_len, double *ms, 
 }  // extern "C"
 
 // ===========================================================================
-// Batched ensemble (cgd_batch_*): the members' steps as one graph of 12
+// Batched ensemble (cgd_batch_*): the members' steps as one graph of 15
 // launches over flat work lists.
 // ===========================================================================
 struct cgd_batch {
@@ -838,6 +855,7 @@ void batch_enqueue_t(cgd_batch *b, WItem *const *w)
       cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, COL_WARPS * COL_ARR * 64 * (int)sizeof(double));
     attr = true;
   }
+  kb_pressure<<<b->n[1], 256, 0, b->stream>>>(w[1], 0);
   for (int stage = 0; stage < 3; ++stage) {
     kb_hypervisc1<N, R><<<b->n[0], 256, 0, b->stream>>>(w[0], stage);
     kb_gather<<<b->n[1], 256, 0, b->stream>>>(w[1]);
@@ -845,6 +863,7 @@ void batch_enqueue_t(cgd_batch *b, WItem *const *w)
     if (stage == 0) kb_column<0><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);
     else if (stage == 1) kb_column<1><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);
     else kb_column<2><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);
+    if (stage < 2) kb_pressure<<<b->n[1], 256, 0, b->stream>>>(w[1], 1);
   }
 }
 
@@ -973,7 +992,7 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
   auto set_members = [&](double *const *state) {
     for (int m = 0; m < nm; ++m) {
       const cgd_handle *h = b->mem[m];
-      b->bms[m] = BMember{state[m], h->Vst, h->k1, h->k2, h->C, h->T1, h->jbg, dt[m]};
+      b->bms[m] = BMember{state[m], h->Vst, h->k1, h->k2, h->C, h->T1, h->jbg, h->pres, h->pres_st, dt[m]};
     }
   };
   const int nord = b->autotune ? cgd_batch::NORD : 1;

@@ -6,7 +6,7 @@
 // A work item is (member, block x, block y) of the member's own launch grid;
 // the kernel bodies are the single-member ones, given the member's
 // parameters from constant memory.  One ensemble step is one CUDA graph of
-// 12 launches, whatever the number of members.
+// 15 launches, whatever the number of members.
 #pragma once
 #include "cgd_phase2.cuh"
 
@@ -17,6 +17,7 @@ constexpr int BMAX = 64;   // members of one ensemble
 struct BMember {
   double *U;                     // the member's state (device), updated in place
   double *Vst, *k1, *k2, *C, *T1, *jbg;
+  double *P0, *Pst;              // pressure of the state and of the stage state
   double dt;
 };
 
@@ -36,6 +37,14 @@ __global__ void __launch_bounds__(256, 4) kb_hypervisc1(const WItem *__restrict_
   hypervisc1_body<N, R>(c_bgp[it.m], stage == 0 ? B.U : B.Vst, B.C, it.x, it.y);
 }
 
+__global__ void __launch_bounds__(256) kb_pressure(const WItem *__restrict__ w, const int stage_state)
+{
+  const WItem it = w[blockIdx.x];
+  const BMember &B = c_bm[it.m];
+  pressure_body(c_bgp[it.m], stage_state ? B.Vst : B.U, stage_state ? B.Pst : B.P0,
+                (long long)it.x * blockDim.x + threadIdx.x);
+}
+
 __global__ void __launch_bounds__(256) kb_gather(const WItem *__restrict__ w)
 {
   const WItem it = w[blockIdx.x];
@@ -44,15 +53,15 @@ __global__ void __launch_bounds__(256) kb_gather(const WItem *__restrict__ w)
 }
 
 template <int N, int NT, typename R>
-__global__ void __launch_bounds__(P2Cfg<N, NT, R>::THREADS, 2) kb_phase2(const WItem *__restrict__ w, const int stage)
+__global__ void __launch_bounds__(P2Cfg<N, NT, R>::THREADS, P2Cfg<N, NT, R>::MINB) kb_phase2(const WItem *__restrict__ w, const int stage)
 {
   const WItem it = w[blockIdx.x];
   const BMember &B = c_bm[it.m];
-  phase2_body<N, NT, R>(c_bgp[it.m], stage == 0 ? B.U : B.Vst, B.T1, B.C, it.x, it.y);
+  phase2_body<N, NT, R>(c_bgp[it.m], stage == 0 ? B.U : B.Vst, stage == 0 ? B.P0 : B.Pst, B.T1, B.C, it.x, it.y);
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(32 * COL_WARPS, 3) kb_column(const WItem *__restrict__ w)
+__global__ void __launch_bounds__(32 * COL_WARPS, MODE == 2 ? 3 : 4) kb_column(const WItem *__restrict__ w)
 {
   const WItem it = w[blockIdx.x];
   const BMember &B = c_bm[it.m];

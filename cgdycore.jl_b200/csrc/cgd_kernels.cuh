@@ -611,7 +611,7 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(32 * COL_WARPS, 3) k_column(const GP P, const ColArgs A)
+__global__ void __launch_bounds__(32 * COL_WARPS, MODE == 2 ? 3 : 4) k_column(const GP P, const ColArgs A)
 {
   column_body<MODE>(P, A, blockIdx.x);
 }
@@ -665,12 +665,17 @@ __global__ void k_jac(const GP P, const double *__restrict__ U, double *__restri
     for (int r = 0; r < 2; ++r) bands[arr * bs + r + 2 * (l + (size_t)n * g)] = b[arr * 2 + r];
 }
 
-__global__ void k_pressure(const GP P, const double *__restrict__ U, double *__restrict__ p)
+__device__ __forceinline__ void pressure_body(const GP &P, const double *__restrict__ U, double *__restrict__ p,
+                                              const long long tid)
 {
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long S = (long long)P.nz * P.NumG;
   if (tid >= S) return;
   p[tid] = pressure_dry(P, U[tid + 4 * S]);
+}
+
+__global__ void __launch_bounds__(256) k_pressure(const GP P, const double *__restrict__ U, double *__restrict__ p)
+{
+  pressure_body(P, U, p, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // 1 if any entry is not finite

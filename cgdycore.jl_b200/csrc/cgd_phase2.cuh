@@ -8,8 +8,9 @@
 // The number of tracers NT is a template parameter.
 //
 //   1. The CTA stages the pointwise quantities of its LC levels plus two halo
-//      planes on each side (state, vertical metric, lumped mass, pressure,
-//      theta and tracer ratios) in shared memory.  One barrier.
+//      planes on each side (state, vertical metric, lumped mass, pressure -
+//      computed beforehand, once per column-level, by the kernel that forms
+//      the state - theta and tracer ratios) in shared memory.  One barrier.
 //   2. One thread per (node, interface) forms the vertical mass flux and the
 //      limited upwind fluxes of the interfaces L0-1 .. L0+LC-1 (the one below
 //      the chunk is formed by both neighbouring chunks, with identical
@@ -44,24 +45,31 @@ enum {
   O_D110 = 0, O_D111, O_D120, O_D121, O_D210, O_D211, O_D220, O_D221, O_J1, O_FC,
   O_T1    // + 5 + NumTr: the DSS'd hyperviscosity cache
 };
-constexpr int P2_WARPS = 8;
 constexpr int P2_NSCR = 12;   // scratch quantities per warp (the largest derivative round)
 
+// Warps (levels) per CTA: 16 for p = 4, one 512-thread CTA per SM, whose
+// 128 registers a thread fill the register file (a deeper chunk re-stages
+// fewer halo planes: measured 1.65 ms against 1.81 ms with 8 warps at the
+// nPanel 30, nz 45 size); 8 for p < 4, whose deeper chunks would not fit in
+// shared memory.
 template <int N, int NT, typename R>
 struct P2Cfg {
+  static constexpr int WARPS = N == 5 ? 16 : 8;
+  static constexpr int MINB = N == 5 ? 1 : 2;     // CTAs per SM the registers are sized for
   static constexpr int DoF = N * N;
   static constexpr int LPW = 32 / DoF;           // levels per warp
-  static constexpr int LC = P2_WARPS * LPW;      // levels per CTA
+  static constexpr int LC = WARPS * LPW;         // levels per CTA
   static constexpr int RP = LC + 4;              // staged planes
-  static constexpr int THREADS = 32 * P2_WARPS;
+  static constexpr int THREADS = 32 * WARPS;
   static constexpr size_t SMEM = ((size_t)(Q_TR0 + NT) * RP * DoF + (size_t)(O_T1 + 5 + NT) * LC * DoF +
                                    (size_t)(2 + NT) * (LC + 1) * DoF) * sizeof(double) +
-                                  (size_t)P2_WARPS * P2_NSCR * 32 * sizeof(R);
+                                  (size_t)WARPS * P2_NSCR * 32 * sizeof(R);
 };
 
 template <int N, int NT, typename R>
-__device__ __forceinline__ void phase2_body(const GP &P, const double *__restrict__ U, const double *__restrict__ T1,
-                                            double *__restrict__ C, const int chunk, const int IF)
+__device__ __forceinline__ void phase2_body(const GP &P, const double *__restrict__ U, const double *__restrict__ Pr,
+                                            const double *__restrict__ T1, double *__restrict__ C, const int chunk,
+                                            const int IF)
 {
   using CF = P2Cfg<N, NT, R>;
   constexpr bool MIX = sizeof(R) == sizeof(float);
@@ -80,7 +88,13 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   // ---------------- 1. stage the pointwise planes L0-2 .. L0+LC+1 ----------------
   // (level fastest: every load is a run of consecutive levels of one column
   // or one metric row) and the own levels' metric and cache
-  for (int s = threadIdx.x; s < DoF * RP; s += CF::THREADS) {
+  // at most two slots per thread (DoF * RP <= 2 * THREADS): the loads of both
+  // are issued before any arithmetic that depends on them
+  static_assert(DoF * RP <= 2 * CF::THREADS, "two staging slots per thread");
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int s = threadIdx.x + r * CF::THREADS;
+    if (s >= DoF * RP) continue;
     const int ID = s / RP, p = s % RP;
     const int lev = L0 - 2 + p;
     if (lev < 0 || lev >= nz) continue;
@@ -97,11 +111,13 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
       o[O_J1 * os] = mt[C_J1 * cs];
       o[O_FC * os] = mt[C_FCOR * cs];
       const double *T = T1 + (size_t)nz * g + lev;
+#pragma unroll
       for (int f = 0; f < 5 + NT; ++f) o[(O_T1 + f) * os] = T[f * fs];
     }
     const double rho = Ug[0], rth = Ug[4 * fs];
     PW(Q_RHO, p, ID) = rho;
     PW(Q_CTH, p, ID) = rth / rho;
+#pragma unroll
     for (int q = 0; q < NT; ++q) PW(Q_TR0 + q, p, ID) = Ug[(5 + q) * fs] / rho;
     if (p == 0 || p == RP - 1) continue;   // the outer halo planes feed the upwind stencil only
     PW(Q_U, p, ID) = Ug[fs];
@@ -113,7 +129,7 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
     PW(Q_J0, p, ID) = mt[C_J0 * cs];
     PW(Q_M0, p, ID) = P.M[lev + (size_t)nz * g];
     PW(Q_M1, p, ID) = P.M[lev + (size_t)nz * (g + (size_t)NumG)];
-    PW(Q_P, p, ID) = pressure_dry(P, rth);
+    PW(Q_P, p, ID) = Pr[lev + (size_t)nz * g];
   }
   __syncthreads();
 
@@ -534,10 +550,11 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
 }
 
 template <int N, int NT, typename R>
-__global__ void __launch_bounds__(P2Cfg<N, NT, R>::THREADS, 2)
-    k_phase2(const GP P, const double *__restrict__ U, const double *__restrict__ T1, double *__restrict__ C)
+__global__ void __launch_bounds__(P2Cfg<N, NT, R>::THREADS, P2Cfg<N, NT, R>::MINB)
+    k_phase2(const GP P, const double *__restrict__ U, const double *__restrict__ Pr, const double *__restrict__ T1,
+             double *__restrict__ C)
 {
-  phase2_body<N, NT, R>(P, U, T1, C, blockIdx.x, blockIdx.y);
+  phase2_body<N, NT, R>(P, U, Pr, T1, C, blockIdx.x, blockIdx.y);
 }
 
 }  // namespace cgd

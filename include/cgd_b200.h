@@ -143,7 +143,7 @@ int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const do
 /* Batched ensemble.  Members are handles that share OrdPoly, NumTr, the
  * precision and the device; their grids (nPanel, nz) may differ.  One
  * ensemble step advances every member by one Rosenbrock-W step of its own
- * dt, as one CUDA graph of 12 launches over flat work lists spanning all
+ * dt, as one CUDA graph of 15 launches over flat work lists spanning all
  * members (the kernels of one stage read each member's parameters from
  * constant memory).  Calls on different batches must not run concurrently:
  * they share those constant tables.  The member handles must stay alive and
