@@ -46,6 +46,13 @@ CASES = {
     "tracers_p3": dict(nPanel=5, p=3, nz=12, NumTr=2, stretch="quadratic"),
     "nz64": dict(nPanel=4, p=4, nz=64, NumTr=1, stretch="quadratic"),
     "p2": dict(nPanel=6, p=2, nz=7, NumTr=0, stretch="uniform"),
+    # edge cases: p = 1 (eight levels per warp), three layers (the upwind
+    # stencil clamped at both ends of every interface), the maximum of four
+    # tracers, the maximum of 64 levels at p = 2
+    "p1": dict(nPanel=5, p=1, nz=9, NumTr=1, stretch="quadratic"),
+    "nz3": dict(nPanel=4, p=4, nz=3, NumTr=0, stretch="uniform"),
+    "tracers4": dict(nPanel=3, p=4, nz=17, NumTr=4, stretch="quadratic"),
+    "p2_nz64": dict(nPanel=3, p=2, nz=64, NumTr=0, stretch="quadratic"),
 }
 
 
@@ -169,4 +176,23 @@ def test_dropin_configuration(oracle_mod, lib_ready, variant):
     Vg = U.copy(order="F")
     d.time_stepper(Vg, 120.0, 2)
     _same(Vg, Vo, d.exact, TOL_STEP)
+    d.close()
+
+
+@pytest.mark.parametrize("variant", ["exact", "fast"])
+def test_two_layers(oracle_mod, lib_ready, variant):
+    """nz = 2, a single interface: tendency, Jacobian and Schur solve.  (The
+    restated reference integration itself blows up within ten steps on two
+    layers at any dt tried down to 10 s, so no steps are compared here.)"""
+    o, g, U, nu = make_case(oracle_mod, 4, 4, 2, 1, "uniform")
+    d = _dycore(g, 1, nu, exact=(variant == "exact"))
+    _same(d.fcn(U), o.rhs(U), d.exact, TOL_RHS)
+    bo, bg = o.jac(U), d.jac(U)
+    assert np.abs(bg - bo).max() <= 1e-14 * np.abs(bo).max()
+    v = np.asfortranarray(np.random.default_rng(3).standard_normal(U.shape))
+    ko, vo = o.schur(v, 300.0)
+    vg = v.copy(order="F")
+    kg = d.schur_solve(vg, 300.0)
+    _same(kg, ko, d.exact, TOL_RHS)
+    _same(vg, vo, d.exact, TOL_RHS)
     d.close()
