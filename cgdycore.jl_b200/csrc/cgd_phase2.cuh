@@ -37,9 +37,18 @@ namespace cgd {
 // pointwise quantities per (plane, node)
 enum {
   Q_RHO = 0, Q_U, Q_V, Q_W, Q_D310, Q_D311, Q_D320, Q_D321, Q_D330, Q_D331,
-  Q_M0, Q_M1, Q_P, Q_J0, Q_CTH,
+  Q_M0, Q_M1, Q_P, Q_J0, Q_CTH, Q_RTH,
   Q_TR0   // + one per tracer: rho*q / rho
 };
+
+// 8-byte asynchronous copy global -> shared (cp.async, sm_80 and later) and
+// the wait for all of a thread's copies
+__device__ __forceinline__ void cp_async8(double *smem_dst, const double *gsrc)
+{
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 // quantities of the CTA's own levels per (level, node)
 enum {
   O_D110 = 0, O_D111, O_D120, O_D121, O_D210, O_D211, O_D220, O_D221, O_J1, O_FC,
@@ -88,8 +97,8 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   // ---------------- 1. stage the pointwise planes L0-2 .. L0+LC+1 ----------------
   // (level fastest: every load is a run of consecutive levels of one column
   // or one metric row) and the own levels' metric and cache
-  // at most two slots per thread (DoF * RP <= 2 * THREADS): the loads of both
-  // are issued before any arithmetic that depends on them
+  // at most two slots per thread (DoF * RP <= 2 * THREADS); every value is
+  // copied with cp.async, so all of a thread's copies are in flight at once
   static_assert(DoF * RP <= 2 * CF::THREADS, "two staging slots per thread");
 #pragma unroll
   for (int r = 0; r < 2; ++r) {
@@ -104,32 +113,46 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
     if (p >= 2 && p <= LC + 1) {
       double *o = ow + (size_t)(p - 2) * DoF + ID;
       constexpr size_t os = (size_t)LC * DoF;
-      o[O_D110 * os] = mt[C_D11_0 * cs]; o[O_D111 * os] = mt[C_D11_1 * cs];
-      o[O_D120 * os] = mt[C_D12_0 * cs]; o[O_D121 * os] = mt[C_D12_1 * cs];
-      o[O_D210 * os] = mt[C_D21_0 * cs]; o[O_D211 * os] = mt[C_D21_1 * cs];
-      o[O_D220 * os] = mt[C_D22_0 * cs]; o[O_D221 * os] = mt[C_D22_1 * cs];
-      o[O_J1 * os] = mt[C_J1 * cs];
-      o[O_FC * os] = mt[C_FCOR * cs];
+      cp_async8(o + O_D110 * os, mt + C_D11_0 * cs); cp_async8(o + O_D111 * os, mt + C_D11_1 * cs);
+      cp_async8(o + O_D120 * os, mt + C_D12_0 * cs); cp_async8(o + O_D121 * os, mt + C_D12_1 * cs);
+      cp_async8(o + O_D210 * os, mt + C_D21_0 * cs); cp_async8(o + O_D211 * os, mt + C_D21_1 * cs);
+      cp_async8(o + O_D220 * os, mt + C_D22_0 * cs); cp_async8(o + O_D221 * os, mt + C_D22_1 * cs);
+      cp_async8(o + O_J1 * os, mt + C_J1 * cs);
+      cp_async8(o + O_FC * os, mt + C_FCOR * cs);
       const double *T = T1 + (size_t)nz * g + lev;
 #pragma unroll
-      for (int f = 0; f < 5 + NT; ++f) o[(O_T1 + f) * os] = T[f * fs];
+      for (int f = 0; f < 5 + NT; ++f) cp_async8(o + (O_T1 + f) * os, T + f * fs);
     }
-    const double rho = Ug[0], rth = Ug[4 * fs];
-    PW(Q_RHO, p, ID) = rho;
-    PW(Q_CTH, p, ID) = rth / rho;
+    cp_async8(&PW(Q_RHO, p, ID), Ug);
+    cp_async8(&PW(Q_RTH, p, ID), Ug + 4 * fs);
 #pragma unroll
-    for (int q = 0; q < NT; ++q) PW(Q_TR0 + q, p, ID) = Ug[(5 + q) * fs] / rho;
+    for (int q = 0; q < NT; ++q) cp_async8(&PW(Q_TR0 + q, p, ID), Ug + (5 + q) * fs);   // rho*q for now
     if (p == 0 || p == RP - 1) continue;   // the outer halo planes feed the upwind stencil only
-    PW(Q_U, p, ID) = Ug[fs];
-    PW(Q_V, p, ID) = Ug[2 * fs];
-    PW(Q_W, p, ID) = Ug[3 * fs];
-    PW(Q_D310, p, ID) = mt[C_D31_0 * cs]; PW(Q_D311, p, ID) = mt[C_D31_1 * cs];
-    PW(Q_D320, p, ID) = mt[C_D32_0 * cs]; PW(Q_D321, p, ID) = mt[C_D32_1 * cs];
-    PW(Q_D330, p, ID) = mt[C_D33_0 * cs]; PW(Q_D331, p, ID) = mt[C_D33_1 * cs];
-    PW(Q_J0, p, ID) = mt[C_J0 * cs];
-    PW(Q_M0, p, ID) = P.M[lev + (size_t)nz * g];
-    PW(Q_M1, p, ID) = P.M[lev + (size_t)nz * (g + (size_t)NumG)];
-    PW(Q_P, p, ID) = Pr[lev + (size_t)nz * g];
+    cp_async8(&PW(Q_U, p, ID), Ug + fs);
+    cp_async8(&PW(Q_V, p, ID), Ug + 2 * fs);
+    cp_async8(&PW(Q_W, p, ID), Ug + 3 * fs);
+    cp_async8(&PW(Q_D310, p, ID), mt + C_D31_0 * cs); cp_async8(&PW(Q_D311, p, ID), mt + C_D31_1 * cs);
+    cp_async8(&PW(Q_D320, p, ID), mt + C_D32_0 * cs); cp_async8(&PW(Q_D321, p, ID), mt + C_D32_1 * cs);
+    cp_async8(&PW(Q_D330, p, ID), mt + C_D33_0 * cs); cp_async8(&PW(Q_D331, p, ID), mt + C_D33_1 * cs);
+    cp_async8(&PW(Q_J0, p, ID), mt + C_J0 * cs);
+    cp_async8(&PW(Q_M0, p, ID), P.M + lev + (size_t)nz * g);
+    cp_async8(&PW(Q_M1, p, ID), P.M + lev + (size_t)nz * (g + (size_t)NumG));
+    cp_async8(&PW(Q_P, p, ID), Pr + lev + (size_t)nz * g);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  // theta and the tracer ratios of the staged planes
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int s = threadIdx.x + r * CF::THREADS;
+    if (s >= DoF * RP) continue;
+    const int ID = s / RP, p = s % RP;
+    const int lev = L0 - 2 + p;
+    if (lev < 0 || lev >= nz) continue;
+    const double rho = PW(Q_RHO, p, ID);
+    PW(Q_CTH, p, ID) = PW(Q_RTH, p, ID) / rho;
+#pragma unroll
+    for (int q = 0; q < NT; ++q) PW(Q_TR0 + q, p, ID) = PW(Q_TR0 + q, p, ID) / rho;
   }
   __syncthreads();
 
