@@ -117,13 +117,25 @@ bool is_device_ptr(const void *p)
 }
 
 
-template <int N>
-void launch_hv1(cgd_handle *h, const double *U, double *C)
+template <int N, int NT>
+void launch_hv1t(cgd_handle *h, const double *U, double *C)
 {
   constexpr int LT = 256 / (N * N);
   dim3 grid((h->nz + LT - 1) / LT, h->NF);   // the level tiles of one element run back to back
-  if (h->mix) k_hypervisc1<N, float><<<grid, 256, 0, h->stream>>>(h->gp, U, C);
-  else k_hypervisc1<N, double><<<grid, 256, 0, h->stream>>>(h->gp, U, C);
+  if (h->mix) k_hypervisc1<N, NT, float><<<grid, 256, 0, h->stream>>>(h->gp, U, C);
+  else k_hypervisc1<N, NT, double><<<grid, 256, 0, h->stream>>>(h->gp, U, C);
+}
+
+template <int N>
+void launch_hv1(cgd_handle *h, const double *U, double *C)
+{
+  switch (h->NumTr) {
+    case 0: launch_hv1t<N, 0>(h, U, C); break;
+    case 1: launch_hv1t<N, 1>(h, U, C); break;
+    case 2: launch_hv1t<N, 2>(h, U, C); break;
+    case 3: launch_hv1t<N, 3>(h, U, C); break;
+    default: launch_hv1t<N, 4>(h, U, C); break;
+  }
 }
 
 template <int N, int NT, typename R>
@@ -857,7 +869,7 @@ void batch_enqueue_t(cgd_batch *b, WItem *const *w)
   }
   kb_pressure<<<b->n[1], 256, 0, b->stream>>>(w[1], 0);
   for (int stage = 0; stage < 3; ++stage) {
-    kb_hypervisc1<N, R><<<b->n[0], 256, 0, b->stream>>>(w[0], stage);
+    kb_hypervisc1<N, NT, R><<<b->n[0], 256, 0, b->stream>>>(w[0], stage);
     kb_gather<<<b->n[1], 256, 0, b->stream>>>(w[1]);
     kb_phase2<N, NT, R><<<b->n[2], CF::THREADS, CF::SMEM, b->stream>>>(w[2], stage);
     if (stage == 0) kb_column<0><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);

@@ -29,12 +29,12 @@ __constant__ GP c_bgp[BMAX];
 __constant__ BMember c_bm[BMAX];
 __constant__ RK c_brk;
 
-template <int N, typename R>
+template <int N, int NT, typename R>
 __global__ void __launch_bounds__(256, 4) kb_hypervisc1(const WItem *__restrict__ w, const int stage)
 {
   const WItem it = w[blockIdx.x];
   const BMember &B = c_bm[it.m];
-  hypervisc1_body<N, R>(c_bgp[it.m], stage == 0 ? B.U : B.Vst, B.C, it.x, it.y);
+  hypervisc1_body<N, NT, R>(c_bgp[it.m], stage == 0 ? B.U : B.Vst, B.C, it.x, it.y);
 }
 
 __global__ void __launch_bounds__(256) kb_pressure(const WItem *__restrict__ w, const int stage_state)

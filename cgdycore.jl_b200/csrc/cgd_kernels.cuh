@@ -117,14 +117,16 @@ __device__ __forceinline__ void recu4(double cLL, double cL, double cR, double c
 // mixed form, where theta enters as its perturbation from the level's FP64
 // reference value.
 // ---------------------------------------------------------------------------
-template <int N, typename R>
+template <int N, int NT, typename R>
 __device__ __forceinline__ void hypervisc1_body(const GP &P, const double *__restrict__ U, double *__restrict__ C,
                                                 const int tile, const int IF)
 {
   constexpr bool MIX = sizeof(R) == sizeof(float);
   constexpr int DoF = N * N;
   constexpr int LT = 256 / DoF;
-  __shared__ R s[9][LT * DoF];
+  // planes: 0-3 curl/contra of (u,v), 4 theta, 5-8 the first derivatives,
+  // then per tracer its ratio and the two components of its gradient
+  __shared__ R s[9 + 3 * NT][LT * DoF];
   const int t = threadIdx.x;
   const int lvl = t % LT, ID = t / LT;
   const int I = ID % N, Jn = ID / N;
@@ -159,6 +161,8 @@ __device__ __forceinline__ void hypervisc1_body(const GP &P, const double *__res
     s[3][si] = d21 * u + d22 * v;
     if (MIX) s[4][si] = (R)(Ug[4 * fs] / Ug[0] - P.thref[l]);
     else s[4][si] = (R)(Ug[4 * fs] / Ug[0]);
+#pragma unroll
+    for (int q = 0; q < NT; ++q) s[9 + 3 * q][si] = (R)(Ug[(5 + q) * fs] / Ug[0]);
     MCD = P.M[l + (size_t)nz * g] + P.M[l + (size_t)nz * (g + (size_t)NumG)];
   }
   const R Js = (R)JsD, MC = (R)MCD;
@@ -184,6 +188,21 @@ __device__ __forceinline__ void hypervisc1_body(const GP &P, const double *__res
     R GradDy = CGD_DIVJ(d12 * Dxc + d22 * Dyc);
     s[7][si] = d11 * GradDx + d12 * GradDy;         // Contra12
     s[8][si] = d21 * GradDx + d22 * GradDy;
+#pragma unroll
+    for (int q = 0; q < NT; ++q) {
+      const R *Tr = s[9 + 3 * q] + row;
+      R Dxt = DI[0] * Tr[N * Jn];
+      R Dyt = DJ[0] * Tr[I];
+#pragma unroll
+      for (int k = 1; k < N; ++k) {
+        Dxt = rsum1(Dxt, DI[k], Tr[k + N * Jn]);
+        Dyt = rsum1(Dyt, DJ[k], Tr[I + N * k]);
+      }
+      R GDx = CGD_DIVJ(d11 * Dxt + d21 * Dyt);
+      R GDy = CGD_DIVJ(d12 * Dxt + d22 * Dyt);
+      s[10 + 3 * q][si] = d11 * GDx + d12 * GDy;
+      s[11 + 3 * q][si] = d21 * GDx + d22 * GDy;
+    }
   }
   __syncthreads();
   double *out = C + ((size_t)IF * P.NC * DoF + ID) * nz + l;
@@ -215,45 +234,22 @@ __device__ __forceinline__ void hypervisc1_body(const GP &P, const double *__res
     out[2 * cs] = (double)CGD_DIVM(FuD);
     out[3 * cs] = (double)CGD_DIVM(FvD);
     out[4 * cs] = (double)CGD_DIVM(DivTh);
-  }
-  for (int iT = 0; iT < P.NumTr; ++iT) {
-    if (act) {
-      const size_t fs = (size_t)nz * NumG;
-      const double *Ug = U + l + (size_t)nz * g;
-      s[4][si] = (R)(Ug[(5 + iT) * fs] / Ug[0]);
-    }
-    __syncthreads();
-    if (act) {
-      const R *Tr = s[4] + row;
-      R Dxc = DI[0] * Tr[N * Jn];
-      R Dyc = DJ[0] * Tr[I];
 #pragma unroll
-      for (int k = 1; k < N; ++k) {
-        Dxc = rsum1(Dxc, DI[k], Tr[k + N * Jn]);
-        Dyc = rsum1(Dyc, DJ[k], Tr[I + N * k]);
-      }
-      R GradDx = CGD_DIVJ(d11 * Dxc + d21 * Dyc);
-      R GradDy = CGD_DIVJ(d12 * Dxc + d22 * Dyc);
-      s[7][si] = d11 * GradDx + d12 * GradDy;
-      s[8][si] = d21 * GradDx + d22 * GradDy;
-    }
-    __syncthreads();
-    if (act) {
-      const R *Cx = s[7] + row, *Cy = s[8] + row;
-      R DivTr = WI[0] * Cx[N * Jn] + WJ[0] * Cy[I];
+    for (int q = 0; q < NT; ++q) {
+      const R *Tx = s[10 + 3 * q] + row, *Ty = s[11 + 3 * q] + row;
+      R DivTr = WI[0] * Tx[N * Jn] + WJ[0] * Ty[I];
 #pragma unroll
-      for (int k = 1; k < N; ++k) DivTr = rsum2(DivTr, WI[k], Cx[k + N * Jn], WJ[k], Cy[I + N * k]);
-      out[(5 + iT) * cs] = (double)CGD_DIVM(DivTr);
+      for (int k = 1; k < N; ++k) DivTr = rsum2(DivTr, WI[k], Tx[k + N * Jn], WJ[k], Ty[I + N * k]);
+      out[(5 + q) * cs] = (double)CGD_DIVM(DivTr);
     }
-    __syncthreads();
   }
 }
 
-template <int N, typename R>
+template <int N, int NT, typename R>
 __global__ void __launch_bounds__(256, 4) k_hypervisc1(const GP P, const double *__restrict__ U,
                                                       double *__restrict__ C)
 {
-  hypervisc1_body<N, R>(P, U, C, blockIdx.x, blockIdx.y);
+  hypervisc1_body<N, NT, R>(P, U, C, blockIdx.x, blockIdx.y);
 }
 
 // Sum the contributions of the element nodes sharing global DOF g at level l
