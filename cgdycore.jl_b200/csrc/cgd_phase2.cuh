@@ -37,7 +37,7 @@ namespace cgd {
 // pointwise quantities per (plane, node)
 enum {
   Q_RHO = 0, Q_U, Q_V, Q_W, Q_D310, Q_D311, Q_D320, Q_D321, Q_D330, Q_D331,
-  Q_M0, Q_M1, Q_P, Q_J0, Q_CTH, Q_RTH,
+  Q_M0, Q_M1, Q_P, Q_J0, Q_CTH,
   Q_TR0   // + one per tracer: rho*q / rho
 };
 
@@ -54,7 +54,6 @@ enum {
   O_D110 = 0, O_D111, O_D120, O_D121, O_D210, O_D211, O_D220, O_D221, O_J1, O_FC,
   O_T1    // + 5 + NumTr: the DSS'd hyperviscosity cache
 };
-constexpr int P2_NSCR = 12;   // scratch quantities per warp (the largest derivative round)
 
 // Warps (levels) per CTA: 16 for p = 4, one 512-thread CTA per SM, whose
 // 128 registers a thread fill the register file (a deeper chunk re-stages
@@ -70,9 +69,13 @@ struct P2Cfg {
   static constexpr int LC = WARPS * LPW;         // levels per CTA
   static constexpr int RP = LC + 4;              // staged planes
   static constexpr int THREADS = 32 * WARPS;
+  // scratch quantities per warp (the largest derivative round: 5+NT, 4+2NT,
+  // 6 for each half of the momentum round, 6+NT) and the scratch row length
+  static constexpr int NSCR = (4 + 2 * NT) > (6 + NT) ? (4 + 2 * NT) : (6 + NT);
+  static constexpr int SCS = LPW * DoF;
   static constexpr size_t SMEM = ((size_t)(Q_TR0 + NT) * RP * DoF + (size_t)(O_T1 + 5 + NT) * LC * DoF +
                                    (size_t)(2 + NT) * (LC + 1) * DoF) * sizeof(double) +
-                                  (size_t)WARPS * P2_NSCR * 32 * sizeof(R);
+                                  (size_t)WARPS * NSCR * SCS * sizeof(R);
 };
 
 template <int N, int NT, typename R>
@@ -90,7 +93,7 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   double *pw = sm;                                             // [Q][R][DoF]
   double *ow = pw + (size_t)(Q_TR0 + NT) * RP * DoF;             // [O][LC][DoF]
   double *fx = ow + (size_t)(O_T1 + 5 + NT) * LC * DoF;         // [2+NT][LC+1][DoF] interface fluxes
-  R *scr = (R *)(fx + (size_t)(2 + NT) * (LC + 1) * DoF);      // [warp][P2_NSCR][32]
+  R *scr = (R *)(fx + (size_t)(2 + NT) * (LC + 1) * DoF);      // [warp][NSCR][SCS]
   const double *mte = P.met + (size_t)IF * NCOMP * cs;
 #define PW(q, p, id) pw[((size_t)(q) * RP + (p)) * DoF + (id)]
 
@@ -124,7 +127,7 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
       for (int f = 0; f < 5 + NT; ++f) cp_async8(o + (O_T1 + f) * os, T + f * fs);
     }
     cp_async8(&PW(Q_RHO, p, ID), Ug);
-    cp_async8(&PW(Q_RTH, p, ID), Ug + 4 * fs);
+    cp_async8(&PW(Q_CTH, p, ID), Ug + 4 * fs);   // rho*theta for now
 #pragma unroll
     for (int q = 0; q < NT; ++q) cp_async8(&PW(Q_TR0 + q, p, ID), Ug + (5 + q) * fs);   // rho*q for now
     if (p == 0 || p == RP - 1) continue;   // the outer halo planes feed the upwind stencil only
@@ -150,7 +153,7 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
     const int lev = L0 - 2 + p;
     if (lev < 0 || lev >= nz) continue;
     const double rho = PW(Q_RHO, p, ID);
-    PW(Q_CTH, p, ID) = PW(Q_RTH, p, ID) / rho;
+    PW(Q_CTH, p, ID) = PW(Q_CTH, p, ID) / rho;
 #pragma unroll
     for (int q = 0; q < NT; ++q) PW(Q_TR0 + q, p, ID) = PW(Q_TR0 + q, p, ID) / rho;
   }
@@ -198,8 +201,9 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   const bool act = sub < LPW && lv < nz;
   const int I = ID % N, Jn = ID / N;
   const int p0 = lv - (L0 - 2);          // own plane
-  R *sw = scr + (size_t)warp * P2_NSCR * 32 + sub * DoF;        // this level's scratch row base
-#define SC(q, id) sw[(q) * 32 + (id)]
+  constexpr int SCS = CF::SCS;
+  R *sw = scr + (size_t)warp * CF::NSCR * SCS + sub * DoF;     // this level's scratch row base
+#define SC(q, id) sw[(q) * SCS + (id)]
 
   // derivative coefficients of this node
   R DI[N], DJ[N];
@@ -350,19 +354,44 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
 #pragma unroll
     for (int q = 0; q < NT; ++q) acc_tr[q] += CGD_DIVM(FX(2 + q, lv - 1));
   }
-  // ---- round 3: vector-invariant momentum ----
+  // ---- round 3: vector-invariant momentum, in two halves of six quantities ----
+  const double tu0 = e330 * v - e320 * wl, tu1 = e331 * v - e321 * wh;
+  const double tv0 = e330 * u - e310 * wl, tv1 = e331 * u - e311 * wh;
+  const double tw0 = e320 * u - e310 * v, tw1 = e321 * u - e311 * v;
+  R U1 = 0, U2 = 0, V1 = 0, V2 = 0, W1 = 0, W2 = 0;
+  if (act) {
+    const R d110 = (R)OW(O_D110), d111 = (R)OW(O_D111), d120 = (R)OW(O_D120), d121 = (R)OW(O_D121);
+    const R d210 = (R)OW(O_D210), d220 = (R)OW(O_D220), d221 = (R)OW(O_D221);
+    const R wlR = (R)wl, whR = (R)wh;
+    SC(0, ID) = -d120 * wlR;  SC(1, ID) = -d121 * whR;    // tempuZ1
+    SC(2, ID) = -d220 * wlR;  SC(3, ID) = -d221 * whR;    // tempuZ2
+    SC(4, ID) = -d110 * wlR;                              // tempvZ1 (lower)
+    SC(5, ID) = -d210 * wlR;                              // tempvZ2 (lower)
+    (void)d111;
+  }
+  __syncwarp();
+  if (act) {
+    U1 = (R)(0.5 * (tu1 - tu0)); U2 = U1;
+    V1 = (R)(0.5 * (tv1 - tv0)); V2 = V1;
+    W1 = (R)(0.5 * (tw1 - tw0)); W2 = W1;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      U1 = rsum2(U1, DI[k], SC(0, k + N * Jn), DJ[k], SC(2, I + N * k));
+      U2 = rsum2(U2, DI[k], SC(1, k + N * Jn), DJ[k], SC(3, I + N * k));
+      V1 = rsum2(V1, DI[k], SC(4, k + N * Jn), DJ[k], SC(5, I + N * k));
+    }
+  }
+  __syncwarp();
   if (act) {
     const R d110 = (R)OW(O_D110), d111 = (R)OW(O_D111), d120 = (R)OW(O_D120), d121 = (R)OW(O_D121);
     const R d210 = (R)OW(O_D210), d211 = (R)OW(O_D211), d220 = (R)OW(O_D220), d221 = (R)OW(O_D221);
-    const R uR = (R)u, vR = (R)v, wlR = (R)wl, whR = (R)wh;
-    SC(0, ID) = -d120 * wlR;  SC(1, ID) = -d121 * whR;    // tempuZ1
-    SC(2, ID) = -d220 * wlR;  SC(3, ID) = -d221 * whR;    // tempuZ2
-    SC(4, ID) = -d110 * wlR;  SC(5, ID) = -d111 * whR;    // tempvZ1
-    SC(6, ID) = -d210 * wlR;  SC(7, ID) = -d211 * whR;    // tempvZ2
-    SC(8, ID) = d120 * uR - d110 * vR;                    // tempwZ1
-    SC(9, ID) = d121 * uR - d111 * vR;
-    SC(10, ID) = d220 * uR - d210 * vR;                   // tempwZ2
-    SC(11, ID) = d221 * uR - d211 * vR;
+    const R uR = (R)u, vR = (R)v, whR = (R)wh;
+    SC(0, ID) = -d111 * whR;                              // tempvZ1 (upper)
+    SC(1, ID) = -d211 * whR;                              // tempvZ2 (upper)
+    SC(2, ID) = d120 * uR - d110 * vR;                    // tempwZ1
+    SC(3, ID) = d121 * uR - d111 * vR;
+    SC(4, ID) = d220 * uR - d210 * vR;                    // tempwZ2
+    SC(5, ID) = d221 * uR - d211 * vR;
   }
   __syncwarp();
   // the w denominators (rho_l M1_l + rho_l+1 M0_l+1 at the interface); the fast
@@ -374,20 +403,11 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
 #define CGD_DIVW(x, d) ((x) / (d))
 #endif
   if (act) {
-    const double tu0 = e330 * v - e320 * wl, tu1 = e331 * v - e321 * wh;
-    const double tv0 = e330 * u - e310 * wl, tv1 = e331 * u - e311 * wh;
-    const double tw0 = e320 * u - e310 * v, tw1 = e321 * u - e311 * v;
-    R U1 = (R)(0.5 * (tu1 - tu0)), U2 = U1;
-    R V1 = (R)(0.5 * (tv1 - tv0)), V2 = V1;
-    R W1 = (R)(0.5 * (tw1 - tw0)), W2 = W1;
 #pragma unroll
     for (int k = 0; k < N; ++k) {
-      U1 = rsum2(U1, DI[k], SC(0, k + N * Jn), DJ[k], SC(2, I + N * k));
-      U2 = rsum2(U2, DI[k], SC(1, k + N * Jn), DJ[k], SC(3, I + N * k));
-      V1 = rsum2(V1, DI[k], SC(4, k + N * Jn), DJ[k], SC(6, I + N * k));
-      V2 = rsum2(V2, DI[k], SC(5, k + N * Jn), DJ[k], SC(7, I + N * k));
-      W1 = rsum2(W1, DI[k], SC(8, k + N * Jn), DJ[k], SC(10, I + N * k));
-      W2 = rsum2(W2, DI[k], SC(9, k + N * Jn), DJ[k], SC(11, I + N * k));
+      V2 = rsum2(V2, DI[k], SC(0, k + N * Jn), DJ[k], SC(1, I + N * k));
+      W1 = rsum2(W1, DI[k], SC(2, k + N * Jn), DJ[k], SC(4, I + N * k));
+      W2 = rsum2(W2, DI[k], SC(3, k + N * Jn), DJ[k], SC(5, I + N * k));
     }
     // vertical parts from the neighbour levels
     double FU = 0.0, FV = 0.0, FW1 = 0.0, FW2 = 0.0;
