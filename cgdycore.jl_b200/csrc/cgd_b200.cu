@@ -196,24 +196,42 @@ void pressure(cgd_handle *h, const double *U, double *p)
   k_pressure<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->gp, U, p);
 }
 
-void gather(cgd_handle *h, const double *C, double *out, bool wsplit)
+// wsplit: the phase-2 tendency (w split into two contributions, FP64 output);
+// otherwise phase 1, whose output is the cache (stored like the contributions)
+// or, with tendency_out, an FP64 array for the caller.
+void gather(cgd_handle *h, const double *C, double *out, bool wsplit, bool tendency_out = false)
 {
   long long n = (long long)h->nz * h->NumG;
-  if (wsplit) k_gather<true><<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->gp, C, out);
-  else k_gather<false><<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->gp, C, out);
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  if (h->mix) {
+    if (wsplit) k_gather<true, false, true><<<nb, 256, 0, h->stream>>>(h->gp, C, out);
+    else if (tendency_out) k_gather<false, false, true><<<nb, 256, 0, h->stream>>>(h->gp, C, out);
+    else k_gather<false, true, true><<<nb, 256, 0, h->stream>>>(h->gp, C, out);
+  } else {
+    if (wsplit) k_gather<true, false, false><<<nb, 256, 0, h->stream>>>(h->gp, C, out);
+    else if (tendency_out) k_gather<false, false, false><<<nb, 256, 0, h->stream>>>(h->gp, C, out);
+    else k_gather<false, true, false><<<nb, 256, 0, h->stream>>>(h->gp, C, out);
+  }
+}
+
+template <int MODE, bool C32>
+void column_t(cgd_handle *h, const ColArgs &a)
+{
+  size_t smem = (size_t)COL_WARPS * COL_ARR * h->nz * sizeof(double);
+  static bool attr = false;
+  if (!attr) {   // up to 8 warps x 15 arrays x 64 levels
+    cudaFuncSetAttribute(k_column<MODE, C32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         COL_WARPS * COL_ARR * 64 * (int)sizeof(double));
+    attr = true;
+  }
+  k_column<MODE, C32><<<(h->NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, h->stream>>>(h->gp, a);
 }
 
 template <int MODE>
 void column(cgd_handle *h, const ColArgs &a)
 {
-  size_t smem = (size_t)COL_WARPS * COL_ARR * h->nz * sizeof(double);
-  static bool attr = false;
-  if (!attr) {   // up to 8 warps x 15 arrays x 64 levels
-    cudaFuncSetAttribute(k_column<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         COL_WARPS * COL_ARR * 64 * (int)sizeof(double));
-    attr = true;
-  }
-  k_column<MODE><<<(h->NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, h->stream>>>(h->gp, a);
+  if (h->mix) column_t<MODE, true>(h, a);
+  else column_t<MODE, false>(h, a);
 }
 
 // Event between two kernels of a step launched without the graph (the
@@ -552,7 +570,7 @@ int cgd_hypervisc_phase1(cgd_handle *h, const double *U, double *Temp1)
   double *td = tdev ? Temp1 : h->Fbuf;
   ensure_ref(h, Ud);
   hv1(h, Ud, h->C);
-  gather(h, h->C, td, false);
+  gather(h, h->C, td, false, true);
   if (!tdev)
     CK(cudaMemcpyAsync(Temp1, td, (size_t)h->nz * h->NumG * h->NV * 8, cudaMemcpyDeviceToHost, h->stream));
   return finish(h);
@@ -705,7 +723,7 @@ int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const do
     if (!g_noalloc_ptr[dev]) {
       void *p = nullptr;
       CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-      CK(cudaFuncSetAttribute(k_column<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      CK(cudaFuncSetAttribute(k_column<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               COL_WARPS * COL_ARR * 64 * (int)sizeof(double)));
       g_noalloc_ptr[dev] = static_cast<double *>(p);
     }
@@ -724,7 +742,7 @@ int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const do
   a.fac = fac;
   a.dt = fac;
   const size_t smem = (size_t)COL_WARPS * COL_ARR * P.nz * sizeof(double);
-  k_column<3><<<(P.NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, st>>>(P, a);
+  k_column<3, false><<<(P.NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, st>>>(P, a);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(st));
   return CGD_OK;
@@ -863,18 +881,20 @@ void batch_enqueue_t(cgd_batch *b, WItem *const *w)
   const size_t csmem = (size_t)COL_WARPS * COL_ARR * b->nzmax * sizeof(double);
   if (!attr) {
     cudaFuncSetAttribute(kb_phase2<N, NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
-    for (auto f : {kb_column<0>, kb_column<1>, kb_column<2>})
+    constexpr bool C32 = sizeof(R) == sizeof(float);
+    for (auto f : {kb_column<0, C32>, kb_column<1, C32>, kb_column<2, C32>})
       cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, COL_WARPS * COL_ARR * 64 * (int)sizeof(double));
     attr = true;
   }
   kb_pressure<<<b->n[1], 256, 0, b->stream>>>(w[1], 0);
   for (int stage = 0; stage < 3; ++stage) {
     kb_hypervisc1<N, NT, R><<<b->n[0], 256, 0, b->stream>>>(w[0], stage);
-    kb_gather<<<b->n[1], 256, 0, b->stream>>>(w[1]);
+    kb_gather<sizeof(R) == sizeof(float)><<<b->n[1], 256, 0, b->stream>>>(w[1]);
     kb_phase2<N, NT, R><<<b->n[2], CF::THREADS, CF::SMEM, b->stream>>>(w[2], stage);
-    if (stage == 0) kb_column<0><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);
-    else if (stage == 1) kb_column<1><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);
-    else kb_column<2><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);
+    constexpr bool C32 = sizeof(R) == sizeof(float);
+    if (stage == 0) kb_column<0, C32><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);
+    else if (stage == 1) kb_column<1, C32><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);
+    else kb_column<2, C32><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);
     if (stage < 2) kb_pressure<<<b->n[1], 256, 0, b->stream>>>(w[1], 1);
   }
 }

@@ -45,11 +45,12 @@ __global__ void __launch_bounds__(256) kb_pressure(const WItem *__restrict__ w, 
                 (long long)it.x * blockDim.x + threadIdx.x);
 }
 
+template <bool C32>
 __global__ void __launch_bounds__(256) kb_gather(const WItem *__restrict__ w)
 {
   const WItem it = w[blockIdx.x];
   const BMember &B = c_bm[it.m];
-  gather_body<false>(c_bgp[it.m], B.C, B.T1, (long long)it.x * blockDim.x + threadIdx.x);
+  gather_body<false, true, C32>(c_bgp[it.m], B.C, B.T1, (long long)it.x * blockDim.x + threadIdx.x);
 }
 
 template <int N, int NT, typename R>
@@ -60,7 +61,7 @@ __global__ void __launch_bounds__(P2Cfg<N, NT, R>::THREADS, P2Cfg<N, NT, R>::MIN
   phase2_body<N, NT, R>(c_bgp[it.m], stage == 0 ? B.U : B.Vst, stage == 0 ? B.P0 : B.Pst, B.T1, B.C, it.x, it.y);
 }
 
-template <int MODE>
+template <int MODE, bool C32>
 __global__ void __launch_bounds__(32 * COL_WARPS, MODE == 2 ? 3 : 4) kb_column(const WItem *__restrict__ w)
 {
   const WItem it = w[blockIdx.x];
@@ -79,7 +80,7 @@ __global__ void __launch_bounds__(32 * COL_WARPS, MODE == 2 ? 3 : 4) kb_column(c
   if (MODE == 0) { a.kout = B.k1; a.Vout = B.Vst; }
   else if (MODE == 1) { a.kout = B.k2; a.Vout = B.Vst; }
   else { a.kout = nullptr; a.Vout = B.U; }
-  column_body<MODE>(c_bgp[it.m], a, it.x);
+  column_body<MODE, C32>(c_bgp[it.m], a, it.x);
 }
 
 }  // namespace cgd

@@ -22,6 +22,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <type_traits>
 #include "../../include/cgd_math.h"
 
 // Two builds come from this source, both compiled without multiply-add
@@ -205,7 +206,8 @@ __device__ __forceinline__ void hypervisc1_body(const GP &P, const double *__res
     }
   }
   __syncthreads();
-  double *out = C + ((size_t)IF * P.NC * DoF + ID) * nz + l;
+  using CT = typename std::conditional<MIX, float, double>::type;   // stored contributions
+  CT *out = reinterpret_cast<CT *>(C) + ((size_t)IF * P.NC * DoF + ID) * nz + l;
   R WI[N], WJ[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) {
@@ -229,18 +231,18 @@ __device__ __forceinline__ void hypervisc1_body(const GP &P, const double *__res
     R FvC = -d11 * DxCurl - d21 * DyCurl;
     R FuD = d11 * DxDiv + d21 * DyDiv;         // Grad12
     R FvD = d12 * DxDiv + d22 * DyDiv;
-    out[0 * cs] = (double)CGD_DIVM(-FuC);
-    out[1 * cs] = (double)CGD_DIVM(-FvC);
-    out[2 * cs] = (double)CGD_DIVM(FuD);
-    out[3 * cs] = (double)CGD_DIVM(FvD);
-    out[4 * cs] = (double)CGD_DIVM(DivTh);
+    out[0 * cs] = (CT)CGD_DIVM(-FuC);
+    out[1 * cs] = (CT)CGD_DIVM(-FvC);
+    out[2 * cs] = (CT)CGD_DIVM(FuD);
+    out[3 * cs] = (CT)CGD_DIVM(FvD);
+    out[4 * cs] = (CT)CGD_DIVM(DivTh);
 #pragma unroll
     for (int q = 0; q < NT; ++q) {
       const R *Tx = s[10 + 3 * q] + row, *Ty = s[11 + 3 * q] + row;
       R DivTr = WI[0] * Tx[N * Jn] + WJ[0] * Ty[I];
 #pragma unroll
       for (int k = 1; k < N; ++k) DivTr = rsum2(DivTr, WI[k], Tx[k + N * Jn], WJ[k], Ty[I + N * k]);
-      out[(5 + q) * cs] = (double)CGD_DIVM(DivTr);
+      out[(5 + q) * cs] = (CT)CGD_DIVM(DivTr);
     }
   }
 }
@@ -252,13 +254,27 @@ __global__ void __launch_bounds__(256, 4) k_hypervisc1(const GP P, const double 
   hypervisc1_body<N, NT, R>(P, U, C, blockIdx.x, blockIdx.y);
 }
 
+// Contributions and the phase-1 cache: double, or float in the mixed form
+// (C32, a compile-time choice of every kernel that reads or writes them).
+template <bool C32>
+__device__ __forceinline__ double cload(const double *C, long long i)
+{
+  return C32 ? (double)reinterpret_cast<const float *>(C)[i] : C[i];
+}
+template <bool C32>
+__device__ __forceinline__ void cstore(double *C, long long i, double v)
+{
+  if (C32) reinterpret_cast<float *>(C)[i] = (float)v;
+  else C[i] = v;
+}
+
 // Sum the contributions of the element nodes sharing global DOF g at level l
 // (ascending element, node order) for every field.  Up to four contributors
 // (every cubed-sphere node) are loaded with independent loads.  WSPLIT (the
 // phase-2 tendency): a node's contribution to w at interface l is its upper
 // part (slot 3, level l) plus its lower part (slot NV, stored at level l),
 // zero at the top level.
-template <bool WSPLIT>
+template <bool WSPLIT, bool C32>
 __device__ __forceinline__ void gather_node(const GP &P, const double *__restrict__ C, int g, int l, size_t fstr,
                                             double *acc)
 {
@@ -272,14 +288,14 @@ __device__ __forceinline__ void gather_node(const GP &P, const double *__restric
     double wlo[4];
     if (WSPLIT) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) wlo[j] = j < nq && !wtop ? C[o[j] + P.NV * fstr] : 0.0;
+      for (int j = 0; j < 4; ++j) wlo[j] = j < nq && !wtop ? cload<C32>(C, o[j] + P.NV * fstr) : 0.0;
     }
 #pragma unroll
     for (int f = 0; f < MAXNV; ++f) {
       if (f < P.NV) {
         double x[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) x[j] = j < nq && !(WSPLIT && f == 3 && wtop) ? C[o[j] + f * fstr] : 0.0;
+        for (int j = 0; j < 4; ++j) x[j] = j < nq && !(WSPLIT && f == 3 && wtop) ? cload<C32>(C, o[j] + f * fstr) : 0.0;
         if (WSPLIT && f == 3) {
 #pragma unroll
           for (int j = 0; j < 4; ++j) x[j] = wtop ? 0.0 : x[j] + wlo[j];
@@ -298,8 +314,8 @@ __device__ __forceinline__ void gather_node(const GP &P, const double *__restric
         double a = 0.0;
         for (int q = q0; q < q1; ++q) {
           const long long o = P.inv_off[q] + l;
-          double x = C[o + f * fstr];
-          if (WSPLIT && f == 3) x = wtop ? 0.0 : x + C[o + P.NV * fstr];
+          double x = cload<C32>(C, o + f * fstr);
+          if (WSPLIT && f == 3) x = wtop ? 0.0 : x + cload<C32>(C, o + P.NV * fstr);
           a += x;
         }
         acc[f] = a;
@@ -312,7 +328,9 @@ __device__ __forceinline__ void gather_node(const GP &P, const double *__restric
 // Owner gather (DSS): out(l, g, f) = sum over contributors in ascending
 // (element, node) order.  Thread per (g, l), level fastest.
 // ---------------------------------------------------------------------------
-template <bool WSPLIT>
+// OUTC: the output is the phase-1 cache (stored like the contributions),
+// otherwise an FP64 tendency.
+template <bool WSPLIT, bool OUTC, bool C32>
 __device__ __forceinline__ void gather_body(const GP &P, const double *__restrict__ C, double *__restrict__ out,
                                             const long long tid)
 {
@@ -321,17 +339,21 @@ __device__ __forceinline__ void gather_body(const GP &P, const double *__restric
   const int g = (int)(tid / nz), l = (int)(tid % nz);
   const size_t fstr = (size_t)P.DoF * nz;
   double acc[MAXNV];
-  gather_node<WSPLIT>(P, C, g, l, fstr, acc);
+  gather_node<WSPLIT, C32>(P, C, g, l, fstr, acc);
 #pragma unroll
   for (int f = 0; f < MAXNV; ++f)
-    if (f < P.NV) out[l + (size_t)nz * (g + (size_t)P.NumG * f)] = acc[f];
+    if (f < P.NV) {
+      const long long o = l + (long long)nz * (g + (long long)P.NumG * f);
+      if (OUTC) cstore<C32>(out, o, acc[f]);
+      else out[o] = acc[f];
+    }
 }
 
-template <bool WSPLIT>
+template <bool WSPLIT, bool OUTC, bool C32>
 __global__ void __launch_bounds__(256) k_gather(const GP P, const double *__restrict__ C,
                                                 double *__restrict__ out)
 {
-  gather_body<WSPLIT>(P, C, out, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+  gather_body<WSPLIT, OUTC, C32>(P, C, out, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -397,7 +419,7 @@ __device__ __forceinline__ void jac_at(const GP &P, double RhoL, double RhoR, do
   jac_bands(P, RhoL, RhoR, RhoThL0, RhoThR0, dpdrhoth(P, RhoThL0), dpdrhoth(P, RhoThR0), dzL, dzR, jb);
 }
 
-template <int MODE>
+template <int MODE, bool C32>
 __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const int bx)
 {
   extern __shared__ double csm[];
@@ -427,7 +449,7 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
     if (MODE <= 2) {
       const size_t fstr = (size_t)P.DoF * nz;
       double gacc[MAXNV];
-      gather_node<true>(P, A.C, g, l, fstr, gacc);
+      gather_node<true, C32>(P, A.C, g, l, fstr, gacc);
 #pragma unroll
       for (int f = 0; f < MAXNV; ++f) {
         if (f >= NV) break;
@@ -606,10 +628,10 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
 #undef FV4
 }
 
-template <int MODE>
+template <int MODE, bool C32>
 __global__ void __launch_bounds__(32 * COL_WARPS, MODE == 2 ? 3 : 4) k_column(const GP P, const ColArgs A)
 {
-  column_body<MODE>(P, A, blockIdx.x);
+  column_body<MODE, C32>(P, A, blockIdx.x);
 }
 
 // Mixed form: the FP64 reference profile of pressure and theta, the

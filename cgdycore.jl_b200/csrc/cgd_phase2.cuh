@@ -122,9 +122,15 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
       cp_async8(o + O_D220 * os, mt + C_D22_0 * cs); cp_async8(o + O_D221 * os, mt + C_D22_1 * cs);
       cp_async8(o + O_J1 * os, mt + C_J1 * cs);
       cp_async8(o + O_FC * os, mt + C_FCOR * cs);
-      const double *T = T1 + (size_t)nz * g + lev;
+      if (MIX) {   // the mixed form's phase-1 cache is stored as float
+        const float *T = reinterpret_cast<const float *>(T1) + (size_t)nz * g + lev;
 #pragma unroll
-      for (int f = 0; f < 5 + NT; ++f) cp_async8(o + (O_T1 + f) * os, T + f * fs);
+        for (int f = 0; f < 5 + NT; ++f) o[(O_T1 + f) * os] = (double)T[f * fs];
+      } else {
+        const double *T = T1 + (size_t)nz * g + lev;
+#pragma unroll
+        for (int f = 0; f < 5 + NT; ++f) cp_async8(o + (O_T1 + f) * os, T + f * fs);
+      }
     }
     cp_async8(&PW(Q_RHO, p, ID), Ug);
     cp_async8(&PW(Q_CTH, p, ID), Ug + 4 * fs);   // rho*theta for now
@@ -571,15 +577,16 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
     }
   }
   // --- store the contributions
-  double *out = C + ((size_t)IF * P.NC * DoF + ID) * nz + lv;
-  out[0] = acc_r;
-  out[cs] = acc_u;
-  out[2 * cs] = acc_v;
-  out[3 * cs] = whi;
-  if (bot) out[(size_t)P.NV * cs - 1] = wlo;   // slot NV, one level down
-  out[4 * cs] = acc_th;
+  using CT = typename std::conditional<MIX, float, double>::type;   // stored contributions
+  CT *out = reinterpret_cast<CT *>(C) + ((size_t)IF * P.NC * DoF + ID) * nz + lv;
+  out[0] = (CT)acc_r;
+  out[cs] = (CT)acc_u;
+  out[2 * cs] = (CT)acc_v;
+  out[3 * cs] = (CT)whi;
+  if (bot) out[(size_t)P.NV * cs - 1] = (CT)wlo;   // slot NV, one level down
+  out[4 * cs] = (CT)acc_th;
 #pragma unroll
-  for (int q = 0; q < NT; ++q) out[(5 + q) * cs] = acc_tr[q];
+  for (int q = 0; q < NT; ++q) out[(5 + q) * cs] = (CT)acc_tr[q];
 #undef CGD_DIVR
 #undef FX
 #undef CGD_DIVW
