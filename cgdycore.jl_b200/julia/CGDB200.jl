@@ -55,9 +55,11 @@ function config(CG, Global, Phys; mixed = false, check_finite = false)
             Global.Model.HyperDCurl, Global.Model.HyperDGrad, Global.Model.HyperDDiv)
 end
 
-function handle(CG, Metric, Phys, Global)
+# mixed = true selects the mixed form (FP32 horizontal derivative sums and DSS
+# around an FP64 per-level reference; FP64 column solve).
+function handle(CG, Metric, Phys, Global; mixed = false)
   get!(HANDLES, Metric) do
-    cfg = Ref(config(CG, Global, Phys))
+    cfg = Ref(config(CG, Global, Phys; mixed = mixed))
     glob = Int64.(hostcopy(CG.Glob))
     DS, DW = hostcopy(CG.DS), hostcopy(CG.DW)
     dXdxI, J, X = hostcopy(Metric.dXdxI), hostcopy(Metric.J), hostcopy(Metric.X)
@@ -140,6 +142,32 @@ function JacSchurSolveNoAlloc!(k, v, U, dz, CG, Global, Phys, fac; stream = C_NU
     check(ccall((:cgd_jac_schur_solve_noalloc, libcgd), Cint,
                 (Ref{CgdConfig}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Cdouble, Ptr{Cvoid}),
                 cfg, dptr(U), dptr(dz), dptr(k), dptr(v), fac, stream), "cgd_jac_schur_solve_noalloc")
+  end
+end
+
+# Batched ensemble: member handles (same OrdPoly, NumTr, precision) advance
+# together, one CUDA graph per ensemble step (cgd_batch_step); states must be
+# CuArrays.
+mutable struct Batch
+  ptr::Ptr{Cvoid}
+  members::Vector{Handle}
+end
+
+function Batch(members::Vector{Handle}; autotune = true)
+  out = Ref{Ptr{Cvoid}}(C_NULL)
+  ptrs = [m.ptr for m in members]
+  check(ccall((:cgd_batch_create, libcgd), Cint, (Ptr{Ptr{Cvoid}}, Int32, Int32, Ref{Ptr{Cvoid}}),
+              ptrs, Int32(length(ptrs)), Int32(autotune ? 1 : 0), out), "cgd_batch_create")
+  b = Batch(out[], members)
+  finalizer(x -> ccall((:cgd_batch_destroy, libcgd), Cvoid, (Ptr{Cvoid},), x.ptr), b)
+  b
+end
+
+function step!(b::Batch, states, dts::Vector{Float64}; nsteps = 1)
+  ptrs = [dptr(u) for u in states]
+  GC.@preserve states begin
+    check(ccall((:cgd_batch_step, libcgd), Cint, (Ptr{Cvoid}, Ptr{Ptr{Float64}}, Ptr{Float64}, Int32),
+                b.ptr, ptrs, dts, Int32(nsteps)), "cgd_batch_step")
   end
 end
 
