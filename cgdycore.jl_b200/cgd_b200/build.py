@@ -25,7 +25,7 @@ import sys
 from ._lib import LIB_PATH, LIB_PATH_EXACT, PKG_DIR
 
 SRC = os.path.join(PKG_DIR, "csrc", "cgd_b200.cu")
-DEPS = [os.path.join(PKG_DIR, "csrc", f) for f in ("cgd_b200.cu", "cgd_kernels.cuh", "cgd_phase2.cuh", "cgd_batch.cuh")] + [
+DEPS = [os.path.join(PKG_DIR, "csrc", f) for f in ("cgd_b200.cu", "cgd_kernels.cuh", "cgd_phase2.cuh", "cgd_batch.cuh", "cgd_adjoint.cuh")] + [
     os.path.join(os.path.dirname(PKG_DIR), "include", f) for f in ("cgd_b200.h", "cgd_math.h")]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",

@@ -108,6 +108,14 @@ class Dycore:
         _lib.check(self._L.cgd_rhs(self.h, _ptr(U, self.shape), _ptr(F, self.shape, True)), "cgd_rhs")
         return F
 
+    def fcn_adjoint(self, U, LF, LU=None):
+        """(dF/dU)^T LF at U: the hand-written adjoint of the tendency (FP64, no
+        tracers)."""
+        LU = self.new_state() if LU is None else LU
+        _lib.check(self._L.cgd_rhs_adjoint(self.h, _ptr(U, self.shape), _ptr(LF, self.shape),
+                                           _ptr(LU, self.shape, True)), "cgd_rhs_adjoint")
+        return LU
+
     def hypervisc_phase1(self, U, Temp1=None):
         T = self.new_state() if Temp1 is None else Temp1
         _lib.check(self._L.cgd_hypervisc_phase1(self.h, _ptr(U, self.shape), _ptr(T, self.shape, True)),

@@ -9,6 +9,7 @@
 #include "cgd_kernels.cuh"
 #include "cgd_phase2.cuh"
 #include "cgd_batch.cuh"
+#include "cgd_adjoint.cuh"
 
 #include <cuda_runtime.h>
 #include <cmath>
@@ -47,6 +48,7 @@ struct cgd_handle {
   double *Ubuf = nullptr, *Fbuf = nullptr, *bands = nullptr, *part = nullptr, *scal = nullptr;
   double *jbg = nullptr;   // Jacobian bands of the current step, [8][NumG][nz-1]
   double *pres = nullptr, *pres_st = nullptr;   // pressure of the state and of the stage state
+  double *aLF = nullptr, *aLU = nullptr, *aLT1 = nullptr;   // adjoint buffers (allocated on first use)
   double *mmass = nullptr;
   int *flag = nullptr;
   GP gp{};
@@ -289,6 +291,24 @@ void ensure_ref(cgd_handle *h, const double *Ud)
   if (!h->mix || h->have_ref) return;
   k_refprof<<<h->nz, 256, 0, h->stream>>>(h->gp, Ud, h->pref, h->thref);
   h->have_ref = true;
+}
+
+// Reverse of the tendency (no tracers, FP64): phase 2 into the state and
+// cache adjoints, then phase 1 from the cache adjoint into the state adjoint.
+template <int N>
+int rhs_adjoint_launch(cgd_handle *h, const double *Ud, const double *LF, double *LU)
+{
+  using CF = AdjCfg<N>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_phase2_adj<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
+    attr = true;
+  }
+  dim3 grid((h->nz + CF::LC - 1) / CF::LC, h->NF);
+  k_phase2_adj<N><<<grid, CF::THREADS, CF::SMEM, h->stream>>>(h->gp, Ud, h->pres, h->T1, LF, LU, h->aLT1);
+  k_hypervisc1_adj<N><<<grid, CF::THREADS, 0, h->stream>>>(h->gp, Ud, h->aLT1, LU);
+  CK(cudaGetLastError());
+  return CGD_OK;
 }
 
 void free_graph(cgd_handle *h)
@@ -746,6 +766,44 @@ int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const do
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(st));
   return CGD_OK;
+}
+
+int cgd_rhs_adjoint(cgd_handle *h, const double *U, const double *LF, double *LU)
+{
+  if (!h || !U || !LF || !LU) return CGD_ERR_INVALID_ARG;
+  if (h->mix || h->NumTr != 0) return CGD_ERR_UNSUPPORTED;
+  const size_t S = (size_t)h->nz * h->NumG;
+  if (!h->aLF) {
+    int rc = dalloc(h, &h->aLF, S * h->NV);
+    if (!rc) rc = dalloc(h, &h->aLU, S * h->NV);
+    if (!rc) rc = dalloc(h, &h->aLT1, S * 5);
+    if (rc) return rc;
+  }
+  double *Ud;
+  int rc = stage_in(h, U, h->Ubuf, true, &Ud);
+  if (rc) return rc;
+  const double *LFd = LF;
+  if (!is_device_ptr(LF)) {
+    CK(cudaMemcpyAsync(h->aLF, LF, S * h->NV * 8, cudaMemcpyHostToDevice, h->stream));
+    LFd = h->aLF;
+  }
+  const bool udev = is_device_ptr(LU);
+  double *LUd = udev ? LU : h->aLU;
+  // forward quantities: the DSS'd phase-1 cache and the pressure
+  hv1(h, Ud, h->C);
+  gather(h, h->C, h->T1, false);
+  pressure(h, Ud, h->pres);
+  CK(cudaMemsetAsync(LUd, 0, S * h->NV * 8, h->stream));
+  CK(cudaMemsetAsync(h->aLT1, 0, S * 5 * 8, h->stream));
+  switch (h->N) {
+    case 2: rc = rhs_adjoint_launch<2>(h, Ud, LFd, LUd); break;
+    case 3: rc = rhs_adjoint_launch<3>(h, Ud, LFd, LUd); break;
+    case 4: rc = rhs_adjoint_launch<4>(h, Ud, LFd, LUd); break;
+    default: rc = rhs_adjoint_launch<5>(h, Ud, LFd, LUd); break;
+  }
+  if (rc) return rc;
+  if (!udev) CK(cudaMemcpyAsync(LU, LUd, S * h->NV * 8, cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
 }
 
 int cgd_get_stream(cgd_handle *h, void **stream)

@@ -95,6 +95,14 @@ int cgd_hypervisc_phase1(cgd_handle *h, const double *U, double *Temp1);
  * Replaces GPU.FcnGPU!(F,U,...,::CompressibleShallow) (src/GPU/FcnGPU.jl:552-968). */
 int cgd_rhs(cgd_handle *h, const double *U, double *F);
 
+/* Adjoint of the tendency: LU = (dF/dU)^T LF at the state U (all three
+ * (nz, NumG, NV)), FP64, no tracers (CGD_ERR_UNSUPPORTED otherwise).
+ * Hand-written reverse of the two phases and their direct-stiffness
+ * summations (the adjoint of the owner gather is a broadcast).  Sums are
+ * accumulated with atomics, so repeated calls agree to rounding, not bit for
+ * bit.  No counterpart in the reference (it has no adjoint). */
+int cgd_rhs_adjoint(cgd_handle *h, const double *U, const double *LF, double *LU);
+
 /* Vertical acoustic Jacobian bands from U, kept in the handle; optionally
  * copied to bands (4, 2, nz-1, NumG) = JRhoW, JWRho, JWRhoTh, JRhoThW.
  * Replaces DyCore.JacSchurGPU! (src/DyCore/JacSchur.jl:3-75). */
