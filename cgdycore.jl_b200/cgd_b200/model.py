@@ -116,6 +116,43 @@ class Dycore:
                                            _ptr(LU, self.shape, True)), "cgd_rhs_adjoint")
         return LU
 
+    def ros_step_adjoint(self, U0, Lout, dt, Lin=None):
+        """(dU1/dU0)^T Lout for one Rosenbrock-W step U1 = step(U0, dt): the
+        hand-written adjoint of the step (FP64, no tracers).  U0 is left
+        unchanged."""
+        Lin = self.new_state() if Lin is None else Lin
+        _lib.check(self._L.cgd_ros_step_adjoint(self.h, _ptr(U0, self.shape), _ptr(Lout, self.shape),
+                                                _ptr(Lin, self.shape, True), float(dt)),
+                   "cgd_ros_step_adjoint")
+        return Lin
+
+    def steps_adjoint(self, U0, Lout, dt, nsteps, every=None):
+        """(dU_n/dU0)^T Lout for n = nsteps Rosenbrock-W steps from U0, by
+        chaining ros_step_adjoint backwards over checkpoints: the forward run
+        keeps the state every `every` steps (default about sqrt(nsteps)), and
+        the reverse sweep recomputes each segment's states from its
+        checkpoint, so at most nsteps/every + every states are held."""
+        nsteps = int(nsteps)
+        every = max(1, int(round(nsteps ** 0.5))) if every is None else max(1, int(every))
+        checkpoints = {0: np.array(U0, order="F", copy=True)}
+        V = checkpoints[0].copy(order="F")
+        for s in range(1, nsteps):
+            self.time_stepper(V, dt, 1)
+            if s % every == 0:
+                checkpoints[s] = V.copy(order="F")
+        L = np.array(Lout, order="F", copy=True)
+        top = nsteps
+        for start in sorted(checkpoints, reverse=True):
+            seg = [checkpoints[start]]
+            for _ in range(start + 1, top):
+                W = seg[-1].copy(order="F")
+                self.time_stepper(W, dt, 1)
+                seg.append(W)
+            for W in reversed(seg):
+                L = self.ros_step_adjoint(W, L, dt)
+            top = start
+        return L
+
     def hypervisc_phase1(self, U, Temp1=None):
         T = self.new_state() if Temp1 is None else Temp1
         _lib.check(self._L.cgd_hypervisc_phase1(self.h, _ptr(U, self.shape), _ptr(T, self.shape, True)),

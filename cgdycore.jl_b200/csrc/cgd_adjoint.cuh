@@ -693,4 +693,187 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_hypervisc1_adj(const GP P, c
 #undef SC
 }
 
+
+// out = a x + b y + c z, elementwise (null pointers count as zero)
+__global__ void __launch_bounds__(256) k_lincomb(long long n, double *__restrict__ out, double a,
+                                                 const double *__restrict__ x, double b, const double *__restrict__ y,
+                                                 double c, const double *__restrict__ z)
+{
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  if (x) s += a * x[i];
+  if (y) s += b * y[i];
+  if (z) s += c * z[i];
+  out[i] = s;
+}
+
+// Reverse of the column Schur solve of one stage, k = L(bands) r with
+// r = F + cA k1 + cB k2 (TriDiagKernel!, SchurSolveFKernel!, triSolve!,
+// SchurSolveBKernel!: src/Integration/SchurSolve.jl:1-114).  Given mu, the
+// adjoint of k, writes AR, the adjoint of r, and adds the adjoint that flows
+// through the Jacobian bands (JacSchur.jl:40-73) into LV (fields rho and
+// rho*theta of the step's initial state).  One warp per column; the forward
+// and the transposed tridiagonal solves run on the warp's first lane.
+constexpr int CA_ARR = 25;   // per-warp arrays of nz entries
+
+__global__ void __launch_bounds__(32 * COL_WARPS) k_column_adj(const GP P, const double *__restrict__ mu,
+                                                              const double *__restrict__ F,
+                                                              const double *__restrict__ k1, double cA,
+                                                              const double *__restrict__ k2, double cB,
+                                                              const double *__restrict__ jbg,
+                                                              const double *__restrict__ Vn, double fac,
+                                                              double *__restrict__ AR, double *__restrict__ LV)
+{
+  extern __shared__ double csm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = blockIdx.x * COL_WARPS + warp;
+  const int nz = P.nz, n = nz - 1, NV = P.NV, NumG = P.NumG;
+  if (g >= NumG) return;   // warp-uniform; this kernel synchronises within warps only
+  const int LS = nz;
+  double *sw = csm + (size_t)warp * CA_ARR * LS;
+  double *r0 = sw, *r3 = sw + LS, *r4 = sw + 2 * LS;
+  double *jb = sw + 3 * LS;          // [8][nz]
+  double *tri = sw + 11 * LS;        // [3][nz]
+  double *x = sw + 14 * LS, *b = sw + 15 * LS, *y = sw + 16 * LS, *ax = sw + 17 * LS;
+  double *av0 = sw + 18 * LS, *av4 = sw + 19 * LS;
+  double *accL0 = sw + 20 * LS, *accL4 = sw + 21 * LS, *accR0 = sw + 22 * LS, *accR4 = sw + 23 * LS;
+  double *cp = sw + 24 * LS;         // the transposed sweep's modified super-diagonal
+  const size_t fs = (size_t)nz * NumG;
+  const size_t js = (size_t)NumG * n;
+#define JB(arr, r, i) jb[((arr) * 2 + (r)) * LS + (i)]
+  // 1. the stage's right-hand side r; fields outside the Schur system: AR = fac mu
+  for (int l = lane; l < nz; l += 32) {
+    const size_t o0 = l + (size_t)nz * g;
+#pragma unroll
+    for (int f = 0; f < MAXNV; ++f) {
+      if (f >= NV) break;
+      const size_t o = o0 + f * fs;
+      if (f == 0 || f == 3 || f == 4) {
+        double r = F[o];
+        if (k1) r = r + cA * k1[o];
+        if (k2) r = r + cB * k2[o];
+        (f == 0 ? r0 : f == 3 ? r3 : r4)[l] = r;
+      } else {
+        AR[o] = fac * mu[o];
+      }
+    }
+    av0[l] = fac * mu[o0];
+    av4[l] = fac * mu[o0 + 4 * fs];
+    if (l < n)
+      for (int rr = 0; rr < 8; ++rr) jb[rr * LS + l] = jbg[rr * js + (size_t)g * n + l];
+  }
+  __syncwarp();
+  const double invfac = 1.0 / fac, invfac2 = invfac / fac;
+  for (int l = lane; l < n; l += 32) {
+    tri[LS + l] = invfac2 - JB(1, 1, l) * JB(0, 0, l) - JB(1, 0, l) * JB(0, 1, l) - JB(2, 1, l) * JB(3, 0, l) -
+                  JB(2, 0, l) * JB(3, 1, l);
+    tri[l] = l == 0 ? 0.0 : -JB(1, 0, l - 1) * JB(0, 0, l) - JB(2, 0, l - 1) * JB(3, 0, l);
+    tri[2 * LS + l] = l == n - 1 ? 0.0 : -JB(1, 1, l + 1) * JB(0, 1, l) - JB(2, 1, l + 1) * JB(3, 1, l);
+    b[l] = r3[l] / fac + JB(1, 1, l) * r0[l] + JB(1, 0, l) * r0[l + 1] + JB(2, 1, l) * r4[l] + JB(2, 0, l) * r4[l + 1];
+  }
+  __syncwarp();
+  // 2. forward solve T x = b (the same sweep as the forward kernel)
+  if (lane == 0) {
+    x[0] = tri[LS];
+    for (int i = 0; i < n - 1; ++i) {
+      const double m = tri[2 * LS + i] / x[i];
+      x[i + 1] = tri[LS + i + 1] - m * tri[i + 1];
+      b[i + 1] = b[i + 1] - m * b[i];
+    }
+    x[n - 1] = b[n - 1] / x[n - 1];
+    for (int i = n - 2; i >= 0; --i) x[i] = (b[i] - tri[i + 1] * x[i + 1]) / x[i];
+  }
+  __syncwarp();
+  // 3. reverse of SchurSolveB: v0'(l) = r0(l) + JB(0,0,l) x(l) + JB(0,1,l-1) x(l-1), v4' likewise;
+  //    kw = x
+  for (int l = lane; l < n; l += 32) {
+    ax[l] = mu[l + (size_t)nz * g + 3 * fs] + JB(0, 0, l) * av0[l] + JB(3, 0, l) * av4[l] +
+            JB(0, 1, l) * av0[l + 1] + JB(3, 1, l) * av4[l + 1];
+  }
+  __syncwarp();
+  // 4. The forward sweep solves M x = b with M(i,i) = t1(i), M(i+1,i) = t2(i),
+  //    M(i,i+1) = t0(i+1) (the reference's triSolve!).  Transposed solve
+  //    M^T y = ax: row i is t0(i) y(i-1) + t1(i) y(i) + t2(i) y(i+1).
+  if (lane == 0) {
+    double bb = tri[LS];
+    cp[0] = (n > 1 ? tri[2 * LS] : 0.0) / bb;
+    y[0] = ax[0] / bb;
+    for (int i = 1; i < n; ++i) {
+      const double a = tri[i];
+      bb = tri[LS + i] - a * cp[i - 1];
+      cp[i] = (i + 1 < n ? tri[2 * LS + i] : 0.0) / bb;
+      y[i] = (ax[i] - a * y[i - 1]) / bb;
+    }
+    for (int i = n - 2; i >= 0; --i) y[i] = y[i] - cp[i] * y[i + 1];
+  }
+  __syncwarp();
+  // 5. band adjoints (TriDiag, SchurSolveF, SchurSolveB) and the adjoint of r
+  for (int l = lane; l < nz; l += 32) {
+    const size_t o0 = l + (size_t)nz * g;
+    double ar0 = av0[l], ar4 = av4[l];
+    if (l < n) { ar0 += JB(1, 1, l) * y[l]; ar4 += JB(2, 1, l) * y[l]; }
+    if (l > 0) { ar0 += JB(1, 0, l - 1) * y[l - 1]; ar4 += JB(2, 0, l - 1) * y[l - 1]; }
+    AR[o0] = ar0;
+    AR[o0 + 3 * fs] = l < n ? y[l] / fac : 0.0;
+    AR[o0 + 4 * fs] = ar4;
+    accL0[l] = accL4[l] = accR0[l] = accR4[l] = 0.0;
+  }
+  __syncwarp();
+  for (int l = lane; l < n; l += 32) {
+    double a[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};   // a[arr][r] = adjoint of JB(arr, r, l)
+    // adjoint of M(i,j) is -y(i) x(j)
+    const double at1 = -y[l] * x[l];
+    const double at0 = l > 0 ? -y[l - 1] * x[l] : 0.0;              // t0(l) = M(l-1,l)
+    const double at0n = l + 1 < n ? -y[l] * x[l + 1] : 0.0;         // t0(l+1) = M(l,l+1)
+    const double at2 = l + 1 < n ? -y[l + 1] * x[l] : 0.0;          // t2(l) = M(l+1,l)
+    const double at2p = l > 0 ? -y[l] * x[l - 1] : 0.0;             // t2(l-1) = M(l,l-1)
+    // t1(l)
+    a[1][1] += -JB(0, 0, l) * at1; a[0][0] += -JB(1, 1, l) * at1;
+    a[1][0] += -JB(0, 1, l) * at1; a[0][1] += -JB(1, 0, l) * at1;
+    a[2][1] += -JB(3, 0, l) * at1; a[3][0] += -JB(2, 1, l) * at1;
+    a[2][0] += -JB(3, 1, l) * at1; a[3][1] += -JB(2, 0, l) * at1;
+    // t0(l) = -JB(1,0,l-1) JB(0,0,l) - JB(2,0,l-1) JB(3,0,l)
+    if (l > 0) { a[0][0] += -JB(1, 0, l - 1) * at0; a[3][0] += -JB(2, 0, l - 1) * at0; }
+    // t0(l+1) = -JB(1,0,l) JB(0,0,l+1) - JB(2,0,l) JB(3,0,l+1)
+    if (l + 1 < n) { a[1][0] += -JB(0, 0, l + 1) * at0n; a[2][0] += -JB(3, 0, l + 1) * at0n; }
+    // t2(l) = -JB(1,1,l+1) JB(0,1,l) - JB(2,1,l+1) JB(3,1,l)
+    if (l + 1 < n) { a[0][1] += -JB(1, 1, l + 1) * at2; a[3][1] += -JB(2, 1, l + 1) * at2; }
+    // t2(l-1) = -JB(1,1,l) JB(0,1,l-1) - JB(2,1,l) JB(3,1,l-1)
+    if (l > 0) { a[1][1] += -JB(0, 1, l - 1) * at2p; a[2][1] += -JB(3, 1, l - 1) * at2p; }
+    // SchurSolveF: v3new(l) = r3/fac + JB(1,1,l) r0(l) + JB(1,0,l) r0(l+1) + JB(2,1,l) r4(l) + JB(2,0,l) r4(l+1)
+    a[1][1] += y[l] * r0[l]; a[1][0] += y[l] * r0[l + 1];
+    a[2][1] += y[l] * r4[l]; a[2][0] += y[l] * r4[l + 1];
+    // SchurSolveB: JB(0,0,l) x(l) in v0'(l), JB(0,1,l) x(l) in v0'(l+1), JB(3,.) in v4'
+    a[0][0] += av0[l] * x[l]; a[0][1] += av0[l + 1] * x[l];
+    a[3][0] += av4[l] * x[l]; a[3][1] += av4[l + 1] * x[l];
+    // bands of interface l from rho, rho*theta at l, l+1 (JacSchurKernel!)
+    const double *V0 = Vn + (size_t)nz * g;
+    const double RhoL = V0[l], RhoR = V0[l + 1], ThL = V0[l + 4 * fs] + 0.0, ThR = V0[l + 1 + 4 * fs] + 0.0;
+    const double dzL = P.dz[l + (size_t)nz * g], dzR = P.dz[l + 1 + (size_t)nz * g], dzs = dzL + dzR;
+    const double RhoF = (RhoL * dzL + RhoR * dzR) / dzs;
+    const double ex = P.kappa / (1.0 - P.kappa);
+    const double dPL = dpdrhoth(P, ThL), dPR = dpdrhoth(P, ThR);
+    const double h = 0.5 * dzs;
+    // jb0 = -RhoF/dzL, jb1 = RhoF/dzR, jb4 = -dPR/RhoF/h, jb5 = dPL/RhoF/h,
+    // jb2 = -g dzR/RhoF/dzs, jb3 = -g dzL/RhoF/dzs, jb6 = -RhoThF/dzL, jb7 = RhoThF/dzR
+    const double aRhoF = -a[0][0] / dzL + a[0][1] / dzR + a[2][0] * dPR / (RhoF * RhoF * h) -
+                         a[2][1] * dPL / (RhoF * RhoF * h) + a[1][0] * P.Grav * dzR / (RhoF * RhoF * dzs) +
+                         a[1][1] * P.Grav * dzL / (RhoF * RhoF * dzs);
+    const double adPR = -a[2][0] / (RhoF * h), adPL = a[2][1] / (RhoF * h);
+    const double aThF = -a[3][0] / dzL + a[3][1] / dzR;
+    accL0[l] = aRhoF * dzL / dzs;
+    accR0[l + 1] = aRhoF * dzR / dzs;
+    accL4[l] = aThF * dzL / dzs + adPL * ex * dPL / ThL;
+    accR4[l + 1] = aThF * dzR / dzs + adPR * ex * dPR / ThR;
+  }
+  __syncwarp();
+  for (int l = lane; l < nz; l += 32) {
+    const size_t o0 = l + (size_t)nz * g;
+    LV[o0] += accL0[l] + accR0[l];
+    LV[o0 + 4 * fs] += accL4[l] + accR4[l];
+  }
+#undef JB
+}
+
 }  // namespace cgd

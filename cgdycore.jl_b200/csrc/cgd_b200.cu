@@ -49,6 +49,8 @@ struct cgd_handle {
   double *jbg = nullptr;   // Jacobian bands of the current step, [8][NumG][nz-1]
   double *pres = nullptr, *pres_st = nullptr;   // pressure of the state and of the stage state
   double *aLF = nullptr, *aLU = nullptr, *aLT1 = nullptr;   // adjoint buffers (allocated on first use)
+  // step adjoint workspace: stage states, stage tendencies, k adjoints, ...
+  double *sV2 = nullptr, *sV3 = nullptr, *sF[3] = {}, *aLk[3] = {}, *aAR = nullptr, *aLV = nullptr, *aLt = nullptr;
   double *mmass = nullptr;
   int *flag = nullptr;
   GP gp{};
@@ -768,17 +770,147 @@ int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const do
   return CGD_OK;
 }
 
-int cgd_rhs_adjoint(cgd_handle *h, const double *U, const double *LF, double *LU)
+}  // extern "C"
+
+namespace {
+
+int adjoint_alloc(cgd_handle *h, bool step)
+{
+  const size_t S = (size_t)h->nz * h->NumG, SV = S * h->NV;
+  int rc = CGD_OK;
+  if (!h->aLF) {
+    rc = dalloc(h, &h->aLF, SV);
+    if (!rc) rc = dalloc(h, &h->aLU, SV);
+    if (!rc) rc = dalloc(h, &h->aLT1, S * 5);
+  }
+  if (!rc && step && !h->sV2) {
+    rc = dalloc(h, &h->sV2, SV);
+    if (!rc) rc = dalloc(h, &h->sV3, SV);
+    for (int i = 0; i < 3 && !rc; ++i) rc = dalloc(h, &h->sF[i], SV);
+    for (int i = 0; i < 3 && !rc; ++i) rc = dalloc(h, &h->aLk[i], SV);
+    if (!rc) rc = dalloc(h, &h->aAR, SV);
+    if (!rc) rc = dalloc(h, &h->aLV, SV);
+    if (!rc) rc = dalloc(h, &h->aLt, SV);
+  }
+  return rc;
+}
+
+// LU = (dF/dU)^T LF at the device state Ud (LU zeroed here)
+int rhs_adjoint_core(cgd_handle *h, const double *Ud, const double *LFd, double *LUd)
+{
+  const size_t S = (size_t)h->nz * h->NumG;
+  hv1(h, Ud, h->C);
+  gather(h, h->C, h->T1, false);
+  pressure(h, Ud, h->pres);
+  CK(cudaMemsetAsync(LUd, 0, S * h->NV * 8, h->stream));
+  CK(cudaMemsetAsync(h->aLT1, 0, S * 5 * 8, h->stream));
+  switch (h->N) {
+    case 2: return rhs_adjoint_launch<2>(h, Ud, LFd, LUd);
+    case 3: return rhs_adjoint_launch<3>(h, Ud, LFd, LUd);
+    case 4: return rhs_adjoint_launch<4>(h, Ud, LFd, LUd);
+    default: return rhs_adjoint_launch<5>(h, Ud, LFd, LUd);
+  }
+}
+
+void lincomb(cgd_handle *h, double *out, double a, const double *x, double b = 0.0, const double *y = nullptr,
+             double c = 0.0, const double *z = nullptr)
+{
+  const long long n = (long long)h->nz * h->NumG * h->NV;
+  k_lincomb<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(n, out, a, x, b, y, c, z);
+}
+
+int column_adj(cgd_handle *h, const double *mu, const double *F, const double *k1, double cA, const double *k2,
+               double cB, const double *Vn, double fac, double *AR, double *LV)
+{
+  CK(cudaFuncSetAttribute(k_column_adj, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          COL_WARPS * CA_ARR * 64 * (int)sizeof(double)));
+  const size_t smem = (size_t)COL_WARPS * CA_ARR * h->nz * sizeof(double);
+  k_column_adj<<<(h->NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, h->stream>>>(
+      h->gp, mu, F, k1, cA, k2, cB, h->jbg, Vn, fac, AR, LV);
+  CK(cudaGetLastError());
+  return CGD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cgd_ros_step_adjoint(cgd_handle *h, const double *U0, const double *Lout, double *Lin, double dt)
+{
+  if (!h || !U0 || !Lout || !Lin || !(dt > 0)) return CGD_ERR_INVALID_ARG;
+  if (h->mix || h->NumTr != 0) return CGD_ERR_UNSUPPORTED;
+  int rc = adjoint_alloc(h, true);
+  if (rc) return rc;
+  const size_t SV = (size_t)h->nz * h->NumG * h->NV;
+  double *Ud;
+  rc = stage_in(h, U0, h->Ubuf, true, &Ud);
+  if (rc) return rc;
+  const double *L = Lout;
+  if (!is_device_ptr(Lout)) {
+    CK(cudaMemcpyAsync(h->aLF, Lout, SV * 8, cudaMemcpyHostToDevice, h->stream));
+    L = h->aLF;
+  }
+  const RK &rk = h->rk;
+  const double fac = dt * rk.gamma;
+  // forward replay of the step, keeping the stage states and tendencies
+  ColArgs a{};
+  a.Vn = Ud;
+  a.k1 = h->k1;
+  a.k2 = h->k2;
+  a.dt = dt;
+  a.fac = fac;
+  a.rk = rk;
+  a.C = h->C;
+  a.jbg = h->jbg;
+  const double *Vs[3] = {Ud, h->sV2, h->sV3};
+  for (int st = 0; st < 3; ++st) {
+    const double *V = Vs[st];
+    hv1(h, V, h->C);
+    gather(h, h->C, h->T1, false);
+    pressure(h, V, h->pres);
+    phase2(h, V, h->pres, h->T1, h->C);
+    gather(h, h->C, h->sF[st], true);
+    if (st == 0) {
+      a.kout = h->k1; a.Vout = h->Vst;
+      column<0>(h, a);
+      CK(cudaMemcpyAsync(h->sV2, h->Vst, SV * 8, cudaMemcpyDeviceToDevice, h->stream));
+    } else if (st == 1) {
+      a.kout = h->k2; a.Vout = h->Vst;
+      column<1>(h, a);
+      CK(cudaMemcpyAsync(h->sV3, h->Vst, SV * 8, cudaMemcpyDeviceToDevice, h->stream));
+    }
+  }
+  // reverse: U1 = U0 + sum m_i k_i; k_i = L (F(V_i) + sum_j c_ij/dt k_j); V_i = U0 + sum_j a_ij k_j
+  for (int i = 0; i < 3; ++i) lincomb(h, h->aLk[i], rk.m[i], L);
+  lincomb(h, h->aLV, 1.0, L);
+  for (int st = 2; st >= 0; --st) {
+    const double cA = st >= 1 ? rk.c[st][0] / dt : 0.0, cB = st == 2 ? rk.c[st][1] / dt : 0.0;
+    rc = column_adj(h, h->aLk[st], h->sF[st], st >= 1 ? h->k1 : nullptr, cA, st == 2 ? h->k2 : nullptr, cB, Ud,
+                    fac, h->aAR, h->aLV);
+    if (rc) return rc;
+    rc = rhs_adjoint_core(h, Vs[st], h->aAR, h->aLt);
+    if (rc) return rc;
+    // r_st = F(V_st) + c_st0/dt k1 + c_st1/dt k2; V_st = U0 + a_st0 k1 + a_st1 k2
+    if (st >= 1) lincomb(h, h->aLk[0], 1.0, h->aLk[0], cA, h->aAR, rk.a[st][0], h->aLt);
+    if (st == 2) lincomb(h, h->aLk[1], 1.0, h->aLk[1], cB, h->aAR, rk.a[st][1], h->aLt);
+    lincomb(h, h->aLV, 1.0, h->aLV, 1.0, h->aLt);
+  }
+  if (is_device_ptr(Lin)) CK(cudaMemcpyAsync(Lin, h->aLV, SV * 8, cudaMemcpyDeviceToDevice, h->stream));
+  else CK(cudaMemcpyAsync(Lin, h->aLV, SV * 8, cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
+}
+
+}  // extern "C"
+
+namespace {
+
+int cgd_rhs_adjoint_impl(cgd_handle *h, const double *U, const double *LF, double *LU)
 {
   if (!h || !U || !LF || !LU) return CGD_ERR_INVALID_ARG;
   if (h->mix || h->NumTr != 0) return CGD_ERR_UNSUPPORTED;
   const size_t S = (size_t)h->nz * h->NumG;
-  if (!h->aLF) {
-    int rc = dalloc(h, &h->aLF, S * h->NV);
-    if (!rc) rc = dalloc(h, &h->aLU, S * h->NV);
-    if (!rc) rc = dalloc(h, &h->aLT1, S * 5);
-    if (rc) return rc;
-  }
+  int arc = adjoint_alloc(h, false);
+  if (arc) return arc;
   double *Ud;
   int rc = stage_in(h, U, h->Ubuf, true, &Ud);
   if (rc) return rc;
@@ -789,21 +921,18 @@ int cgd_rhs_adjoint(cgd_handle *h, const double *U, const double *LF, double *LU
   }
   const bool udev = is_device_ptr(LU);
   double *LUd = udev ? LU : h->aLU;
-  // forward quantities: the DSS'd phase-1 cache and the pressure
-  hv1(h, Ud, h->C);
-  gather(h, h->C, h->T1, false);
-  pressure(h, Ud, h->pres);
-  CK(cudaMemsetAsync(LUd, 0, S * h->NV * 8, h->stream));
-  CK(cudaMemsetAsync(h->aLT1, 0, S * 5 * 8, h->stream));
-  switch (h->N) {
-    case 2: rc = rhs_adjoint_launch<2>(h, Ud, LFd, LUd); break;
-    case 3: rc = rhs_adjoint_launch<3>(h, Ud, LFd, LUd); break;
-    case 4: rc = rhs_adjoint_launch<4>(h, Ud, LFd, LUd); break;
-    default: rc = rhs_adjoint_launch<5>(h, Ud, LFd, LUd); break;
-  }
+  rc = rhs_adjoint_core(h, Ud, LFd, LUd);
   if (rc) return rc;
   if (!udev) CK(cudaMemcpyAsync(LU, LUd, S * h->NV * 8, cudaMemcpyDeviceToHost, h->stream));
   return finish(h);
+}
+
+}  // namespace
+
+extern "C" {
+int cgd_rhs_adjoint(cgd_handle *h, const double *U, const double *LF, double *LU)
+{
+  return cgd_rhs_adjoint_impl(h, U, LF, LU);
 }
 
 int cgd_get_stream(cgd_handle *h, void **stream)

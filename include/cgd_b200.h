@@ -120,6 +120,16 @@ int cgd_schur_solve(cgd_handle *h, double *k, double *v, double fac);
  * inside TimeStepper! (src/Integration/TimeStepper.jl:103-124). */
 int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps);
 
+/* Adjoint of one Rosenbrock-W step U1 = step(U0, dt): Lin = (dU1/dU0)^T Lout
+ * (all three (nz, NumG, NV)), FP64, no tracers (CGD_ERR_UNSUPPORTED
+ * otherwise).  Replays the forward step from U0 (the three stage states and
+ * tendencies, the bands), then runs the stages in reverse: the transposed
+ * column Schur solve (including the derivative of the Jacobian bands with
+ * respect to U0), the tendency adjoint at the stage state, and the stage
+ * combinations.  Multi-step gradients chain this call over checkpointed
+ * states.  No counterpart in the reference (it has no adjoint). */
+int cgd_ros_step_adjoint(cgd_handle *h, const double *U0, const double *Lout, double *Lin, double dt);
+
 /* sum(rho * MMass) over all DOFs, reduced in FP64 on the device (MMass is
  * the caller's lumped quadrature mass (nz, NumG)).
  * Replaces Parallels.GlobalIntegral (src/Parallels/Exchange.jl:1163-1166). */
