@@ -58,14 +58,14 @@ __device__ __forceinline__ void upwind_adj(double cLL, double cL, double cR, dou
   aL = (1.0 - phi1) * acFL;
   aR = phi1 * acFL;
   const double ar1 = dphi1 * (cR - cL) * acFL;
-  const double an1 = ar1 / den1, ad1 = -ar1 * num1 / (den1 * den1);
+  const double an1 = ar1 / den1, ad1 = -an1 * r1;
   aL += an1 - ad1;
   aLL -= an1;
   aR += ad1;
   aR += (1.0 - phi2) * acFR;
   aL += phi2 * acFR;
   const double ar2 = dphi2 * (cL - cR) * acFR;
-  const double an2 = ar2 / den2, ad2 = -ar2 * num2 / (den2 * den2);
+  const double an2 = ar2 / den2, ad2 = -an2 * r2;
   aR += an2 - ad2;
   aRR -= an2;
   aL += ad2;
@@ -74,7 +74,7 @@ __device__ __forceinline__ void upwind_adj(double cLL, double cL, double cR, dou
 
 // staged quantities of the adjoint kernels
 enum {
-  A_RHO = 0, A_U, A_V, A_W, A_TH, A_RTH, A_P, A_D310, A_D311, A_D320, A_D321, A_D330, A_D331, A_J0, A_M0, A_M1,
+  A_RHO = 0, A_U, A_V, A_W, A_TH, A_IR, A_DPD, A_P, A_D310, A_D311, A_D320, A_D321, A_D330, A_D331, A_J0, A_M0, A_M1,
   A_NQ
 };
 enum { B_D110 = 0, B_D111, B_D120, B_D121, B_D210, B_D211, B_D220, B_D221, B_J1, B_FC, B_C1, B_NQ = B_C1 + 5 };
@@ -112,7 +112,7 @@ __device__ __forceinline__ void adj_stage(const GP &P, const double *__restrict_
 #define AWs(q) pw[((q) * RP + p) * DoF + ID]
     const double rho = Ug[0], rth = Ug[4 * fs];
     AWs(A_RHO) = rho;
-    AWs(A_RTH) = rth;
+    AWs(A_IR) = 1.0 / rho;
     AWs(A_TH) = rth / rho;
     if (p >= 2 && p <= LC + 1) {
       double *o = ow + (size_t)(p - 2) * DoF + ID;
@@ -138,7 +138,9 @@ __device__ __forceinline__ void adj_stage(const GP &P, const double *__restrict_
     AWs(A_J0) = mt[C_J0 * cs];
     AWs(A_M0) = P.M[lev + (size_t)nz * g];
     AWs(A_M1) = P.M[lev + (size_t)nz * (g + (size_t)NumG)];
-    AWs(A_P) = Pr ? Pr[lev + (size_t)nz * g] : 0.0;
+    const double pr = Pr ? Pr[lev + (size_t)nz * g] : 0.0;
+    AWs(A_P) = pr;
+    AWs(A_DPD) = pr / ((1.0 - P.kappa) * rth);   // dp/d(rho*theta)
 #undef AWs
   }
 }
@@ -146,8 +148,10 @@ __device__ __forceinline__ void adj_stage(const GP &P, const double *__restrict_
 // Reverse of phase 2 (no tracers): LU += (d phase2 / d U)^T lambda and
 // LT1 += (d phase2 / d T1)^T lambda, lambda being lambda_F broadcast to the
 // element nodes.  One CTA per (element, chunk of LC levels), one warp per level.
+// Two blocks per SM (128 registers, a few hundred bytes of spills) run this
+// latency-bound kernel faster than one block at its natural 198 registers.
 template <int N>
-__global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const double *__restrict__ U,
+__global__ void __launch_bounds__(32 * ADJ_WARPS, 2) k_phase2_adj(const GP P, const double *__restrict__ U,
                                                               const double *__restrict__ Pr,
                                                               const double *__restrict__ T1,
                                                               const double *__restrict__ LF, double *__restrict__ LU,
@@ -197,15 +201,14 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const
   // adjoint of theta at level lev of this node -> rho*theta and rho
   auto add_theta = [&](int lev, double ath) {
     const int pl = lev - (L0 - 2);
-    const double rho = AW(A_RHO, pl, ID);
-    ADDU(4, lev, ath / rho);
-    ADDU(0, lev, -ath * AW(A_TH, pl, ID) / rho);
+    const double q = ath * AW(A_IR, pl, ID);
+    ADDU(4, lev, q);
+    ADDU(0, lev, -q * AW(A_TH, pl, ID));
   };
   // adjoint of the pressure at level lev of this node -> rho*theta
-  const double eP = 1.0 / (1.0 - P.kappa);
   auto add_p = [&](int lev, double ap) {
     const int pl = lev - (L0 - 2);
-    ADDU(4, lev, ap * eP * AW(A_P, pl, ID) / AW(A_RTH, pl, ID));
+    ADDU(4, lev, ap * AW(A_DPD, pl, ID));
   };
 
   // ---------------- forward quantities of this node ----------------
@@ -215,6 +218,7 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const
   double e310 = 0, e311 = 0, e320 = 0, e321 = 0, e330 = 1, e331 = 1;
   double lam_r = 0, lam_u = 0, lam_v = 0, lam_th = 0, lam_whi = 0, lam_wlo = 0;
   double GDx = 0, GDy = 0, U1 = 0, U2 = 0, V1 = 0, V2 = 0, W1 = 0, W2 = 0, Gradu = 0, Gradv = 0;
+  double iMC = 1, iJs = 1, irho = 1, i33 = 0.5;   // reciprocals used throughout
   if (act) {
     rho = AW(A_RHO, p0, ID); u = AW(A_U, p0, ID); v = AW(A_V, p0, ID); wh = AW(A_W, p0, ID); th = AW(A_TH, p0, ID);
     e310 = AW(A_D310, p0, ID); e311 = AW(A_D311, p0, ID); e320 = AW(A_D320, p0, ID);
@@ -223,6 +227,10 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const
     M0 = AW(A_M0, p0, ID); M1 = AW(A_M1, p0, ID);
     MC = M0 + M1;
     Js = J0 + J1;
+    iMC = 1.0 / MC;
+    iJs = 1.0 / Js;
+    irho = 1.0 / rho;
+    i33 = 1.0 / (e330 + e331);
     wl = wl_at(ID);
     d110 = BW(B_D110, ID); d111 = BW(B_D111, ID); d120 = BW(B_D120, ID); d121 = BW(B_D121, ID);
     d210 = BW(B_D210, ID); d211 = BW(B_D211, ID); d220 = BW(B_D220, ID); d221 = BW(B_D221, ID);
@@ -240,9 +248,9 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const
       DXp += DI[k] * AW(A_P, p0, k + N * Jn);
       DYp += DJ[k] * AW(A_P, p0, I + N * k);
     }
-    GDx = (d11 * Dxc + d21 * Dyc) / Js;
-    GDy = (d12 * Dxc + d22 * Dyc) / Js;
-    const double GZg = -P.Grav * rho * Js / (e330 + e331);
+    GDx = (d11 * Dxc + d21 * Dyc) * iJs;
+    GDy = (d12 * Dxc + d22 * Dyc) * iJs;
+    const double GZg = -P.Grav * rho * Js * i33;
     Gradu = d11 * DXp + d21 * DYp + GZg * (e310 + e311);
     Gradv = d12 * DXp + d22 * DYp + GZg * (e320 + e321);
     // momentum: U1..W2
@@ -271,7 +279,7 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const
   // ---------------- reverse ----------------
   double ar = 0, au = 0, av = 0, awh = 0, awl = 0, ath = 0, ap = 0;
   // mu, mv: (-v W1 - wl V1 - v W2 - wh V2 + FU)/MC, (u W1 - wl U1 + u W2 - wh U2 + FV)/MC
-  const double amu = lam_u / MC, amv = lam_v / MC;
+  const double amu = lam_u * iMC, amv = lam_v * iMC;
   double aU1 = -wl * amv, aU2 = -wh * amv, aV1 = -wl * amu, aV2 = -wh * amu;
   double aW1 = -v * amu + u * amv, aW2 = aW1;
   av += -(W1 + W2) * amu;
@@ -283,9 +291,9 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const
   av += fc * Js * aFU;
   au += -fc * Js * aFV;
   // gradient part: gu = (GuF1 + GuF2 - Gradu/rho)/MC, gv likewise
-  const double aG1u = lam_u / MC, aG1v = lam_v / MC;   // adjoints of GuF1 = GuF2, GvF1 = GvF2
-  double aGradu = -lam_u / (MC * rho), aGradv = -lam_v / (MC * rho);
-  ar += (Gradu * lam_u + Gradv * lam_v) / (MC * rho * rho);
+  const double aG1u = amu, aG1v = amv;   // adjoints of GuF1 = GuF2, GvF1 = GvF2
+  double aGradu = -amu * irho, aGradv = -amv * irho;
+  ar += (Gradu * amu + Gradv * amv) * irho * irho;
   const double aDXK1 = -(d110 * aG1u + d120 * aG1v), aDYK1 = -(d210 * aG1u + d220 * aG1v);
   const double aDXK2 = -(d111 * aG1u + d121 * aG1v), aDYK2 = -(d211 * aG1u + d221 * aG1v);
   double aK1s = 0, aK2s = 0;
@@ -311,11 +319,13 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const
     const double GwF2 = -rho * GZt * e331 - rho * GZs * e331;
     const double GZp = 0.5 * (pa_ - AW(A_P, p0, ID));
     const double Gradp = -(GZp * (e331 + D330a) + P.Grav * (rho * J1 + rho1 * J0a));
-    const double whi = (rho * Nh + GwF2 + Gradp) / den;
+    const double iden = 1.0 / den;
+    const double whi = (rho * Nh + GwF2 + Gradp) * iden;
     // whi = (rho Nh + GwF2 + Gradp) / den
-    aNh = rho * lam_whi / den;
-    ar += Nh * lam_whi / den;
-    const double aGwF2 = lam_whi / den, aGradp = lam_whi / den, aden = -whi * lam_whi / den;
+    const double lw = lam_whi * iden;
+    aNh = rho * lw;
+    ar += Nh * lw;
+    const double aGwF2 = lw, aGradp = lw, aden = -whi * lw;
     const double arho1 = M0a * aden - P.Grav * J0a * aGradp;
     ar += M1 * aden - P.Grav * J1 * aGradp;
     add_p(lv + 1, -0.5 * (e331 + D330a) * aGradp);
@@ -369,10 +379,12 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const
     const double K2b = 0.5 * (ub * ub + vb * vb) + 0.5 * (wb * wb);
     const double GZ1 = 0.5 * (K1s - K2b), GZ2 = 0.5 * (K2s - K1s);
     const double GwF1 = -rho * GZ1 * e330 - rho * GZ2 * e330;
-    const double wlo = (rho * Nl + GwF1) / den;
-    aNl = rho * lam_wlo / den;
-    ar += Nl * lam_wlo / den;
-    const double aGwF1 = lam_wlo / den, aden = -wlo * lam_wlo / den;
+    const double iden = 1.0 / den;
+    const double wlo = (rho * Nl + GwF1) * iden;
+    const double lw = lam_wlo * iden;
+    aNl = rho * lw;
+    ar += Nl * lw;
+    const double aGwF1 = lw, aden = -wlo * lw;
     double arhob = M1b * aden;
     ar += M0 * aden;
     ar += -(GZ1 + GZ2) * e330 * aGwF1;
@@ -428,7 +440,7 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const
   // Gradu = d11 DXp + d21 DYp + GZg (e310 + e311); GZg = -g rho Js / (e330 + e331)
   {
     const double aGZg = (e310 + e311) * aGradu + (e320 + e321) * aGradv;
-    ar += -P.Grav * Js / (e330 + e331) * aGZg;
+    ar += -P.Grav * Js * i33 * aGZg;
   }
   const double aDXp = d11 * aGradu + d12 * aGradv, aDYp = d21 * aGradu + d22 * aGradv;
 
@@ -475,7 +487,7 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const
   }
   __syncwarp();
   // ---- transposed round 3: flux divergences (HR, HTH) ----
-  const double aDivRho = lam_r / MC, aDivTr = lam_th / MC;
+  const double aDivRho = lam_r * iMC, aDivTr = lam_th * iMC;
   if (act) { SC(0, ID) = aDivRho; SC(1, ID) = aDivTr; }
   __syncwarp();
   if (act) {
@@ -497,13 +509,13 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const
   __syncwarp();
   // ---- transposed round 4: weak derivatives of the hyperviscosity ----
   const double nuC = P.nuCurl, nuG = P.nuGrad, nuD = P.nuDiv;
-  const double aFuC = nuC * lam_u / MC, aFuD = -nuG * lam_u / MC, aFvC = nuC * lam_v / MC, aFvD = -nuG * lam_v / MC;
+  const double aFuC = nuC * amu, aFuD = -nuG * amu, aFvC = nuC * amv, aFvD = -nuG * amv;
   if (act) {
     SC(0, ID) = d12 * aFuC - d11 * aFvC;   // DxCurl
     SC(1, ID) = d22 * aFuC - d21 * aFvC;   // DyCurl
     SC(2, ID) = d11 * aFuD + d12 * aFvD;   // DxDiv
     SC(3, ID) = d21 * aFuD + d22 * aFvD;   // DyDiv
-    SC(4, ID) = -nuD * lam_th / MC;        // DivTh
+    SC(4, ID) = -nuD * aDivTr;             // DivTh
   }
   __syncwarp();
   double acu = 0, adv = 0, aDxc = 0, aDyc = 0;
@@ -516,13 +528,13 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const
       ab3 += WTI[k] * SC(4, k + N * Jn);
       ab4 += WTJ[k] * SC(4, I + N * k);
     }
-    acu = ab1 / Js;
-    adv = ab2 / Js;
+    acu = ab1 * iJs;
+    adv = ab2 * iJs;
     // b3 = rho (d11 GDx + d12 GDy), b4 = rho (d21 GDx + d22 GDy)
     ar += (d11 * GDx + d12 * GDy) * ab3 + (d21 * GDx + d22 * GDy) * ab4;
     const double aGDx = rho * (d11 * ab3 + d21 * ab4), aGDy = rho * (d12 * ab3 + d22 * ab4);
-    aDxc = (d11 * aGDx + d12 * aGDy) / Js;
-    aDyc = (d21 * aGDx + d22 * aGDy) / Js;
+    aDxc = (d11 * aGDx + d12 * aGDy) * iJs;
+    aDyc = (d21 * aGDx + d22 * aGDy) * iJs;
   }
   __syncwarp();
   // ---- transposed round 5: first derivatives of the cache ----
@@ -577,8 +589,8 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const
     ADDU(1, il + 1, rR * b310 * awc);
     ADDU(2, il + 1, rR * b320 * awc);
   };
-  if (top) iface(lv, -0.5 * lam_r / MC, -lam_th / MC);
-  if (bot) iface(lv - 1, 0.5 * lam_r / MC, lam_th / MC);
+  if (top) iface(lv, -0.5 * aDivRho, -aDivTr);
+  if (bot) iface(lv - 1, 0.5 * aDivRho, aDivTr);
 
   // ---- own node: pressure, theta, lower w ----
   add_p(lv, ap);
@@ -603,7 +615,7 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_phase2_adj(const GP P, const
 // cache, broadcast to the element nodes).  Phase 1 is linear in u, v and
 // theta = rho*theta / rho.
 template <int N>
-__global__ void __launch_bounds__(32 * ADJ_WARPS) k_hypervisc1_adj(const GP P, const double *__restrict__ U,
+__global__ void __launch_bounds__(32 * ADJ_WARPS, 3) k_hypervisc1_adj(const GP P, const double *__restrict__ U,
                                                                   const double *__restrict__ LT1,
                                                                   double *__restrict__ LU)
 {
@@ -640,8 +652,9 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_hypervisc1_adj(const GP P, c
     MC = P.M[l + (size_t)nz * g] + P.M[l + (size_t)nz * (g + (size_t)NumG)];
     const double *L = LT1 + (size_t)nz * g + l;
     // out0 = -FuC/MC, out1 = -FvC/MC, out2 = FuD/MC, out3 = FvD/MC, out4 = DivTh/MC
-    const double aFuC = -L[0] / MC, aFvC = -L[fs] / MC, aFuD = L[2 * fs] / MC, aFvD = L[3 * fs] / MC;
-    a4 = L[4 * fs] / MC;   // DivTh
+    const double iMC = 1.0 / MC;
+    const double aFuC = -L[0] * iMC, aFvC = -L[fs] * iMC, aFuD = L[2 * fs] * iMC, aFvD = L[3 * fs] * iMC;
+    a4 = L[4 * fs] * iMC;   // DivTh
     a0 = d12 * aFuC - d11 * aFvC;   // DxCurl
     a1 = d22 * aFuC - d21 * aFvC;   // DyCurl
     a2 = d11 * aFuD + d12 * aFvD;   // DxDiv
@@ -663,11 +676,11 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_hypervisc1_adj(const GP P, c
   // s5 = cu/Js, s6 = dv/Js, s7 = d11 GDx + d12 GDy, s8 = d21 GDx + d22 GDy,
   // GDx = (d11 Dxc + d21 Dyc)/Js, GDy = (d12 Dxc + d22 Dyc)/Js
   if (act) {
-    const double aGDx = d11 * as7 + d21 * as8, aGDy = d12 * as7 + d22 * as8;
-    SC(0, ID) = as5 / Js;
-    SC(1, ID) = as6 / Js;
-    SC(2, ID) = (d11 * aGDx + d12 * aGDy) / Js;
-    SC(3, ID) = (d21 * aGDx + d22 * aGDy) / Js;
+    const double aGDx = d11 * as7 + d21 * as8, aGDy = d12 * as7 + d22 * as8, iJs = 1.0 / Js;
+    SC(0, ID) = as5 * iJs;
+    SC(1, ID) = as6 * iJs;
+    SC(2, ID) = (d11 * aGDx + d12 * aGDy) * iJs;
+    SC(3, ID) = (d21 * aGDx + d22 * aGDy) * iJs;
   }
   __syncwarp();
   if (!act) return;
@@ -688,139 +701,172 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS) k_hypervisc1_adj(const GP P, c
   double *LUg = LU + (size_t)nz * g + l;
   atomicAdd(LUg + fs, au);
   atomicAdd(LUg + 2 * fs, av);
-  atomicAdd(LUg + 4 * fs, as4 / rho);
-  atomicAdd(LUg, -as4 * rth / (rho * rho));
+  const double q = as4 / rho;
+  atomicAdd(LUg + 4 * fs, q);
+  atomicAdd(LUg, -q * (rth / rho));
 #undef SC
 }
 
 
-// out = a x + b y + c z, elementwise (null pointers count as zero)
-__global__ void __launch_bounds__(256) k_lincomb(long long n, double *__restrict__ out, double a,
-                                                 const double *__restrict__ x, double b, const double *__restrict__ y,
-                                                 double c, const double *__restrict__ z)
+// One reverse sweep of the three stage quantities: Lk0, Lk1 (adjoints of k1,
+// k2) and LV (adjoint of the step's initial state), from Lt = F'^T AR of the
+// stage and AR (adjoint of its right-hand side r = F + cA k1 + cB k2):
+//   stage 3 (L != null): Lk0 = m0 L + cA AR + a0 Lt, Lk1 = m1 L + cB AR + a1 Lt, LV += L + Lt
+//   stage 2 (Lk0 != null): Lk0 += cA AR + a0 Lt, LV += Lt
+//   stage 1: LV += Lt
+__global__ void __launch_bounds__(256) k_adj_update(long long n, const double *__restrict__ L,
+                                                    const double *__restrict__ AR, const double *__restrict__ Lt,
+                                                    double *__restrict__ LV, double *__restrict__ Lk0,
+                                                    double *__restrict__ Lk1, double m0, double m1, double cA,
+                                                    double cB, double a0, double a1)
 {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  double s = 0.0;
-  if (x) s += a * x[i];
-  if (y) s += b * y[i];
-  if (z) s += c * z[i];
-  out[i] = s;
+  const double lt = Lt[i];
+  if (L) {
+    const double l = L[i], ar = AR[i];
+    Lk0[i] = m0 * l + cA * ar + a0 * lt;
+    Lk1[i] = m1 * l + cB * ar + a1 * lt;
+    LV[i] = LV[i] + (l + lt);
+  } else if (Lk0) {
+    Lk0[i] = Lk0[i] + (cA * AR[i] + a0 * lt);
+    LV[i] = LV[i] + lt;
+  } else {
+    LV[i] = LV[i] + lt;
+  }
 }
 
-// Reverse of the column Schur solve of one stage, k = L(bands) r with
-// r = F + cA k1 + cB k2 (TriDiagKernel!, SchurSolveFKernel!, triSolve!,
-// SchurSolveBKernel!: src/Integration/SchurSolve.jl:1-114).  Given mu, the
+// Reverse of the column Schur solve of one stage, k = L(bands) r
+// (TriDiagKernel!, SchurSolveFKernel!, triSolve!, SchurSolveBKernel!:
+// src/Integration/SchurSolve.jl:1-114).  Given mu (times the scalar mus), the
 // adjoint of k, writes AR, the adjoint of r, and adds the adjoint that flows
 // through the Jacobian bands (JacSchur.jl:40-73) into LV (fields rho and
-// rho*theta of the step's initial state).  One warp per column; the forward
-// and the transposed tridiagonal solves run on the warp's first lane.
-constexpr int CA_ARR = 25;   // per-warp arrays of nz entries
+// rho*theta of the step's initial state).
+//
+// The stage's k (kx), kept by the forward stage, gives everything else the
+// reverse needs: the tridiagonal solution x is its w field, and the
+// right-hand side of rho and rho*theta follows from SchurSolveB,
+// r0(l) = k0(l)/fac - JB(0,0,l) x(l) - JB(0,1,l-1) x(l-1) (r4 with JB(3,.)).  The forward sweep solves M x = b with M(i,i) = t1(i),
+// M(i+1,i) = t2(i), M(i,i+1) = t0(i+1) (the reference's triSolve!); here
+// M = L U with pivots d(i) and multipliers m(i) = t2(i)/d(i), and M^T y = ax is
+// U^T z = ax, L^T y = z.  One warp per column for the level-parallel parts;
+// the serial recurrences of the block's columns run together, one per lane of
+// the first warp.
+constexpr int CA_ARR = 18;   // per-warp arrays of nz entries
 
-__global__ void __launch_bounds__(32 * COL_WARPS) k_column_adj(const GP P, const double *__restrict__ mu,
-                                                              const double *__restrict__ F,
-                                                              const double *__restrict__ k1, double cA,
-                                                              const double *__restrict__ k2, double cB,
-                                                              const double *__restrict__ jbg,
-                                                              const double *__restrict__ Vn, double fac,
-                                                              double *__restrict__ AR, double *__restrict__ LV)
+__global__ void __launch_bounds__(32 * COL_WARPS, 3) k_column_adj(const GP P, const double *__restrict__ mu, double mus,
+                                                                 const double *__restrict__ kx,
+                                                                 const double *__restrict__ jbg,
+                                                                 const double *__restrict__ Vn, double fac,
+                                                                 double *__restrict__ AR, double *__restrict__ LV)
 {
   extern __shared__ double csm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = blockIdx.x * COL_WARPS + warp;
+  const int g0 = blockIdx.x * COL_WARPS, g = g0 + warp;
   const int nz = P.nz, n = nz - 1, NV = P.NV, NumG = P.NumG;
-  if (g >= NumG) return;   // warp-uniform; this kernel synchronises within warps only
+  const bool valid = g < NumG;   // no early return: the block synchronises
   const int LS = nz;
   double *sw = csm + (size_t)warp * CA_ARR * LS;
-  double *r0 = sw, *r3 = sw + LS, *r4 = sw + 2 * LS;
-  double *jb = sw + 3 * LS;          // [8][nz]
-  double *tri = sw + 11 * LS;        // [3][nz]
-  double *x = sw + 14 * LS, *b = sw + 15 * LS, *y = sw + 16 * LS, *ax = sw + 17 * LS;
-  double *av0 = sw + 18 * LS, *av4 = sw + 19 * LS;
-  double *accL0 = sw + 20 * LS, *accL4 = sw + 21 * LS, *accR0 = sw + 22 * LS, *accR4 = sw + 23 * LS;
-  double *cp = sw + 24 * LS;         // the transposed sweep's modified super-diagonal
+  double *r0 = sw, *r4 = sw + LS, *av0 = sw + 2 * LS, *av4 = sw + 3 * LS;
+  double *jb = sw + 4 * LS;          // [8][nz]
+  double *tri = sw + 12 * LS;        // [3][nz]: t0, t1, t2
+  double *x = sw + 15 * LS;
+  double *ay = sw + 16 * LS;         // ax, then y
+  double *accR0 = sw + 17 * LS;      // interface l-1's share of level l (rho)
   const size_t fs = (size_t)nz * NumG;
   const size_t js = (size_t)NumG * n;
 #define JB(arr, r, i) jb[((arr) * 2 + (r)) * LS + (i)]
-  // 1. the stage's right-hand side r; fields outside the Schur system: AR = fac mu
-  for (int l = lane; l < nz; l += 32) {
-    const size_t o0 = l + (size_t)nz * g;
+  // 1. x, the bands, the adjoints of the k of rho and rho*theta; fields
+  //    outside the Schur system: AR = fac mu; then the right-hand side of rho
+  //    and rho*theta
+  if (valid) {
+    for (int l = lane; l < nz; l += 32) {
+      const size_t o0 = l + (size_t)nz * g;
 #pragma unroll
-    for (int f = 0; f < MAXNV; ++f) {
-      if (f >= NV) break;
-      const size_t o = o0 + f * fs;
-      if (f == 0 || f == 3 || f == 4) {
-        double r = F[o];
-        if (k1) r = r + cA * k1[o];
-        if (k2) r = r + cB * k2[o];
-        (f == 0 ? r0 : f == 3 ? r3 : r4)[l] = r;
-      } else {
-        AR[o] = fac * mu[o];
+      for (int f = 1; f < MAXNV; ++f) {
+        if (f >= NV) break;
+        if (f != 3 && f != 4) AR[o0 + f * fs] = fac * (mus * mu[o0 + f * fs]);
+      }
+      av0[l] = fac * (mus * mu[o0]);
+      av4[l] = fac * (mus * mu[o0 + 4 * fs]);
+      if (l < n) {
+        x[l] = kx[o0 + 3 * fs];
+        for (int rr = 0; rr < 8; ++rr) jb[rr * LS + l] = jbg[rr * js + (size_t)g * n + l];
       }
     }
-    av0[l] = fac * mu[o0];
-    av4[l] = fac * mu[o0 + 4 * fs];
-    if (l < n)
-      for (int rr = 0; rr < 8; ++rr) jb[rr * LS + l] = jbg[rr * js + (size_t)g * n + l];
+    __syncwarp();
+    const double invfac2 = 1.0 / fac / fac;
+    for (int l = lane; l < nz; l += 32) {
+      const size_t o0 = l + (size_t)nz * g;
+      double s0 = kx[o0] / fac, s4 = kx[o0 + 4 * fs] / fac;
+      if (l < n) { s0 -= JB(0, 0, l) * x[l]; s4 -= JB(3, 0, l) * x[l]; }
+      if (l > 0) { s0 -= JB(0, 1, l - 1) * x[l - 1]; s4 -= JB(3, 1, l - 1) * x[l - 1]; }
+      r0[l] = s0;
+      r4[l] = s4;
+    }
+    for (int l = lane; l < n; l += 32) {
+      tri[LS + l] = invfac2 - JB(1, 1, l) * JB(0, 0, l) - JB(1, 0, l) * JB(0, 1, l) - JB(2, 1, l) * JB(3, 0, l) -
+                    JB(2, 0, l) * JB(3, 1, l);
+      tri[l] = l == 0 ? 0.0 : -JB(1, 0, l - 1) * JB(0, 0, l) - JB(2, 0, l - 1) * JB(3, 0, l);
+      tri[2 * LS + l] = l == n - 1 ? 0.0 : -JB(1, 1, l + 1) * JB(0, 1, l) - JB(2, 1, l + 1) * JB(3, 1, l);
+      // reverse of SchurSolveB: v0'(l) = r0(l) + JB(0,0,l) x(l) + JB(0,1,l-1) x(l-1), v4' likewise; kw = x
+      ay[l] = mus * mu[l + (size_t)nz * g + 3 * fs] + JB(0, 0, l) * av0[l] + JB(3, 0, l) * av4[l] +
+              JB(0, 1, l) * av0[l + 1] + JB(3, 1, l) * av4[l + 1];
+    }
   }
-  __syncwarp();
-  const double invfac = 1.0 / fac, invfac2 = invfac / fac;
-  for (int l = lane; l < n; l += 32) {
-    tri[LS + l] = invfac2 - JB(1, 1, l) * JB(0, 0, l) - JB(1, 0, l) * JB(0, 1, l) - JB(2, 1, l) * JB(3, 0, l) -
-                  JB(2, 0, l) * JB(3, 1, l);
-    tri[l] = l == 0 ? 0.0 : -JB(1, 0, l - 1) * JB(0, 0, l) - JB(2, 0, l - 1) * JB(3, 0, l);
-    tri[2 * LS + l] = l == n - 1 ? 0.0 : -JB(1, 1, l + 1) * JB(0, 1, l) - JB(2, 1, l + 1) * JB(3, 1, l);
-    b[l] = r3[l] / fac + JB(1, 1, l) * r0[l] + JB(1, 0, l) * r0[l + 1] + JB(2, 1, l) * r4[l] + JB(2, 0, l) * r4[l + 1];
-  }
-  __syncwarp();
-  // 2. forward solve T x = b (the same sweep as the forward kernel)
-  if (lane == 0) {
-    x[0] = tri[LS];
+  __syncthreads();
+  // 2. M^T y = ax for the block's columns, one lane each
+  if (threadIdx.x < COL_WARPS && g0 + (int)threadIdx.x < NumG) {
+    double *c = csm + (size_t)threadIdx.x * CA_ARR * LS;
+    const double *t0 = c + 12 * LS, *t1 = c + 13 * LS, *t2 = c + 14 * LS;
+    double *q = c + 17 * LS;     // multipliers m(i) (accR0 is not in use yet)
+    double *yy = c + 16 * LS;
+    double inv = 1.0 / t1[0];
+    double z = yy[0] * inv;
+    yy[0] = z;
     for (int i = 0; i < n - 1; ++i) {
-      const double m = tri[2 * LS + i] / x[i];
-      x[i + 1] = tri[LS + i + 1] - m * tri[i + 1];
-      b[i + 1] = b[i + 1] - m * b[i];
+      const double m = t2[i] * inv;
+      q[i] = m;
+      inv = 1.0 / (t1[i + 1] - m * t0[i + 1]);
+      z = (yy[i + 1] - t0[i + 1] * z) * inv;
+      yy[i + 1] = z;
     }
-    x[n - 1] = b[n - 1] / x[n - 1];
-    for (int i = n - 2; i >= 0; --i) x[i] = (b[i] - tri[i + 1] * x[i + 1]) / x[i];
-  }
-  __syncwarp();
-  // 3. reverse of SchurSolveB: v0'(l) = r0(l) + JB(0,0,l) x(l) + JB(0,1,l-1) x(l-1), v4' likewise;
-  //    kw = x
-  for (int l = lane; l < n; l += 32) {
-    ax[l] = mu[l + (size_t)nz * g + 3 * fs] + JB(0, 0, l) * av0[l] + JB(3, 0, l) * av4[l] +
-            JB(0, 1, l) * av0[l + 1] + JB(3, 1, l) * av4[l + 1];
-  }
-  __syncwarp();
-  // 4. The forward sweep solves M x = b with M(i,i) = t1(i), M(i+1,i) = t2(i),
-  //    M(i,i+1) = t0(i+1) (the reference's triSolve!).  Transposed solve
-  //    M^T y = ax: row i is t0(i) y(i-1) + t1(i) y(i) + t2(i) y(i+1).
-  if (lane == 0) {
-    double bb = tri[LS];
-    cp[0] = (n > 1 ? tri[2 * LS] : 0.0) / bb;
-    y[0] = ax[0] / bb;
-    for (int i = 1; i < n; ++i) {
-      const double a = tri[i];
-      bb = tri[LS + i] - a * cp[i - 1];
-      cp[i] = (i + 1 < n ? tri[2 * LS + i] : 0.0) / bb;
-      y[i] = (ax[i] - a * y[i - 1]) / bb;
+    for (int i = n - 2; i >= 0; --i) {
+      z = yy[i] - q[i] * z;
+      yy[i] = z;
     }
-    for (int i = n - 2; i >= 0; --i) y[i] = y[i] - cp[i] * y[i + 1];
   }
-  __syncwarp();
-  // 5. band adjoints (TriDiag, SchurSolveF, SchurSolveB) and the adjoint of r
+  __syncthreads();
+  if (!valid) return;
+  // 3. adjoint of r, and the band adjoints (TriDiag, SchurSolveF, SchurSolveB)
+  //    of interface l, whose share of level l is added here and whose share
+  //    of level l+1 is passed on through aR0 / aR4
+  double *aR0 = accR0, *aR4 = tri + 1 * LS;   // the multipliers and t1 are dead after the sweep
   for (int l = lane; l < nz; l += 32) {
     const size_t o0 = l + (size_t)nz * g;
     double ar0 = av0[l], ar4 = av4[l];
-    if (l < n) { ar0 += JB(1, 1, l) * y[l]; ar4 += JB(2, 1, l) * y[l]; }
-    if (l > 0) { ar0 += JB(1, 0, l - 1) * y[l - 1]; ar4 += JB(2, 0, l - 1) * y[l - 1]; }
+    if (l < n) { ar0 += JB(1, 1, l) * ay[l]; ar4 += JB(2, 1, l) * ay[l]; }
+    if (l > 0) { ar0 += JB(1, 0, l - 1) * ay[l - 1]; ar4 += JB(2, 0, l - 1) * ay[l - 1]; }
     AR[o0] = ar0;
-    AR[o0 + 3 * fs] = l < n ? y[l] / fac : 0.0;
+    AR[o0 + 3 * fs] = l < n ? ay[l] / fac : 0.0;
     AR[o0 + 4 * fs] = ar4;
-    accL0[l] = accL4[l] = accR0[l] = accR4[l] = 0.0;
+  }
+  // dp/d(rho*theta) of every level and its derivative factor kappa/(1-kappa) dp/(rho*theta)
+  const double ex = P.kappa / (1.0 - P.kappa);
+  double *dP = tri, *dPd = tri + 2 * LS;   // t0, t2 are dead after the sweep
+  for (int l = lane; l < nz; l += 32) {
+    const double Th = Vn[l + (size_t)nz * g + 4 * fs] + 0.0;
+    const double d = dpdrhoth(P, Th);
+    dP[l] = d;
+    dPd[l] = ex * d / Th;
   }
   __syncwarp();
-  for (int l = lane; l < n; l += 32) {
+  double accL0[2] = {0.0, 0.0}, accL4[2] = {0.0, 0.0};
+#pragma unroll
+  for (int it = 0; it < 2; ++it) {
+    const int l = lane + 32 * it;
+    if (l >= n) continue;
+    const double *y = ay;
     double a[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};   // a[arr][r] = adjoint of JB(arr, r, l)
     // adjoint of M(i,j) is -y(i) x(j)
     const double at1 = -y[l] * x[l];
@@ -849,29 +895,30 @@ __global__ void __launch_bounds__(32 * COL_WARPS) k_column_adj(const GP P, const
     a[3][0] += av4[l] * x[l]; a[3][1] += av4[l + 1] * x[l];
     // bands of interface l from rho, rho*theta at l, l+1 (JacSchurKernel!)
     const double *V0 = Vn + (size_t)nz * g;
-    const double RhoL = V0[l], RhoR = V0[l + 1], ThL = V0[l + 4 * fs] + 0.0, ThR = V0[l + 1 + 4 * fs] + 0.0;
+    const double RhoL = V0[l], RhoR = V0[l + 1];
     const double dzL = P.dz[l + (size_t)nz * g], dzR = P.dz[l + 1 + (size_t)nz * g], dzs = dzL + dzR;
-    const double RhoF = (RhoL * dzL + RhoR * dzR) / dzs;
-    const double ex = P.kappa / (1.0 - P.kappa);
-    const double dPL = dpdrhoth(P, ThL), dPR = dpdrhoth(P, ThR);
-    const double h = 0.5 * dzs;
-    // jb0 = -RhoF/dzL, jb1 = RhoF/dzR, jb4 = -dPR/RhoF/h, jb5 = dPL/RhoF/h,
+    const double idzL = 1.0 / dzL, idzR = 1.0 / dzR, idzs = 1.0 / dzs, ih = 2.0 * idzs;
+    const double iR = 1.0 / ((RhoL * dzL + RhoR * dzR) * idzs);   // 1 / RhoF
+    // jb0 = -RhoF/dzL, jb1 = RhoF/dzR, jb4 = -dPR/RhoF/h, jb5 = dPL/RhoF/h, h = dzs/2,
     // jb2 = -g dzR/RhoF/dzs, jb3 = -g dzL/RhoF/dzs, jb6 = -RhoThF/dzL, jb7 = RhoThF/dzR
-    const double aRhoF = -a[0][0] / dzL + a[0][1] / dzR + a[2][0] * dPR / (RhoF * RhoF * h) -
-                         a[2][1] * dPL / (RhoF * RhoF * h) + a[1][0] * P.Grav * dzR / (RhoF * RhoF * dzs) +
-                         a[1][1] * P.Grav * dzL / (RhoF * RhoF * dzs);
-    const double adPR = -a[2][0] / (RhoF * h), adPL = a[2][1] / (RhoF * h);
-    const double aThF = -a[3][0] / dzL + a[3][1] / dzR;
-    accL0[l] = aRhoF * dzL / dzs;
-    accR0[l + 1] = aRhoF * dzR / dzs;
-    accL4[l] = aThF * dzL / dzs + adPL * ex * dPL / ThL;
-    accR4[l + 1] = aThF * dzR / dzs + adPR * ex * dPR / ThR;
+    const double aRhoF = -a[0][0] * idzL + a[0][1] * idzR + (a[2][0] * dP[l + 1] - a[2][1] * dP[l]) * iR * iR * ih +
+                         (a[1][0] * dzR + a[1][1] * dzL) * P.Grav * iR * iR * idzs;
+    const double adPR = -a[2][0] * iR * ih, adPL = a[2][1] * iR * ih;
+    const double aThF = -a[3][0] * idzL + a[3][1] * idzR;
+    accL0[it] = aRhoF * dzL * idzs;
+    accL4[it] = aThF * dzL * idzs + adPL * dPd[l];
+    aR0[l + 1] = aRhoF * dzR * idzs;
+    aR4[l + 1] = aThF * dzR * idzs + adPR * dPd[l + 1];
   }
   __syncwarp();
-  for (int l = lane; l < nz; l += 32) {
+#pragma unroll
+  for (int it = 0; it < 2; ++it) {
+    const int l = lane + 32 * it;
+    if (l >= nz) continue;
     const size_t o0 = l + (size_t)nz * g;
-    LV[o0] += accL0[l] + accR0[l];
-    LV[o0 + 4 * fs] += accL4[l] + accR4[l];
+    const double r0s = l > 0 ? aR0[l] : 0.0, r4s = l > 0 ? aR4[l] : 0.0;
+    LV[o0] += accL0[it] + r0s;
+    LV[o0 + 4 * fs] += accL4[it] + r4s;
   }
 #undef JB
 }

@@ -50,7 +50,8 @@ struct cgd_handle {
   double *pres = nullptr, *pres_st = nullptr;   // pressure of the state and of the stage state
   double *aLF = nullptr, *aLU = nullptr, *aLT1 = nullptr;   // adjoint buffers (allocated on first use)
   // step adjoint workspace: stage states, stage tendencies, k adjoints, ...
-  double *sV2 = nullptr, *sV3 = nullptr, *sF[3] = {}, *aLk[3] = {}, *aAR = nullptr, *aLV = nullptr, *aLt = nullptr;
+  double *sV2 = nullptr, *sV3 = nullptr, *sT1[3] = {}, *sP[3] = {}, *sk3 = nullptr;
+  double *aLk[2] = {}, *aAR = nullptr, *aLV = nullptr, *aLt = nullptr;
   double *mmass = nullptr;
   int *flag = nullptr;
   GP gp{};
@@ -298,7 +299,8 @@ void ensure_ref(cgd_handle *h, const double *Ud)
 // Reverse of the tendency (no tracers, FP64): phase 2 into the state and
 // cache adjoints, then phase 1 from the cache adjoint into the state adjoint.
 template <int N>
-int rhs_adjoint_launch(cgd_handle *h, const double *Ud, const double *LF, double *LU)
+int rhs_adjoint_launch(cgd_handle *h, const double *Ud, const double *T1, const double *pres, const double *LF,
+                       double *LU)
 {
   using CF = AdjCfg<N>;
   static bool attr = false;
@@ -307,7 +309,7 @@ int rhs_adjoint_launch(cgd_handle *h, const double *Ud, const double *LF, double
     attr = true;
   }
   dim3 grid((h->nz + CF::LC - 1) / CF::LC, h->NF);
-  k_phase2_adj<N><<<grid, CF::THREADS, CF::SMEM, h->stream>>>(h->gp, Ud, h->pres, h->T1, LF, LU, h->aLT1);
+  k_phase2_adj<N><<<grid, CF::THREADS, CF::SMEM, h->stream>>>(h->gp, Ud, pres, T1, LF, LU, h->aLT1);
   k_hypervisc1_adj<N><<<grid, CF::THREADS, 0, h->stream>>>(h->gp, Ud, h->aLT1, LU);
   CK(cudaGetLastError());
   return CGD_OK;
@@ -786,8 +788,10 @@ int adjoint_alloc(cgd_handle *h, bool step)
   if (!rc && step && !h->sV2) {
     rc = dalloc(h, &h->sV2, SV);
     if (!rc) rc = dalloc(h, &h->sV3, SV);
-    for (int i = 0; i < 3 && !rc; ++i) rc = dalloc(h, &h->sF[i], SV);
-    for (int i = 0; i < 3 && !rc; ++i) rc = dalloc(h, &h->aLk[i], SV);
+    for (int i = 0; i < 3 && !rc; ++i) rc = dalloc(h, &h->sT1[i], S * 5);
+    for (int i = 0; i < 3 && !rc; ++i) rc = dalloc(h, &h->sP[i], S);
+    for (int i = 0; i < 2 && !rc; ++i) rc = dalloc(h, &h->aLk[i], SV);
+    if (!rc) rc = dalloc(h, &h->sk3, SV);
     if (!rc) rc = dalloc(h, &h->aAR, SV);
     if (!rc) rc = dalloc(h, &h->aLV, SV);
     if (!rc) rc = dalloc(h, &h->aLt, SV);
@@ -795,38 +799,38 @@ int adjoint_alloc(cgd_handle *h, bool step)
   return rc;
 }
 
-// LU = (dF/dU)^T LF at the device state Ud (LU zeroed here)
-int rhs_adjoint_core(cgd_handle *h, const double *Ud, const double *LFd, double *LUd)
+// LU = (dF/dU)^T LF at the device state Ud (LU zeroed here).  T1 and pres
+// are the state's DSS'd phase-1 cache and pressure when the caller has them,
+// else null (computed here).
+int rhs_adjoint_core(cgd_handle *h, const double *Ud, const double *LFd, double *LUd, const double *T1 = nullptr,
+                     const double *pres = nullptr)
 {
   const size_t S = (size_t)h->nz * h->NumG;
-  hv1(h, Ud, h->C);
-  gather(h, h->C, h->T1, false);
-  pressure(h, Ud, h->pres);
+  if (!T1) {
+    hv1(h, Ud, h->C);
+    gather(h, h->C, h->T1, false);
+    pressure(h, Ud, h->pres);
+    T1 = h->T1;
+    pres = h->pres;
+  }
   CK(cudaMemsetAsync(LUd, 0, S * h->NV * 8, h->stream));
   CK(cudaMemsetAsync(h->aLT1, 0, S * 5 * 8, h->stream));
   switch (h->N) {
-    case 2: return rhs_adjoint_launch<2>(h, Ud, LFd, LUd);
-    case 3: return rhs_adjoint_launch<3>(h, Ud, LFd, LUd);
-    case 4: return rhs_adjoint_launch<4>(h, Ud, LFd, LUd);
-    default: return rhs_adjoint_launch<5>(h, Ud, LFd, LUd);
+    case 2: return rhs_adjoint_launch<2>(h, Ud, T1, pres, LFd, LUd);
+    case 3: return rhs_adjoint_launch<3>(h, Ud, T1, pres, LFd, LUd);
+    case 4: return rhs_adjoint_launch<4>(h, Ud, T1, pres, LFd, LUd);
+    default: return rhs_adjoint_launch<5>(h, Ud, T1, pres, LFd, LUd);
   }
 }
 
-void lincomb(cgd_handle *h, double *out, double a, const double *x, double b = 0.0, const double *y = nullptr,
-             double c = 0.0, const double *z = nullptr)
-{
-  const long long n = (long long)h->nz * h->NumG * h->NV;
-  k_lincomb<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(n, out, a, x, b, y, c, z);
-}
-
-int column_adj(cgd_handle *h, const double *mu, const double *F, const double *k1, double cA, const double *k2,
-               double cB, const double *Vn, double fac, double *AR, double *LV)
+int column_adj(cgd_handle *h, const double *mu, double mus, const double *kx, const double *Vn, double fac, double *AR,
+               double *LV)
 {
   CK(cudaFuncSetAttribute(k_column_adj, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           COL_WARPS * CA_ARR * 64 * (int)sizeof(double)));
   const size_t smem = (size_t)COL_WARPS * CA_ARR * h->nz * sizeof(double);
   k_column_adj<<<(h->NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, h->stream>>>(
-      h->gp, mu, F, k1, cA, k2, cB, h->jbg, Vn, fac, AR, LV);
+      h->gp, mu, mus, kx, h->jbg, Vn, fac, AR, LV);
   CK(cudaGetLastError());
   return CGD_OK;
 }
@@ -852,7 +856,8 @@ int cgd_ros_step_adjoint(cgd_handle *h, const double *U0, const double *Lout, do
   }
   const RK &rk = h->rk;
   const double fac = dt * rk.gamma;
-  // forward replay of the step, keeping the stage states and tendencies
+  // forward replay of the step, keeping each stage's state, phase-1 cache,
+  // pressure and k
   ColArgs a{};
   a.Vn = Ud;
   a.k1 = h->k1;
@@ -863,37 +868,46 @@ int cgd_ros_step_adjoint(cgd_handle *h, const double *U0, const double *Lout, do
   a.C = h->C;
   a.jbg = h->jbg;
   const double *Vs[3] = {Ud, h->sV2, h->sV3};
+  const double *ks[3] = {h->k1, h->k2, h->sk3};
   for (int st = 0; st < 3; ++st) {
     const double *V = Vs[st];
     hv1(h, V, h->C);
-    gather(h, h->C, h->T1, false);
-    pressure(h, V, h->pres);
-    phase2(h, V, h->pres, h->T1, h->C);
-    gather(h, h->C, h->sF[st], true);
+    gather(h, h->C, h->sT1[st], false);
+    pressure(h, V, h->sP[st]);
+    phase2(h, V, h->sP[st], h->sT1[st], h->C);
     if (st == 0) {
-      a.kout = h->k1; a.Vout = h->Vst;
+      a.kout = h->k1; a.Vout = h->sV2;
       column<0>(h, a);
-      CK(cudaMemcpyAsync(h->sV2, h->Vst, SV * 8, cudaMemcpyDeviceToDevice, h->stream));
     } else if (st == 1) {
-      a.kout = h->k2; a.Vout = h->Vst;
+      a.kout = h->k2; a.Vout = h->sV3;
       column<1>(h, a);
-      CK(cudaMemcpyAsync(h->sV3, h->Vst, SV * 8, cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+      a.kout = h->sk3; a.Vout = h->Vst;   // U1 itself is not needed
+      column<2>(h, a);
     }
   }
   // reverse: U1 = U0 + sum m_i k_i; k_i = L (F(V_i) + sum_j c_ij/dt k_j); V_i = U0 + sum_j a_ij k_j
-  for (int i = 0; i < 3; ++i) lincomb(h, h->aLk[i], rk.m[i], L);
-  lincomb(h, h->aLV, 1.0, L);
+  CK(cudaMemsetAsync(h->aLV, 0, SV * 8, h->stream));
+  const long long n = (long long)SV;
+  const unsigned nb = (unsigned)((n + 255) / 256);
   for (int st = 2; st >= 0; --st) {
     const double cA = st >= 1 ? rk.c[st][0] / dt : 0.0, cB = st == 2 ? rk.c[st][1] / dt : 0.0;
-    rc = column_adj(h, h->aLk[st], h->sF[st], st >= 1 ? h->k1 : nullptr, cA, st == 2 ? h->k2 : nullptr, cB, Ud,
-                    fac, h->aAR, h->aLV);
+    const double *mu = st == 2 ? L : h->aLk[st];
+    rc = column_adj(h, mu, st == 2 ? rk.m[2] : 1.0, ks[st], Ud, fac, h->aAR, h->aLV);
     if (rc) return rc;
-    rc = rhs_adjoint_core(h, Vs[st], h->aAR, h->aLt);
+    rc = rhs_adjoint_core(h, Vs[st], h->aAR, h->aLt, h->sT1[st], h->sP[st]);
     if (rc) return rc;
     // r_st = F(V_st) + c_st0/dt k1 + c_st1/dt k2; V_st = U0 + a_st0 k1 + a_st1 k2
-    if (st >= 1) lincomb(h, h->aLk[0], 1.0, h->aLk[0], cA, h->aAR, rk.a[st][0], h->aLt);
-    if (st == 2) lincomb(h, h->aLk[1], 1.0, h->aLk[1], cB, h->aAR, rk.a[st][1], h->aLt);
-    lincomb(h, h->aLV, 1.0, h->aLV, 1.0, h->aLt);
+    if (st == 2)
+      k_adj_update<<<nb, 256, 0, h->stream>>>(n, L, h->aAR, h->aLt, h->aLV, h->aLk[0], h->aLk[1], rk.m[0], rk.m[1],
+                                               cA, cB, rk.a[2][0], rk.a[2][1]);
+    else if (st == 1)
+      k_adj_update<<<nb, 256, 0, h->stream>>>(n, nullptr, h->aAR, h->aLt, h->aLV, h->aLk[0], nullptr, 0.0, 0.0, cA,
+                                               0.0, rk.a[1][0], 0.0);
+    else
+      k_adj_update<<<nb, 256, 0, h->stream>>>(n, nullptr, nullptr, h->aLt, h->aLV, nullptr, nullptr, 0.0, 0.0, 0.0,
+                                               0.0, 0.0, 0.0);
+    CK(cudaGetLastError());
   }
   if (is_device_ptr(Lin)) CK(cudaMemcpyAsync(Lin, h->aLV, SV * 8, cudaMemcpyDeviceToDevice, h->stream));
   else CK(cudaMemcpyAsync(Lin, h->aLV, SV * 8, cudaMemcpyDeviceToHost, h->stream));

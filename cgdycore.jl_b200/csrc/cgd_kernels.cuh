@@ -617,6 +617,7 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
         // Vout may alias Vn: this lane alone reads and writes index o
         const double vn = A.Vn[o];
         A.Vout[o] = vn + A.rk.m[0] * s1[it][sf] + A.rk.m[1] * s2[it][sf] + A.rk.m[2] * k;
+        if (A.kout) A.kout[o] = k;   // the last stage's k of rho, w, rho*theta (adjoint replay only)
       } else {
         A.kout[o] = k;
       }
