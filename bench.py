@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision sub-measurement")
     ap.add_argument("--mixed-days", type=float, default=1.0, help="simulated days of the mixed accuracy run")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint sub-measurement")
+    ap.add_argument("--adjoint-window", type=int, default=30,
+                    help="steps of the checkpointed gradient in the adjoint sub-measurement")
     return ap.parse_args()
 
 
@@ -307,6 +310,71 @@ def run_mixed(args, cfg, rank, ranks, U0, fp64_value, torch):
                     "profile; FP64 vertical terms, column Jacobian/Schur solve and reductions"}
 
 
+def run_adjoint(args, rank, ranks, torch):
+    """The hand-written adjoint on the drop-in grid without tracers
+    (physics.CONFIGS['adjoint']), device-resident: the forward step, one step
+    adjoint (forward replay of the step + reverse), the tendency and its
+    adjoint, each timed with CUDA events on the library's stream (max over
+    ranks), and a checkpointed gradient over args.adjoint_window steps against
+    the forward run of the same window."""
+    from cgd_b200 import setup
+    from cgd_b200 import physics as Ph
+    acfg = Ph.CONFIGS["adjoint"]
+    d, U0, _ = setup(member_config(acfg, rank))
+    stream = torch.cuda.ExternalStream(d.stream())
+    dt = acfg.dt
+    U = torch.from_numpy(np.ascontiguousarray(U0.transpose(2, 1, 0))).cuda()
+    d.time_stepper(U, dt, max(3, args.warmup))   # a state with vertical motion
+    gen = torch.Generator(device=U.device).manual_seed(20261203 + rank)
+    L = torch.randn(U.shape, dtype=U.dtype, device=U.device, generator=gen)
+    out = torch.empty_like(U)
+    V = U.clone()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, n):
+        for _ in range(3):
+            fn()
+        ranks.barrier()
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return ranks.max(e0.elapsed_time(e1) / n)
+
+    n = max(3, min(args.steps, 20))
+    fwd = timed(lambda: d.time_stepper(V, dt, n), 1) / n   # captured steps, as in the headline
+    adj = timed(lambda: d.ros_step_adjoint(U, L, dt, out), n)
+    rhs = timed(lambda: d.fcn(U, out), n)
+    rhs_adj = timed(lambda: d.fcn_adjoint(U, L, out), n)
+    W = args.adjoint_window
+    ranks.barrier()
+    e0.record(stream)
+    V.copy_(U)
+    d.time_stepper(V, dt, W)
+    e1.record(stream)
+    e1.synchronize()
+    fwd_w = ranks.max(e0.elapsed_time(e1))
+    e0.record(stream)
+    g = d.steps_adjoint(U, L, dt, W)
+    e1.record(stream)
+    e1.synchronize()
+    grad_w = ranks.max(e0.elapsed_time(e1))
+    finite = bool(torch.isfinite(g).all().item())
+    d.close()
+    return {"config": {"workload": "adjoint", "nPanel": acfg.nPanel, "OrdPoly": acfg.OrdPoly, "nz": acfg.nz,
+                       "NumTr": acfg.NumTr, "dt": dt},
+            "forward_step_ms": fwd, "step_adjoint_ms": adj, "step_ratio": adj / fwd,
+            "tendency_ms": rhs, "tendency_adjoint_ms": rhs_adj, "tendency_ratio": rhs_adj / rhs,
+            "checkpointed_gradient": {"steps": W, "checkpoint_every": max(1, int(round(W ** 0.5))),
+                                      "forward_ms": fwd_w, "gradient_ms": grad_w, "ratio": grad_w / fwd_w,
+                                      "finite": finite},
+            "step_adjoint": "forward replay of the step keeping stage states, phase-1 caches, pressures and k; "
+                            "reverse: transposed column Schur solve with band derivatives, tendency adjoint "
+                            "(phase 2 and phase 1 with their transposed DSS), stage combinations"}
+
+
 def run_ensemble(args, rank, world, local):
     """Batched-ensemble workload (physics.ENSEMBLE): every rank advances its
     own 48-member ensemble, one CUDA graph per ensemble step.  Times K steps
@@ -449,6 +517,9 @@ def run_ours(args, cfg, rank, world, local):
     mixed = None
     if args.precision == "fp64" and not args.no_mixed:
         mixed = run_mixed(args, cfg, rank, ranks, U0, value, torch)
+    adjoint = None
+    if args.precision == "fp64" and not args.no_adjoint:
+        adjoint = run_adjoint(args, rank, ranks, torch)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -488,6 +559,7 @@ def run_ours(args, cfg, rank, world, local):
             "kernel_share": shares,
             "e2e": e2e,
             "mixed": mixed,
+            "adjoint": adjoint,
             "gpu_launches": 15 * args.steps,
             "cpu_baseline": cpu,
             "clocks": clk,

@@ -17,6 +17,9 @@ libcgd_b200.so:
   rosenbrock_schur(U, dt)     Integration.RosenbrockSchur! (RosenbrockSchur.jl:1)
   time_stepper(U, dt, n)      the Rosenbrock branch of TimeStepper! (TimeStepper.jl:103-124)
   mass_integral(U)            Parallels.GlobalIntegral (Exchange.jl:1163)
+  fcn_adjoint(U, LF)          (no counterpart) (dF/dU)^T LF
+  ros_step_adjoint(U0, L, dt) (no counterpart) adjoint of one step
+  steps_adjoint(U0, L, dt, n) (no counterpart) checkpointed n-step gradient
   ==========================  ==============================================
 
 State arrays are (nz, NumG, NV) in column-major order: a Fortran-ordered
@@ -50,6 +53,26 @@ def _ptr(a, shape=None, writable=False):
             raise ValueError("tensor has the wrong number of elements")
         return a.data_ptr()
     raise TypeError("expected a numpy array or a torch tensor")
+
+
+def _copy(a):
+    """A copy of a state array: Fortran-ordered for numpy, a clone for torch."""
+    if isinstance(a, np.ndarray):
+        return np.array(a, order="F", copy=True)
+    return a.clone()
+
+
+def _assign(dst, src):
+    if isinstance(dst, np.ndarray):
+        dst[...] = src
+    else:
+        dst.copy_(src)
+
+
+def _empty_like(a):
+    if isinstance(a, np.ndarray):
+        return np.empty_like(a, order="F")
+    return a.new_empty(a.shape)
 
 
 class Dycore:
@@ -131,25 +154,29 @@ class Dycore:
         chaining ros_step_adjoint backwards over checkpoints: the forward run
         keeps the state every `every` steps (default about sqrt(nsteps)), and
         the reverse sweep recomputes each segment's states from its
-        checkpoint, so at most nsteps/every + every states are held."""
+        checkpoint, so at most nsteps/every + every states are held.  The
+        arrays may be host (numpy) or device (torch) arrays; checkpoints stay
+        where U0 is."""
         nsteps = int(nsteps)
         every = max(1, int(round(nsteps ** 0.5))) if every is None else max(1, int(every))
-        checkpoints = {0: np.array(U0, order="F", copy=True)}
-        V = checkpoints[0].copy(order="F")
+        # one working state for every forward step, so the library's captured
+        # step (bound to the state's address) is reused
+        checkpoints = {0: _copy(U0)}
+        work = _copy(U0)
         for s in range(1, nsteps):
-            self.time_stepper(V, dt, 1)
+            self.time_stepper(work, dt, 1)
             if s % every == 0:
-                checkpoints[s] = V.copy(order="F")
-        L = np.array(Lout, order="F", copy=True)
+                checkpoints[s] = _copy(work)
+        L = _copy(Lout)
         top = nsteps
         for start in sorted(checkpoints, reverse=True):
             seg = [checkpoints[start]]
+            _assign(work, seg[0])
             for _ in range(start + 1, top):
-                W = seg[-1].copy(order="F")
-                self.time_stepper(W, dt, 1)
-                seg.append(W)
+                self.time_stepper(work, dt, 1)
+                seg.append(_copy(work))
             for W in reversed(seg):
-                L = self.ros_step_adjoint(W, L, dt)
+                L = self.ros_step_adjoint(W, L, dt, _empty_like(L))
             top = start
         return L
 

@@ -171,4 +171,26 @@ function step!(b::Batch, states, dts::Vector{Float64}; nsteps = 1)
   end
 end
 
+# Adjoints (no counterpart in the reference; FP64 handles without tracers).
+# FcnAdjointB200!: LU = (dF/dU)^T LF at U, F being FcnB200!'s tendency.
+function FcnAdjointB200!(LU, U, LF, CG, Metric, Phys, Global)
+  h = handle(CG, Metric, Phys, Global)
+  GC.@preserve LU U LF begin
+    check(ccall((:cgd_rhs_adjoint, libcgd), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                h.ptr, dptr(U), dptr(LF), dptr(LU)), "cgd_rhs_adjoint")
+  end
+end
+
+# RosenbrockStepAdjointB200!: Lin = (dU1/dU0)^T Lout for one step
+# U1 = RosenbrockSchurB200!(U0, dt); U0 is not modified.  A gradient over
+# many steps chains this call backwards over stored (checkpointed) states.
+function RosenbrockStepAdjointB200!(Lin, U0, Lout, dt, CG, Metric, Phys, Global)
+  h = handle(CG, Metric, Phys, Global)
+  GC.@preserve Lin U0 Lout begin
+    check(ccall((:cgd_ros_step_adjoint, libcgd), Cint,
+                (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Cdouble),
+                h.ptr, dptr(U0), dptr(Lout), dptr(Lin), dt), "cgd_ros_step_adjoint")
+  end
+end
+
 end # module
