@@ -316,7 +316,8 @@ def run_adjoint(args, rank, ranks, torch):
     adjoint (forward replay of the step + reverse), the tendency and its
     adjoint, each timed with CUDA events on the library's stream (max over
     ranks), and a checkpointed gradient over args.adjoint_window steps against
-    the forward run of the same window."""
+    the forward run of the same window (every state kept when they fit in
+    16 GiB, as Dycore.steps_adjoint does by default)."""
     from cgd_b200 import setup
     from cgd_b200 import physics as Ph
     acfg = Ph.CONFIGS["adjoint"]
@@ -362,12 +363,13 @@ def run_adjoint(args, rank, ranks, torch):
     e1.synchronize()
     grad_w = ranks.max(e0.elapsed_time(e1))
     finite = bool(torch.isfinite(g).all().item())
+    every = d.checkpoint_every(W)
     d.close()
     return {"config": {"workload": "adjoint", "nPanel": acfg.nPanel, "OrdPoly": acfg.OrdPoly, "nz": acfg.nz,
                        "NumTr": acfg.NumTr, "dt": dt},
             "forward_step_ms": fwd, "step_adjoint_ms": adj, "step_ratio": adj / fwd,
             "tendency_ms": rhs, "tendency_adjoint_ms": rhs_adj, "tendency_ratio": rhs_adj / rhs,
-            "checkpointed_gradient": {"steps": W, "checkpoint_every": max(1, int(round(W ** 0.5))),
+            "checkpointed_gradient": {"steps": W, "checkpoint_every": every,
                                       "forward_ms": fwd_w, "gradient_ms": grad_w, "ratio": grad_w / fwd_w,
                                       "finite": finite},
             "step_adjoint": "forward replay of the step keeping stage states, phase-1 caches, pressures and k; "

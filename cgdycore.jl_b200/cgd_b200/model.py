@@ -149,16 +149,25 @@ class Dycore:
                    "cgd_ros_step_adjoint")
         return Lin
 
-    def steps_adjoint(self, U0, Lout, dt, nsteps, every=None):
+    def checkpoint_every(self, nsteps, mem_budget=16 << 30):
+        """Checkpoint spacing of steps_adjoint: every state when the n states
+        fit in mem_budget bytes, else about sqrt(n) (at most n/every + every
+        states held)."""
+        state_bytes = int(np.prod(self.shape)) * 8
+        if int(nsteps) * state_bytes <= mem_budget:
+            return 1
+        return max(1, int(round(int(nsteps) ** 0.5)))
+
+    def steps_adjoint(self, U0, Lout, dt, nsteps, every=None, mem_budget=16 << 30):
         """(dU_n/dU0)^T Lout for n = nsteps Rosenbrock-W steps from U0, by
         chaining ros_step_adjoint backwards over checkpoints: the forward run
-        keeps the state every `every` steps (default about sqrt(nsteps)), and
+        keeps the state every `every` steps (default: checkpoint_every), and
         the reverse sweep recomputes each segment's states from its
         checkpoint, so at most nsteps/every + every states are held.  The
         arrays may be host (numpy) or device (torch) arrays; checkpoints stay
         where U0 is."""
         nsteps = int(nsteps)
-        every = max(1, int(round(nsteps ** 0.5))) if every is None else max(1, int(every))
+        every = self.checkpoint_every(nsteps, mem_budget) if every is None else max(1, int(every))
         # one working state for every forward step, so the library's captured
         # step (bound to the state's address) is reused
         checkpoints = {0: _copy(U0)}
