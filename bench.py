@@ -48,8 +48,10 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision sub-measurement")
     ap.add_argument("--mixed-days", type=float, default=1.0, help="simulated days of the mixed accuracy run")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint sub-measurement")
-    ap.add_argument("--adjoint-window", type=int, default=30,
-                    help="steps of the checkpointed gradient in the adjoint sub-measurement")
+    ap.add_argument("--adjoint-steps", "--adjoint-window", dest="adjoint_steps", type=int, default=120,
+                    help="steps of the adjoint sensitivity study (120 x 120 s = 4 h)")
+    ap.add_argument("--adjoint-fd", action="store_true",
+                    help="add central-difference checks of the sensitivity gradient (about a minute)")
     return ap.parse_args()
 
 
@@ -312,19 +314,27 @@ def run_mixed(args, cfg, rank, ranks, U0, fp64_value, torch):
 
 def run_adjoint(args, rank, ranks, torch):
     """The hand-written adjoint on the drop-in grid without tracers
-    (physics.CONFIGS['adjoint']), device-resident: the forward step, one step
-    adjoint (forward replay of the step + reverse), the tendency and its
-    adjoint, each timed with CUDA events on the library's stream (max over
-    ranks), and a checkpointed gradient over args.adjoint_window steps against
-    the forward run of the same window (every state kept when they fit in
-    16 GiB, as Dycore.steps_adjoint does by default)."""
+    (physics.CONFIGS['adjoint']), device-resident, timed with CUDA events on
+    the library's stream (max over ranks):
+      * the forward step, one step adjoint (replay + reverse), the tendency
+        and its adjoint, at a state with vertical motion;
+      * the sensitivity study (physics.ADJOINT_STUDY): J = mean squared
+        lowest-layer pressure anomaly over the 10x10-degree box at 50N 60E
+        after args.adjoint_steps steps from the baroclinic-wave state, its
+        gradient with a checkpoint every 8 steps, against the forward run of
+        the same steps;
+      * with args.adjoint_fd, central differences of J along seeded random
+        unit directions at several step sizes."""
     from cgd_b200 import setup
     from cgd_b200 import physics as Ph
+    from cgd_b200.adjoint import BoxPressureFunctional, box_columns
     acfg = Ph.CONFIGS["adjoint"]
+    study = Ph.ADJOINT_STUDY
     d, U0, _ = setup(member_config(acfg, rank))
     stream = torch.cuda.ExternalStream(d.stream())
     dt = acfg.dt
-    U = torch.from_numpy(np.ascontiguousarray(U0.transpose(2, 1, 0))).cuda()
+    Ub = torch.from_numpy(np.ascontiguousarray(U0.transpose(2, 1, 0))).cuda()   # baroclinic-wave state
+    U = Ub.clone()
     d.time_stepper(U, dt, max(3, args.warmup))   # a state with vertical motion
     gen = torch.Generator(device=U.device).manual_seed(20261203 + rank)
     L = torch.randn(U.shape, dtype=U.dtype, device=U.device, generator=gen)
@@ -349,32 +359,56 @@ def run_adjoint(args, rank, ranks, torch):
     adj = timed(lambda: d.ros_step_adjoint(U, L, dt, out), n)
     rhs = timed(lambda: d.fcn(U, out), n)
     rhs_adj = timed(lambda: d.fcn_adjoint(U, L, out), n)
-    W = args.adjoint_window
+
+    W = args.adjoint_steps
+    box = box_columns(d.grid, study["box_lat"], study["box_lon"])
+    Jf = BoxPressureFunctional(d, dt, W, box=box, every=study["every"])
     ranks.barrier()
     e0.record(stream)
-    V.copy_(U)
+    V.copy_(Ub)
     d.time_stepper(V, dt, W)
     e1.record(stream)
     e1.synchronize()
     fwd_w = ranks.max(e0.elapsed_time(e1))
     e0.record(stream)
-    g = d.steps_adjoint(U, L, dt, W)
+    J, G = Jf.value_and_grad(Ub)
     e1.record(stream)
     e1.synchronize()
     grad_w = ranks.max(e0.elapsed_time(e1))
-    finite = bool(torch.isfinite(g).all().item())
-    every = d.checkpoint_every(W)
+    finite = bool(torch.isfinite(G).all().item())
+    res = {"config": {"workload": "adjoint", "nPanel": acfg.nPanel, "OrdPoly": acfg.OrdPoly, "nz": acfg.nz,
+                      "NumTr": acfg.NumTr, "dt": dt},
+           "forward_step_ms": fwd, "step_adjoint_ms": adj, "step_ratio": adj / fwd,
+           "tendency_ms": rhs, "tendency_adjoint_ms": rhs_adj, "tendency_ratio": rhs_adj / rhs,
+           "sensitivity": {"J": J, "box_columns": int(box.size), "steps": W, "simulated_hours": W * dt / 3600.0,
+                           "checkpoint_every": study["every"], "forward_ms": fwd_w, "gradient_ms": grad_w,
+                           "ratio": grad_w / fwd_w, "finite": finite,
+                           "functional": "mean over the box columns of (p1(U_n) - p1(U_0))^2, p1 the "
+                                         "lowest-layer pressure, box 45-55N 55-65E"},
+           "step_adjoint": "forward replay of the step keeping stage states, phase-1 caches, pressures and k; "
+                           "reverse: transposed column Schur solve with band derivatives, tendency adjoint "
+                           "(phase 2 and phase 1 with their transposed DSS), stage combinations"}
+    if args.adjoint_fd:
+        # central differences along seeded unit directions of the FP64 state space
+        rng = np.random.default_rng(study["fd_seed"])
+        nrm = float(torch.linalg.norm(Ub))
+        work = Ub.clone()
+        rels = (1e-7, 1e-8, 1e-9)
+        rows = []
+        for _ in range(study["fd_dirs"]):
+            v = torch.from_numpy(rng.standard_normal(tuple(Ub.shape))).to(Ub.device)
+            v /= torch.linalg.norm(v)
+            ad = float(torch.sum(G * v))
+            errs = []
+            for rel in rels:
+                eps = rel * nrm
+                fd = Jf.diff(Ub + eps * v, Ub - eps * v, work) / (2 * eps)
+                errs.append(abs(fd - ad) / abs(fd))
+            rows.append({"adjoint": ad, "rel_err": errs})
+        res["sensitivity"]["fd_check"] = {"directions": rows, "rel_steps": list(rels),
+                                          "step": "eps = rel * |U0|_2 along unit directions of i.i.d. N(0,1)"}
     d.close()
-    return {"config": {"workload": "adjoint", "nPanel": acfg.nPanel, "OrdPoly": acfg.OrdPoly, "nz": acfg.nz,
-                       "NumTr": acfg.NumTr, "dt": dt},
-            "forward_step_ms": fwd, "step_adjoint_ms": adj, "step_ratio": adj / fwd,
-            "tendency_ms": rhs, "tendency_adjoint_ms": rhs_adj, "tendency_ratio": rhs_adj / rhs,
-            "checkpointed_gradient": {"steps": W, "checkpoint_every": every,
-                                      "forward_ms": fwd_w, "gradient_ms": grad_w, "ratio": grad_w / fwd_w,
-                                      "finite": finite},
-            "step_adjoint": "forward replay of the step keeping stage states, phase-1 caches, pressures and k; "
-                            "reverse: transposed column Schur solve with band derivatives, tendency adjoint "
-                            "(phase 2 and phase 1 with their transposed DSS), stage combinations"}
+    return res
 
 
 def run_ensemble(args, rank, world, local):

@@ -6,7 +6,10 @@ Host-side modules:
   grid     cubed-sphere topology, Glob numbering, GLL element, metric, mass
   physics  physical parameters, baroclinic-wave initial state, run configs
   model    Dycore: fcn / fcn_prepare / jac / schur_solve / rosenbrock_schur /
-           time_stepper over libcgd_b200.so; Ensemble: batched members
+           time_stepper over libcgd_b200.so, and their adjoints
+           (fcn_adjoint / ros_step_adjoint / steps_adjoint); Ensemble:
+           batched members
+  adjoint  gradients of scalar functionals of a run (BoxPressureFunctional)
   build    compiles libcgd_b200.so for sm_100a
 """
 from . import grid, physics  # noqa: F401

@@ -27,7 +27,7 @@ EXPORTS = [
     "cgd_create", "cgd_destroy", "cgd_prepare", "cgd_hypervisc_phase1", "cgd_rhs", "cgd_jac",
     "cgd_schur_solve", "cgd_ros_step", "cgd_mass_integral", "cgd_jac_schur_solve_noalloc", "cgd_get_stream",
     "cgd_kernel_times", "cgd_strerror", "cgd_version",
-    "cgd_rhs_adjoint", "cgd_ros_step_adjoint", "cgd_batch_create", "cgd_batch_step", "cgd_batch_tuning", "cgd_batch_get_stream", "cgd_batch_destroy",
+    "cgd_rhs_adjoint", "cgd_ros_step_adjoint", "cgd_set_caller_stream", "cgd_batch_create", "cgd_batch_step", "cgd_batch_tuning", "cgd_batch_get_stream", "cgd_batch_destroy",
 ]
 
 
@@ -68,6 +68,8 @@ def lib(exact=False):
         L.cgd_rhs_adjoint.restype = ctypes.c_int
         L.cgd_ros_step_adjoint.argtypes = [vp, vp, vp, vp, ctypes.c_double]
         L.cgd_ros_step_adjoint.restype = ctypes.c_int
+        L.cgd_set_caller_stream.argtypes = [vp, vp]
+        L.cgd_set_caller_stream.restype = ctypes.c_int
         for f in ("cgd_prepare", "cgd_hypervisc_phase1", "cgd_rhs", "cgd_jac"):
             getattr(L, f).argtypes = [vp, vp, vp]
             getattr(L, f).restype = ctypes.c_int

@@ -165,7 +165,8 @@ class Dycore:
         the reverse sweep recomputes each segment's states from its
         checkpoint, so at most nsteps/every + every states are held.  The
         arrays may be host (numpy) or device (torch) arrays; checkpoints stay
-        where U0 is."""
+        where U0 is.  Lout may be a function of the final state U_n that
+        returns the adjoint seed (U_n comes from the same forward run)."""
         nsteps = int(nsteps)
         every = self.checkpoint_every(nsteps, mem_budget) if every is None else max(1, int(every))
         # one working state for every forward step, so the library's captured
@@ -176,7 +177,13 @@ class Dycore:
             self.time_stepper(work, dt, 1)
             if s % every == 0:
                 checkpoints[s] = _copy(work)
-        L = _copy(Lout)
+        if callable(Lout):
+            Un = _copy(work)
+            if nsteps > 0:
+                self.time_stepper(Un, dt, 1)
+            L = Lout(Un)
+        else:
+            L = _copy(Lout)
         top = nsteps
         for start in sorted(checkpoints, reverse=True):
             seg = [checkpoints[start]]
@@ -224,6 +231,14 @@ class Dycore:
         _lib.check(self._L.cgd_mass_integral(self.h, _ptr(U, self.shape), self._mmass.ctypes.data,
                                                 ctypes.byref(out)), "cgd_mass_integral")
         return out.value
+
+    def set_caller_stream(self, stream=None):
+        """The stream whose queued work every call waits for before it reads
+        its arguments: a cudaStream_t as an integer (e.g.
+        torch.cuda.current_stream().cuda_stream), or None for the legacy
+        default stream, PyTorch's default."""
+        _lib.check(self._L.cgd_set_caller_stream(self.h, ctypes.c_void_p(stream) if stream else None),
+                   "cgd_set_caller_stream")
 
     def stream(self):
         """The library's cudaStream_t as an integer handle."""

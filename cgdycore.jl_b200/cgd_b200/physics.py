@@ -177,6 +177,12 @@ class RunConfig:
         return G.vertical_quadratic(self.nz, self.H)
 
 
+# The adjoint workload's sensitivity study: J = mean squared lowest-layer
+# pressure anomaly over the 10x10-degree box centred at 50N, 60E after 4 h
+# (CONFIGS["adjoint"]: 120 steps of 120 s), gradient through the adjoint with
+# a checkpoint every 8 steps, checked along seeded random directions.
+ADJOINT_STUDY = {"box_lat": (45.0, 55.0), "box_lon": (55.0, 65.0), "every": 8, "fd_seed": 20261205, "fd_dirs": 8}
+
 CONFIGS = {
     # small CPU-runnable case: 10 steps at dt 600 s
     "small": RunConfig("small", 6, 4, 10, 0, 600.0, 10, "uniform"),

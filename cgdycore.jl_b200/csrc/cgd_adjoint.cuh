@@ -573,9 +573,20 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS, 2) k_phase2_adj(const GP P, co
     const double a311 = AW(A_D311, pl, ID), a321 = AW(A_D321, pl, ID), a331 = AW(A_D331, pl, ID);
     const double b310 = AW(A_D310, pl + 1, ID), b320 = AW(A_D320, pl + 1, ID), b330 = AW(A_D330, pl + 1, ID);
     const double wCon = rL * (a311 * uL + a321 * vL + a331 * wI) + rR * (b310 * uR + b320 * vR + b330 * wI);
+    // A mass flux within the rounding of its dot products (metric row times
+    // velocity) has no direction: at a state with w = 0 over flat orography,
+    // the horizontal metric entries of the row (analytically zero) leave
+    // |wCon| ~ 1e-16 |row| |velocity| with a sign set by rounding.  There the
+    // upwind flux sits on its kink and the adjoint takes the symmetric slope
+    // (as for wCon == 0), which central differences see, instead of the side
+    // the rounding picked.
+    const double wMag =
+        fabs(rL) * (fabs(a311) + fabs(a321) + fabs(a331)) * (fabs(uL) + fabs(vL) + fabs(wI)) +
+        fabs(rR) * (fabs(b310) + fabs(b320) + fabs(b330)) * (fabs(uR) + fabs(vR) + fabs(wI));
+    const double wEff = fabs(wCon) <= 1e-13 * wMag ? 0.0 : wCon;
     double aw, aLL, aL, aR, aRR;
     upwind_adj(AW(A_TH, lm - (L0 - 2), ID), AW(A_TH, pl, ID), AW(A_TH, pl + 1, ID), AW(A_TH, lp2 - (L0 - 2), ID), kR1,
-               kL1, kL2, kR2, wCon, aF, aw, aLL, aL, aR, aRR);
+               kL1, kL2, kR2, wEff, aF, aw, aLL, aL, aR, aRR);
     add_theta(lm, aLL);
     add_theta(il, aL);
     add_theta(il + 1, aR);

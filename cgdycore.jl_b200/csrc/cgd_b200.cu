@@ -40,6 +40,12 @@ struct cgd_handle {
   int N = 0, DoF = 0, nz = 0, NF = 0, NumG = 0, NumTr = 0, NV = 0;
   int device = 0;
   cudaStream_t stream = nullptr;
+  // Work the caller queued before a call is ordered before the call's own
+  // work: every entry records order_ev on the caller's stream (the legacy
+  // default stream unless cgd_set_caller_stream names another) and makes the
+  // library's stream wait for it.
+  cudaStream_t caller = cudaStreamLegacy;
+  cudaEvent_t order_ev = nullptr;
   std::vector<Buf> bufs;
   double *met = nullptr, *M = nullptr, *dz = nullptr;
   int *glob = nullptr, *inv_ptr = nullptr;
@@ -460,8 +466,10 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
       }
 
   // ---- device resources
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->order_ev, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
+    if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return CGD_ERR_CUDA;
   }
@@ -546,8 +554,17 @@ void cgd_destroy(cgd_handle *h)
   for (auto &b : h->bufs) cudaFree(b.p);
   for (int i = 0; i <= NPROF; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+  if (h->order_ev) cudaEventDestroy(h->order_ev);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
+}
+
+// Order the call after the caller's queued work (see cgd_handle::caller).
+static int enter(cgd_handle *h)
+{
+  CK(cudaEventRecord(h->order_ev, h->caller));
+  CK(cudaStreamWaitEvent(h->stream, h->order_ev, 0));
+  return CGD_OK;
 }
 
 // Stage a state/tendency pointer: device pointers are used in place, host
@@ -573,6 +590,7 @@ static int finish(cgd_handle *h)
 int cgd_prepare(cgd_handle *h, const double *U, double *p)
 {
   if (!h || !U || !p) return CGD_ERR_INVALID_ARG;
+  if (int erc = enter(h)) return erc;
   double *Ud;
   int rc = stage_in(h, U, h->Ubuf, true, &Ud);
   if (rc) return rc;
@@ -587,6 +605,7 @@ int cgd_prepare(cgd_handle *h, const double *U, double *p)
 int cgd_hypervisc_phase1(cgd_handle *h, const double *U, double *Temp1)
 {
   if (!h || !U || !Temp1) return CGD_ERR_INVALID_ARG;
+  if (int erc = enter(h)) return erc;
   double *Ud;
   int rc = stage_in(h, U, h->Ubuf, true, &Ud);
   if (rc) return rc;
@@ -603,6 +622,7 @@ int cgd_hypervisc_phase1(cgd_handle *h, const double *U, double *Temp1)
 int cgd_rhs(cgd_handle *h, const double *U, double *F)
 {
   if (!h || !U || !F) return CGD_ERR_INVALID_ARG;
+  if (int erc = enter(h)) return erc;
   double *Ud;
   int rc = stage_in(h, U, h->Ubuf, true, &Ud);
   if (rc) return rc;
@@ -621,6 +641,7 @@ int cgd_rhs(cgd_handle *h, const double *U, double *F)
 int cgd_jac(cgd_handle *h, const double *U, double *bands)
 {
   if (!h || !U) return CGD_ERR_INVALID_ARG;
+  if (int erc = enter(h)) return erc;
   double *Ud;
   int rc = stage_in(h, U, h->Ubuf, true, &Ud);
   if (rc) return rc;
@@ -640,6 +661,7 @@ int cgd_schur_solve(cgd_handle *h, double *k, double *v, double fac)
 {
   if (!h || !k || !v || !(fac > 0)) return CGD_ERR_INVALID_ARG;
   if (!h->have_bands) return CGD_ERR_INVALID_ARG;
+  if (int erc = enter(h)) return erc;
   double *vd, *kd;
   int rc = stage_in(h, v, h->Ubuf, true, &vd);
   if (rc) return rc;
@@ -661,6 +683,7 @@ int cgd_schur_solve(cgd_handle *h, double *k, double *v, double fac)
 int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps)
 {
   if (!h || !U || !(dt > 0) || nsteps < 0) return CGD_ERR_INVALID_ARG;
+  if (int erc = enter(h)) return erc;
   double *Ud;
   int rc = stage_in(h, U, h->Ubuf, true, &Ud);
   if (rc) return rc;
@@ -703,6 +726,7 @@ int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps)
 int cgd_mass_integral(cgd_handle *h, const double *U, const double *MMass, double *out)
 {
   if (!h || !U || !MMass || !out) return CGD_ERR_INVALID_ARG;
+  if (int erc = enter(h)) return erc;
   double *Ud;
   int rc = stage_in(h, U, h->Ubuf, true, &Ud);
   if (rc) return rc;
@@ -845,6 +869,8 @@ int cgd_ros_step_adjoint(cgd_handle *h, const double *U0, const double *Lout, do
   if (h->mix || h->NumTr != 0) return CGD_ERR_UNSUPPORTED;
   int rc = adjoint_alloc(h, true);
   if (rc) return rc;
+  rc = enter(h);
+  if (rc) return rc;
   const size_t SV = (size_t)h->nz * h->NumG * h->NV;
   double *Ud;
   rc = stage_in(h, U0, h->Ubuf, true, &Ud);
@@ -924,6 +950,7 @@ int cgd_rhs_adjoint_impl(cgd_handle *h, const double *U, const double *LF, doubl
   if (h->mix || h->NumTr != 0) return CGD_ERR_UNSUPPORTED;
   const size_t S = (size_t)h->nz * h->NumG;
   int arc = adjoint_alloc(h, false);
+  if (!arc) arc = enter(h);
   if (arc) return arc;
   double *Ud;
   int rc = stage_in(h, U, h->Ubuf, true, &Ud);
@@ -947,6 +974,13 @@ extern "C" {
 int cgd_rhs_adjoint(cgd_handle *h, const double *U, const double *LF, double *LU)
 {
   return cgd_rhs_adjoint_impl(h, U, LF, LU);
+}
+
+int cgd_set_caller_stream(cgd_handle *h, void *stream)
+{
+  if (!h) return CGD_ERR_INVALID_ARG;
+  h->caller = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+  return CGD_OK;
 }
 
 int cgd_get_stream(cgd_handle *h, void **stream)
@@ -994,6 +1028,7 @@ struct cgd_batch {
   bool mix = false;
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaEvent_t order_ev = nullptr;   // orders a step after the first member's caller stream
   // work lists, one set per candidate order; order[ci] names it
   static constexpr int NORD = 3;
   WItem *w[NORD][4] = {};
@@ -1166,6 +1201,7 @@ int cgd_batch_create(cgd_handle *const *members, int32_t nmembers, int32_t flags
   do {
     cudaError_t e = cudaSetDevice(b->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->order_ev, cudaEventDisableTiming);
     if (e != cudaSuccess) { rc = batch_fail(b, e, "cgd_batch_create stream"); break; }
     const int nord = b->autotune ? cgd_batch::NORD : 1;
     for (int o = 0; o < nord && !rc; ++o) {
@@ -1201,6 +1237,7 @@ void cgd_batch_destroy(cgd_batch *b)
       if (b->w[o][k]) cudaFree(b->w[o][k]);
   }
   for (void *p : b->scratch) cudaFree(p);
+  if (b->order_ev) cudaEventDestroy(b->order_ev);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -1214,10 +1251,13 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
     if (!is_device_ptr(U[m])) return CGD_ERR_INVALID_ARG;
   }
   BCK(cudaSetDevice(b->device));
+  BCK(cudaEventRecord(b->order_ev, b->mem[0]->caller));
+  BCK(cudaStreamWaitEvent(b->stream, b->order_ev, 0));
   // mixed members: the reference profile from their first state
   for (int m = 0; m < nm; ++m) {
     cgd_handle *h = b->mem[m];
     if (h->mix && !h->have_ref) {
+      if (int erc = enter(h)) return erc;
       ensure_ref(h, U[m]);
       BCK(cudaStreamSynchronize(h->stream));
     }

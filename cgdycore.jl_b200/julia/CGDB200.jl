@@ -171,6 +171,35 @@ function step!(b::Batch, states, dts::Vector{Float64}; nsteps = 1)
   end
 end
 
+# The stream whose queued work every call waits for (a cudaStream_t; a
+# CUDA.jl caller passes CUDA.stream().handle); C_NULL = the legacy default stream.
+function set_caller_stream!(h::Handle, stream)
+  check(ccall((:cgd_set_caller_stream, libcgd), Cint, (Ptr{Cvoid}, Ptr{Cvoid}),
+              h.ptr, reinterpret(Ptr{Cvoid}, stream)), "cgd_set_caller_stream")
+end
+
+# Non-mutating forms of the step and the tendency (the functions the
+# ChainRulesCore rules in CGDB200Rules.jl differentiate).
+function RosenbrockStep(U, dt, CG, Metric, Phys, Global)
+  h = handle(CG, Metric, Phys, Global)
+  U1 = copy(U)
+  GC.@preserve U1 begin
+    check(ccall((:cgd_ros_step, libcgd), Cint, (Ptr{Cvoid}, Ptr{Float64}, Cdouble, Int32),
+                h.ptr, dptr(U1), dt, Int32(1)), "cgd_ros_step")
+  end
+  U1
+end
+
+function Fcn(U, CG, Metric, Phys, Global)
+  h = handle(CG, Metric, Phys, Global)
+  F = similar(U)
+  GC.@preserve F U begin
+    check(ccall((:cgd_rhs, libcgd), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}),
+                h.ptr, dptr(U), dptr(F)), "cgd_rhs")
+  end
+  F
+end
+
 # Adjoints (no counterpart in the reference; FP64 handles without tracers).
 # FcnAdjointB200!: LU = (dF/dU)^T LF at U, F being FcnB200!'s tendency.
 function FcnAdjointB200!(LU, U, LF, CG, Metric, Phys, Global)

@@ -21,8 +21,9 @@
  * State/tendency pointers may be device memory (zero copy, e.g. a CuArray
  * or a torch tensor) or host memory (staged through device buffers owned by
  * the handle); the library tells them apart with cudaPointerGetAttributes.
- * Every call is ordered on the handle's CUDA stream and returns when the
- * result is complete.  A handle is not thread safe.
+ * Every call waits for the work the caller has queued on its stream (see
+ * cgd_set_caller_stream), runs on the handle's CUDA stream and returns when
+ * the result is complete.  A handle is not thread safe.
  *
  * Every function returns CGD_OK (0) or a negative error code; no exception
  * crosses the ABI and no device trap is used.  cgd_strerror() names a code.
@@ -122,8 +123,9 @@ int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps);
 
 /* Adjoint of one Rosenbrock-W step U1 = step(U0, dt): Lin = (dU1/dU0)^T Lout
  * (all three (nz, NumG, NV)), FP64, no tracers (CGD_ERR_UNSUPPORTED
- * otherwise).  Replays the forward step from U0 (the three stage states and
- * tendencies, the bands), then runs the stages in reverse: the transposed
+ * otherwise).  Replays the forward step from U0 (keeping the stage states,
+ * phase-1 caches, pressures and k, and the bands), then runs the stages in
+ * reverse: the transposed
  * column Schur solve (including the derivative of the Jacobian bands with
  * respect to U0), the tendency adjoint at the stage state, and the stage
  * combinations.  Multi-step gradients chain this call over checkpointed
@@ -184,6 +186,18 @@ void cgd_batch_destroy(cgd_batch *b);
  * work or timing events with the library's.  No counterpart in the
  * reference (KernelAbstractions owns its queue). */
 int cgd_get_stream(cgd_handle *h, void **stream);
+
+/* Device arrays the caller passes may still be being written by work it
+ * queued on its own stream.  Every call first makes the handle's stream wait
+ * for that work (an event recorded on the caller's stream), so no explicit
+ * synchronisation is needed before a call; every call returns with its own
+ * work complete.  The caller's stream is the legacy default stream (the one
+ * PyTorch uses by default) unless set here: a cudaStream_t, or NULL for the
+ * legacy default stream again.  A CUDA.jl caller passes its task's stream.
+ * Batches follow the caller stream of their first member.  No counterpart
+ * in the reference (its kernels and arrays share one KernelAbstractions
+ * queue). */
+int cgd_set_caller_stream(cgd_handle *h, void *stream);
 
 /* Average duration (ms) of the last timed launches of each kernel family
  * recorded when CGD_PROFILE=1; names separated by ';'.  Diagnostics only. */
