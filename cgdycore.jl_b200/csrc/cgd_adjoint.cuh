@@ -757,12 +757,11 @@ __global__ void __launch_bounds__(256) k_adj_update(long long n, const double *_
 // The stage's k (kx), kept by the forward stage, gives everything else the
 // reverse needs: the tridiagonal solution x is its w field, and the
 // right-hand side of rho and rho*theta follows from SchurSolveB,
-// r0(l) = k0(l)/fac - JB(0,0,l) x(l) - JB(0,1,l-1) x(l-1) (r4 with JB(3,.)).  The forward sweep solves M x = b with M(i,i) = t1(i),
-// M(i+1,i) = t2(i), M(i,i+1) = t0(i+1) (the reference's triSolve!); here
-// M = L U with pivots d(i) and multipliers m(i) = t2(i)/d(i), and M^T y = ax is
-// U^T z = ax, L^T y = z.  One warp per column for the level-parallel parts;
-// the serial recurrences of the block's columns run together, one per lane of
-// the first warp.
+// r0(l) = k0(l)/fac - JB(0,0,l) x(l) - JB(0,1,l-1) x(l-1) (r4 with JB(3,.)).
+// The forward sweep solves M x = b with M(i,i) = t1(i), M(i+1,i) = t2(i),
+// M(i,i+1) = t0(i+1) (the reference's triSolve!); here M^T y = ax is solved by
+// the warp's lanes (warp_tri_solve on the transposed bands).  One warp per
+// column throughout.
 constexpr int CA_ARR = 18;   // per-warp arrays of nz entries
 
 __global__ void __launch_bounds__(32 * COL_WARPS, 3) k_column_adj(const GP P, const double *__restrict__ mu, double mus,
@@ -775,7 +774,7 @@ __global__ void __launch_bounds__(32 * COL_WARPS, 3) k_column_adj(const GP P, co
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g0 = blockIdx.x * COL_WARPS, g = g0 + warp;
   const int nz = P.nz, n = nz - 1, NV = P.NV, NumG = P.NumG;
-  const bool valid = g < NumG;   // no early return: the block synchronises
+  const bool valid = g < NumG;
   const int LS = nz;
   double *sw = csm + (size_t)warp * CA_ARR * LS;
   double *r0 = sw, *r4 = sw + LS, *av0 = sw + 2 * LS, *av4 = sw + 3 * LS;
@@ -825,34 +824,17 @@ __global__ void __launch_bounds__(32 * COL_WARPS, 3) k_column_adj(const GP P, co
               JB(0, 1, l) * av0[l + 1] + JB(3, 1, l) * av4[l + 1];
     }
   }
-  __syncthreads();
-  // 2. M^T y = ax for the block's columns, one lane each
-  if (threadIdx.x < COL_WARPS && g0 + (int)threadIdx.x < NumG) {
-    double *c = csm + (size_t)threadIdx.x * CA_ARR * LS;
-    const double *t0 = c + 12 * LS, *t1 = c + 13 * LS, *t2 = c + 14 * LS;
-    double *q = c + 17 * LS;     // multipliers m(i) (accR0 is not in use yet)
-    double *yy = c + 16 * LS;
-    double inv = 1.0 / t1[0];
-    double z = yy[0] * inv;
-    yy[0] = z;
-    for (int i = 0; i < n - 1; ++i) {
-      const double m = t2[i] * inv;
-      q[i] = m;
-      inv = 1.0 / (t1[i + 1] - m * t0[i + 1]);
-      z = (yy[i + 1] - t0[i + 1] * z) * inv;
-      yy[i + 1] = z;
-    }
-    for (int i = n - 2; i >= 0; --i) {
-      z = yy[i] - q[i] * z;
-      yy[i] = z;
-    }
-  }
-  __syncthreads();
-  if (!valid) return;
+  __syncwarp();
+  if (!valid) return;   // warp-uniform; nothing below synchronises the block
+  // 2. M^T y = ax with the warp's lanes: M^T(i,i) = t1(i), M^T(i+1,i) = t0(i+1),
+  //    M^T(i,i+1) = t2(i), i.e. warp_tri_solve with t0 and t2 exchanged and
+  //    shifted by one level; y overwrites ax
+  warp_tri_solve(tri + 2 * LS - 1, tri + LS, tri + 1, ay, ay, n, lane);
+  __syncwarp();
   // 3. adjoint of r, and the band adjoints (TriDiag, SchurSolveF, SchurSolveB)
   //    of interface l, whose share of level l is added here and whose share
   //    of level l+1 is passed on through aR0 / aR4
-  double *aR0 = accR0, *aR4 = tri + 1 * LS;   // the multipliers and t1 are dead after the sweep
+  double *aR0 = accR0, *aR4 = tri + 1 * LS;   // t1 is dead after the solve
   for (int l = lane; l < nz; l += 32) {
     const size_t o0 = l + (size_t)nz * g;
     double ar0 = av0[l], ar4 = av4[l];

@@ -419,6 +419,96 @@ __device__ __forceinline__ void jac_at(const GP &P, double RhoL, double RhoR, do
   jac_bands(P, RhoL, RhoR, RhoThL0, RhoThR0, dpdrhoth(P, RhoThL0), dpdrhoth(P, RhoThR0), dzL, dzR, jb);
 }
 
+// Solve M x = b for one column with the warp's 32 lanes (the fast build's
+// triSolve!).  M(i,i) = t1(i), M(i+1,i) = t2(i), M(i,i+1) = t0(i+1), n <= 64
+// rows; lane L holds rows 2L and 2L+1.  The Thomas recurrences become scans:
+//   pivots d(i) = t1(i) - t2(i-1) t0(i) / d(i-1) = p(i)/q(i), (p, q) the first
+//     column of the product M_i ... M_0 with M_i = [[t1(i), -t2(i-1) t0(i)], [1, 0]]
+//     (products rescaled by powers of two, which is exact);
+//   forward b'(i) = b(i) - t2(i-1)/d(i-1) b'(i-1), an affine prefix scan;
+//   back x(i) = (b'(i) - t0(i+1) x(i+1)) / d(i), an affine suffix scan.
+struct Mat2 {
+  double a, b, c, d;
+};
+__device__ __forceinline__ Mat2 mat2_mul(const Mat2 &x, const Mat2 &y)
+{
+  return {x.a * y.a + x.b * y.c, x.a * y.b + x.b * y.d, x.c * y.a + x.d * y.c, x.c * y.b + x.d * y.d};
+}
+__device__ __forceinline__ Mat2 mat2_scaled(Mat2 m)
+{
+  const double mx = fmax(fmax(fabs(m.a), fabs(m.b)), fmax(fabs(m.c), fabs(m.d)));
+  if (mx > 0.0) {
+    int e;
+    frexp(mx, &e);
+    m.a = ldexp(m.a, -e); m.b = ldexp(m.b, -e); m.c = ldexp(m.c, -e); m.d = ldexp(m.d, -e);
+  }
+  return m;
+}
+__device__ __forceinline__ Mat2 mat2_shfl_up(const Mat2 &m, int k)
+{
+  return {__shfl_up_sync(0xffffffffu, m.a, k), __shfl_up_sync(0xffffffffu, m.b, k),
+          __shfl_up_sync(0xffffffffu, m.c, k), __shfl_up_sync(0xffffffffu, m.d, k)};
+}
+__device__ __forceinline__ void warp_tri_solve(const double *t0, const double *t1, const double *t2,
+                                               const double *b, double *x, int n, int lane)
+{
+  constexpr unsigned FULL = 0xffffffffu;
+  const Mat2 I2 = {1.0, 0.0, 0.0, 1.0};
+  const int i0 = 2 * lane, i1 = i0 + 1;
+  auto mi = [&](int i) -> Mat2 {
+    if (i >= n) return I2;
+    return {t1[i], i > 0 ? -t2[i - 1] * t0[i] : 0.0, 1.0, 0.0};
+  };
+  const Mat2 A0 = mi(i0), A1 = mi(i1);
+  // pivots
+  Mat2 S = mat2_scaled(mat2_mul(A1, A0));
+#pragma unroll
+  for (int k = 1; k < 32; k <<= 1) {
+    Mat2 Sp = mat2_shfl_up(S, k);
+    if (lane < k) Sp = I2;
+    S = mat2_scaled(mat2_mul(S, Sp));
+  }
+  Mat2 E = mat2_shfl_up(S, 1);
+  if (lane == 0) E = I2;
+  const Mat2 P0 = mat2_scaled(mat2_mul(A0, E));
+  const Mat2 P1 = mat2_scaled(mat2_mul(A1, P0));
+  const double r0 = i0 < n ? P0.c / P0.a : 0.0;   // 1 / d(i0)
+  const double r1 = i1 < n ? P1.c / P1.a : 0.0;   // 1 / d(i1)
+  // forward substitution
+  const double rprev = __shfl_up_sync(FULL, r1, 1);   // 1 / d(i0 - 1)
+  const double a0 = i0 < n ? (i0 > 0 ? -t2[i0 - 1] * rprev : 0.0) : 1.0;
+  const double a1 = i1 < n ? -t2[i0] * r0 : 1.0;
+  const double c0 = i0 < n ? b[i0] : 0.0, c1 = i1 < n ? b[i1] : 0.0;
+  double CA = a1 * a0, CB = a1 * c0 + c1;
+#pragma unroll
+  for (int k = 1; k < 32; k <<= 1) {
+    double pA = __shfl_up_sync(FULL, CA, k), pB = __shfl_up_sync(FULL, CB, k);
+    if (lane < k) { pA = 1.0; pB = 0.0; }
+    CB = CA * pB + CB;
+    CA = CA * pA;
+  }
+  double yprev = __shfl_up_sync(FULL, CB, 1);
+  if (lane == 0) yprev = 0.0;
+  const double bp0 = a0 * yprev + c0, bp1 = a1 * bp0 + c1;
+  // back substitution
+  const double al0 = i0 + 1 < n ? -t0[i0 + 1] * r0 : 0.0, be0 = bp0 * r0;
+  const double al1 = i1 + 1 < n ? -t0[i1 + 1] * r1 : 0.0, be1 = bp1 * r1;
+  CA = al0 * al1;
+  CB = al0 * be1 + be0;
+#pragma unroll
+  for (int k = 1; k < 32; k <<= 1) {
+    double nA = __shfl_down_sync(FULL, CA, k), nB = __shfl_down_sync(FULL, CB, k);
+    if (lane + k >= 32) { nA = 1.0; nB = 0.0; }
+    CB = CA * nB + CB;
+    CA = CA * nA;
+  }
+  double xnext = __shfl_down_sync(FULL, CB, 1);
+  if (lane == 31) xnext = 0.0;
+  const double x1v = al1 * xnext + be1, x0v = al0 * x1v + be0;
+  if (i0 < n) x[i0] = x0v;
+  if (i1 < n) x[i1] = x1v;
+}
+
 template <int MODE, bool C32>
 __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const int bx)
 {
@@ -554,6 +644,14 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
 #pragma unroll
   for (int it = 0; it < 2; ++it)
     if (valid && lane + 32 * it < n) FV3(lane + 32 * it) = v3new[it];
+#ifdef CGD_FAST
+  // triSolve! as three warp scans over the column's levels (fast build);
+  // the result differs from the sequential sweep by rounding only
+  __syncwarp();
+  if (!valid) return;   // warp-uniform; nothing below synchronises the block
+  warp_tri_solve(tri, tri + LS, tri + 2 * LS, fv + LS, xs, n, lane);
+  __syncwarp();
+#else
   __syncthreads();
   // triSolve! (Thomas), b = FV3, x = xs: the serial sweeps of the block's
   // columns run concurrently, one per lane of the first warp
@@ -572,6 +670,7 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
     for (int i = n - 2; i >= 0; --i) x[i] = (b[i] - tr[i + 1] * x[i + 1]) / x[i];
   }
   __syncthreads();
+#endif
   if (!valid) return;
   // SchurSolveBKernel! and the stage update of rho, w, rho*theta; each lane
   // owns levels lane and lane + 32
