@@ -330,7 +330,17 @@ def run_adjoint(args, rank, ranks, torch):
     from cgd_b200.adjoint import BoxPressureFunctional, box_columns
     acfg = Ph.CONFIGS["adjoint"]
     study = Ph.ADJOINT_STUDY
-    d, U0, _ = setup(member_config(acfg, rank))
+    # no per-kernel event profile here: every forward step of the
+    # checkpointed sweep is one call and should launch the captured graph
+    prof = os.environ.get("CGD_PROFILE")
+    os.environ["CGD_PROFILE"] = "0"
+    try:
+        d, U0, _ = setup(member_config(acfg, rank))
+    finally:
+        if prof is None:
+            os.environ.pop("CGD_PROFILE", None)
+        else:
+            os.environ["CGD_PROFILE"] = prof
     stream = torch.cuda.ExternalStream(d.stream())
     dt = acfg.dt
     Ub = torch.from_numpy(np.ascontiguousarray(U0.transpose(2, 1, 0))).cuda()   # baroclinic-wave state
