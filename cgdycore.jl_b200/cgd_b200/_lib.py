@@ -27,7 +27,9 @@ EXPORTS = [
     "cgd_create", "cgd_destroy", "cgd_prepare", "cgd_hypervisc_phase1", "cgd_rhs", "cgd_jac",
     "cgd_schur_solve", "cgd_ros_step", "cgd_mass_integral", "cgd_jac_schur_solve_noalloc", "cgd_get_stream",
     "cgd_kernel_times", "cgd_strerror", "cgd_version",
-    "cgd_rhs_adjoint", "cgd_ros_step_adjoint", "cgd_set_caller_stream", "cgd_batch_create", "cgd_batch_step", "cgd_batch_tuning", "cgd_batch_get_stream", "cgd_batch_destroy",
+    "cgd_rhs_adjoint", "cgd_ros_step_adjoint", "cgd_set_caller_stream",
+    "cgd_tape_record_step", "cgd_tape_step_adjoint", "cgd_tape_release", "cgd_tape_bytes_per_step",
+    "cgd_batch_create", "cgd_batch_step", "cgd_batch_tuning", "cgd_batch_get_stream", "cgd_batch_destroy",
 ]
 
 
@@ -70,6 +72,14 @@ def lib(exact=False):
         L.cgd_ros_step_adjoint.restype = ctypes.c_int
         L.cgd_set_caller_stream.argtypes = [vp, vp]
         L.cgd_set_caller_stream.restype = ctypes.c_int
+        L.cgd_tape_record_step.argtypes = [vp, i32, vp, ctypes.c_double]
+        L.cgd_tape_record_step.restype = ctypes.c_int
+        L.cgd_tape_step_adjoint.argtypes = [vp, i32, vp, vp]
+        L.cgd_tape_step_adjoint.restype = ctypes.c_int
+        L.cgd_tape_release.argtypes = [vp]
+        L.cgd_tape_release.restype = ctypes.c_int
+        L.cgd_tape_bytes_per_step.argtypes = [vp]
+        L.cgd_tape_bytes_per_step.restype = ctypes.c_int64
         for f in ("cgd_prepare", "cgd_hypervisc_phase1", "cgd_rhs", "cgd_jac"):
             getattr(L, f).argtypes = [vp, vp, vp]
             getattr(L, f).restype = ctypes.c_int

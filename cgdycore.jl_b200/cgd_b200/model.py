@@ -20,6 +20,7 @@ libcgd_b200.so:
   fcn_adjoint(U, LF)          (no counterpart) (dF/dU)^T LF
   ros_step_adjoint(U0, L, dt) (no counterpart) adjoint of one step
   steps_adjoint(U0, L, dt, n) (no counterpart) checkpointed n-step gradient
+  tape_record_step(...)       (no counterpart) recorded steps for it
   ==========================  ==============================================
 
 State arrays are (nz, NumG, NV) in column-major order: a Fortran-ordered
@@ -149,6 +150,26 @@ class Dycore:
                    "cgd_ros_step_adjoint")
         return Lin
 
+    def tape_record_step(self, slot, U, dt):
+        """One step of U in place, recording what its reverse reads in tape
+        slot `slot` (tape_bytes_per_step() bytes of device memory)."""
+        _lib.check(self._L.cgd_tape_record_step(self.h, int(slot), _ptr(U, self.shape, True), float(dt)),
+                   "cgd_tape_record_step")
+        return U
+
+    def tape_step_adjoint(self, slot, Lout, Lin=None):
+        """(dU1/dU0)^T Lout for the step recorded in `slot`."""
+        Lin = self.new_state() if Lin is None else Lin
+        _lib.check(self._L.cgd_tape_step_adjoint(self.h, int(slot), _ptr(Lout, self.shape),
+                                                 _ptr(Lin, self.shape, True)), "cgd_tape_step_adjoint")
+        return Lin
+
+    def tape_release(self):
+        _lib.check(self._L.cgd_tape_release(self.h), "cgd_tape_release")
+
+    def tape_bytes_per_step(self):
+        return int(self._L.cgd_tape_bytes_per_step(self.h))
+
     def checkpoint_every(self, nsteps, mem_budget=16 << 30):
         """Checkpoint spacing of steps_adjoint: every state when the n states
         fit in mem_budget bytes, else about sqrt(n) (at most n/every + every
@@ -158,17 +179,24 @@ class Dycore:
             return 1
         return max(1, int(round(int(nsteps) ** 0.5)))
 
-    def steps_adjoint(self, U0, Lout, dt, nsteps, every=None, mem_budget=16 << 30):
+    def steps_adjoint(self, U0, Lout, dt, nsteps, every=None, mem_budget=16 << 30, tape=None):
         """(dU_n/dU0)^T Lout for n = nsteps Rosenbrock-W steps from U0, by
-        chaining ros_step_adjoint backwards over checkpoints: the forward run
+        chaining step adjoints backwards over checkpoints: the forward run
         keeps the state every `every` steps (default: checkpoint_every), and
-        the reverse sweep recomputes each segment's states from its
-        checkpoint, so at most nsteps/every + every states are held.  The
-        arrays may be host (numpy) or device (torch) arrays; checkpoints stay
-        where U0 is.  Lout may be a function of the final state U_n that
-        returns the adjoint seed (U_n comes from the same forward run)."""
+        the reverse sweep takes the segments from the last to the first.
+        With tape (default: when a segment's recorded steps fit in
+        mem_budget), each segment is re-run from its checkpoint recording
+        every step (tape_record_step) and the step adjoints read the
+        records; otherwise the segment's states are kept and each step
+        adjoint replays its step (ros_step_adjoint).  At most nsteps/every
+        checkpoints plus one segment are held.  The arrays may be host
+        (numpy) or device (torch) arrays; checkpoints stay where U0 is.
+        Lout may be a function of the final state U_n that returns the
+        adjoint seed (U_n comes from the same forward run)."""
         nsteps = int(nsteps)
         every = self.checkpoint_every(nsteps, mem_budget) if every is None else max(1, int(every))
+        if tape is None:
+            tape = every * self.tape_bytes_per_step() <= mem_budget
         # one working state for every forward step, so the library's captured
         # step (bound to the state's address) is reused
         checkpoints = {0: _copy(U0)}
@@ -185,15 +213,25 @@ class Dycore:
         else:
             L = _copy(Lout)
         top = nsteps
-        for start in sorted(checkpoints, reverse=True):
-            seg = [checkpoints[start]]
-            _assign(work, seg[0])
-            for _ in range(start + 1, top):
-                self.time_stepper(work, dt, 1)
-                seg.append(_copy(work))
-            for W in reversed(seg):
-                L = self.ros_step_adjoint(W, L, dt, _empty_like(L))
-            top = start
+        try:
+            for start in sorted(checkpoints, reverse=True):
+                _assign(work, checkpoints[start])
+                if tape:
+                    for j in range(top - start):
+                        self.tape_record_step(j, work, dt)
+                    for j in reversed(range(top - start)):
+                        L = self.tape_step_adjoint(j, L, _empty_like(L))
+                else:
+                    seg = [checkpoints[start]]
+                    for _ in range(start + 1, top):
+                        self.time_stepper(work, dt, 1)
+                        seg.append(_copy(work))
+                    for W in reversed(seg):
+                        L = self.ros_step_adjoint(W, L, dt, _empty_like(L))
+                top = start
+        finally:
+            if tape:
+                self.tape_release()
         return L
 
     def hypervisc_phase1(self, U, Temp1=None):

@@ -12,6 +12,7 @@
 #include "cgd_adjoint.cuh"
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -35,6 +36,18 @@ struct Buf {
 
 }  // namespace
 
+// What the reverse of one Rosenbrock-W step reads: the stage states, their
+// DSS'd phase-1 caches and pressures, the stage k and the Jacobian bands of
+// the step's initial state u0.
+struct StepTape {
+  double *U0 = nullptr, *V2 = nullptr, *V3 = nullptr, *T1[3] = {}, *P[3] = {};
+  double *k[3] = {}, *jbg = nullptr;
+  const double *u0 = nullptr;   // the initial state (U0, or the caller's array)
+  double dt = 0.0;
+  bool recorded = false;
+  std::vector<void *> mem;      // owned device buffers
+};
+
 struct cgd_handle {
   cgd_config cfg{};
   int N = 0, DoF = 0, nz = 0, NF = 0, NumG = 0, NumTr = 0, NV = 0;
@@ -56,8 +69,9 @@ struct cgd_handle {
   double *pres = nullptr, *pres_st = nullptr;   // pressure of the state and of the stage state
   double *aLF = nullptr, *aLU = nullptr, *aLT1 = nullptr;   // adjoint buffers (allocated on first use)
   // step adjoint workspace: stage states, stage tendencies, k adjoints, ...
-  double *sV2 = nullptr, *sV3 = nullptr, *sT1[3] = {}, *sP[3] = {}, *sk3 = nullptr;
   double *aLk[2] = {}, *aAR = nullptr, *aLV = nullptr, *aLt = nullptr;
+  StepTape work_tape;              // cgd_ros_step_adjoint's own replay
+  std::vector<StepTape> tapes;     // cgd_tape_record_step slots
   double *mmass = nullptr;
   int *flag = nullptr;
   GP gp{};
@@ -103,6 +117,17 @@ int cuda_fail(cgd_handle *h, cudaError_t e, const char *what)
     cudaError_t e_ = (call);                             \
     if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
   } while (0)
+
+// True the first time a call site asks on the current device (the site's
+// own mask); launch attributes such as the dynamic shared-memory limit are
+// per device.
+bool first_on_device(std::atomic<unsigned long long> &done)
+{
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
+  const unsigned long long bit = 1ull << dev;
+  return !(done.fetch_or(bit) & bit);
+}
 
 template <typename T>
 int dalloc(cgd_handle *h, T **p, size_t count)
@@ -153,10 +178,9 @@ template <int N, int NT, typename R>
 void launch_p2r(cgd_handle *h, const double *U, const double *Pr, const double *T1, double *C)
 {
   using CF = P2Cfg<N, NT, R>;
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<unsigned long long> attr{0};
+  if (first_on_device(attr)) {
     cudaFuncSetAttribute(k_phase2<N, NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
-    attr = true;
   }
   dim3 grid((h->nz + CF::LC - 1) / CF::LC, h->NF);
   k_phase2<N, NT, R><<<grid, CF::THREADS, CF::SMEM, h->stream>>>(h->gp, U, Pr, T1, C);
@@ -229,11 +253,10 @@ template <int MODE, bool C32>
 void column_t(cgd_handle *h, const ColArgs &a)
 {
   size_t smem = (size_t)COL_WARPS * COL_ARR * h->nz * sizeof(double);
-  static bool attr = false;
-  if (!attr) {   // up to 8 warps x 15 arrays x 64 levels
+  static std::atomic<unsigned long long> attr{0};
+  if (first_on_device(attr)) {   // up to 8 warps x 15 arrays x 64 levels
     cudaFuncSetAttribute(k_column<MODE, C32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          COL_WARPS * COL_ARR * 64 * (int)sizeof(double));
-    attr = true;
   }
   k_column<MODE, C32><<<(h->NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, h->stream>>>(h->gp, a);
 }
@@ -309,10 +332,9 @@ int rhs_adjoint_launch(cgd_handle *h, const double *Ud, const double *T1, const 
                        double *LU)
 {
   using CF = AdjCfg<N>;
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<unsigned long long> attr{0};
+  if (first_on_device(attr)) {
     cudaFuncSetAttribute(k_phase2_adj<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
-    attr = true;
   }
   dim3 grid((h->nz + CF::LC - 1) / CF::LC, h->NF);
   k_phase2_adj<N><<<grid, CF::THREADS, CF::SMEM, h->stream>>>(h->gp, Ud, pres, T1, LF, LU, h->aLT1);
@@ -552,6 +574,9 @@ void cgd_destroy(cgd_handle *h)
   if (h->stream) cudaStreamSynchronize(h->stream);
   free_graph(h);
   for (auto &b : h->bufs) cudaFree(b.p);
+  for (void *q : h->work_tape.mem) cudaFree(q);
+  for (auto &t : h->tapes)
+    for (void *q : t.mem) cudaFree(q);
   for (int i = 0; i <= NPROF; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
   if (h->order_ev) cudaEventDestroy(h->order_ev);
@@ -809,13 +834,8 @@ int adjoint_alloc(cgd_handle *h, bool step)
     if (!rc) rc = dalloc(h, &h->aLU, SV);
     if (!rc) rc = dalloc(h, &h->aLT1, S * 5);
   }
-  if (!rc && step && !h->sV2) {
-    rc = dalloc(h, &h->sV2, SV);
-    if (!rc) rc = dalloc(h, &h->sV3, SV);
-    for (int i = 0; i < 3 && !rc; ++i) rc = dalloc(h, &h->sT1[i], S * 5);
-    for (int i = 0; i < 3 && !rc; ++i) rc = dalloc(h, &h->sP[i], S);
+  if (!rc && step && !h->aAR) {
     for (int i = 0; i < 2 && !rc; ++i) rc = dalloc(h, &h->aLk[i], SV);
-    if (!rc) rc = dalloc(h, &h->sk3, SV);
     if (!rc) rc = dalloc(h, &h->aAR, SV);
     if (!rc) rc = dalloc(h, &h->aLV, SV);
     if (!rc) rc = dalloc(h, &h->aLt, SV);
@@ -847,81 +867,97 @@ int rhs_adjoint_core(cgd_handle *h, const double *Ud, const double *LFd, double 
   }
 }
 
-int column_adj(cgd_handle *h, const double *mu, double mus, const double *kx, const double *Vn, double fac, double *AR,
-               double *LV)
+int column_adj(cgd_handle *h, const double *mu, double mus, const double *kx, const double *jbg, const double *Vn,
+               double fac, double *AR, double *LV)
 {
   CK(cudaFuncSetAttribute(k_column_adj, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           COL_WARPS * CA_ARR * 64 * (int)sizeof(double)));
   const size_t smem = (size_t)COL_WARPS * CA_ARR * h->nz * sizeof(double);
   k_column_adj<<<(h->NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, h->stream>>>(
-      h->gp, mu, mus, kx, h->jbg, Vn, fac, AR, LV);
+      h->gp, mu, mus, kx, jbg, Vn, fac, AR, LV);
   CK(cudaGetLastError());
   return CGD_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-int cgd_ros_step_adjoint(cgd_handle *h, const double *U0, const double *Lout, double *Lin, double dt)
+// Device buffers of a step tape (own_u0: the tape keeps a copy of the step's
+// initial state; otherwise it points at the caller's array during the call).
+int tape_alloc(cgd_handle *h, StepTape &t, bool own_u0)
 {
-  if (!h || !U0 || !Lout || !Lin || !(dt > 0)) return CGD_ERR_INVALID_ARG;
-  if (h->mix || h->NumTr != 0) return CGD_ERR_UNSUPPORTED;
-  int rc = adjoint_alloc(h, true);
-  if (rc) return rc;
-  rc = enter(h);
-  if (rc) return rc;
+  if (!t.mem.empty()) return CGD_OK;
+  const size_t S = (size_t)h->nz * h->NumG, SV = S * h->NV, SJ = (size_t)8 * (h->nz - 1) * h->NumG;
+  auto get = [&](double **p, size_t n) -> int {
+    void *q = nullptr;
+    CK(cudaMalloc(&q, n * sizeof(double)));
+    t.mem.push_back(q);
+    *p = static_cast<double *>(q);
+    return CGD_OK;
+  };
+  int rc = own_u0 ? get(&t.U0, SV) : CGD_OK;
+  if (!rc) rc = get(&t.V2, SV);
+  if (!rc) rc = get(&t.V3, SV);
+  for (int i = 0; i < 3 && !rc; ++i) rc = get(&t.T1[i], S * 5);
+  for (int i = 0; i < 3 && !rc; ++i) rc = get(&t.P[i], S);
+  for (int i = 0; i < 3 && !rc; ++i) rc = get(&t.k[i], SV);
+  if (!rc) rc = get(&t.jbg, SJ);
+  return rc;
+}
+
+// One forward step from the device state u0 (kept in the tape when it owns a
+// copy), recording what its reverse reads; U1 goes to Uout (may be u0's
+// array when the tape owns its copy).  Not captured: the tape's buffers
+// differ from the graph's.
+int record_step(cgd_handle *h, StepTape &t, const double *u0, double dt, double *Uout)
+{
   const size_t SV = (size_t)h->nz * h->NumG * h->NV;
-  double *Ud;
-  rc = stage_in(h, U0, h->Ubuf, true, &Ud);
-  if (rc) return rc;
-  const double *L = Lout;
-  if (!is_device_ptr(Lout)) {
-    CK(cudaMemcpyAsync(h->aLF, Lout, SV * 8, cudaMemcpyHostToDevice, h->stream));
-    L = h->aLF;
+  if (t.U0) {
+    if (t.U0 != u0) CK(cudaMemcpyAsync(t.U0, u0, SV * 8, cudaMemcpyDeviceToDevice, h->stream));
+    t.u0 = t.U0;
+  } else {
+    t.u0 = u0;
   }
-  const RK &rk = h->rk;
-  const double fac = dt * rk.gamma;
-  // forward replay of the step, keeping each stage's state, phase-1 cache,
-  // pressure and k
+  t.dt = dt;
   ColArgs a{};
-  a.Vn = Ud;
-  a.k1 = h->k1;
-  a.k2 = h->k2;
+  a.Vn = t.u0;
+  a.k1 = t.k[0];
+  a.k2 = t.k[1];
   a.dt = dt;
-  a.fac = fac;
-  a.rk = rk;
+  a.fac = dt * h->rk.gamma;
+  a.rk = h->rk;
   a.C = h->C;
-  a.jbg = h->jbg;
-  const double *Vs[3] = {Ud, h->sV2, h->sV3};
-  const double *ks[3] = {h->k1, h->k2, h->sk3};
+  a.jbg = t.jbg;
+  const double *Vs[3] = {t.u0, t.V2, t.V3};
   for (int st = 0; st < 3; ++st) {
-    const double *V = Vs[st];
-    hv1(h, V, h->C);
-    gather(h, h->C, h->sT1[st], false);
-    pressure(h, V, h->sP[st]);
-    phase2(h, V, h->sP[st], h->sT1[st], h->C);
-    if (st == 0) {
-      a.kout = h->k1; a.Vout = h->sV2;
-      column<0>(h, a);
-    } else if (st == 1) {
-      a.kout = h->k2; a.Vout = h->sV3;
-      column<1>(h, a);
-    } else {
-      a.kout = h->sk3; a.Vout = h->Vst;   // U1 itself is not needed
-      column<2>(h, a);
-    }
+    hv1(h, Vs[st], h->C);
+    gather(h, h->C, t.T1[st], false);
+    pressure(h, Vs[st], t.P[st]);
+    phase2(h, Vs[st], t.P[st], t.T1[st], h->C);
+    a.kout = t.k[st];
+    if (st == 0) { a.Vout = t.V2; column<0>(h, a); }
+    else if (st == 1) { a.Vout = t.V3; column<1>(h, a); }
+    else { a.Vout = Uout ? Uout : h->Vst; column<2>(h, a); }
   }
-  // reverse: U1 = U0 + sum m_i k_i; k_i = L (F(V_i) + sum_j c_ij/dt k_j); V_i = U0 + sum_j a_ij k_j
+  CK(cudaGetLastError());
+  t.recorded = true;
+  return CGD_OK;
+}
+
+// Lin (device, h->aLV) = (dU1/dU0)^T L for the recorded step:
+// U1 = U0 + sum m_i k_i; k_i = L (F(V_i) + sum_j c_ij/dt k_j); V_i = U0 + sum_j a_ij k_j
+int reverse_step(cgd_handle *h, const StepTape &t, const double *L)
+{
+  const size_t SV = (size_t)h->nz * h->NumG * h->NV;
+  const RK &rk = h->rk;
+  const double dt = t.dt, fac = dt * rk.gamma;
+  const double *Vs[3] = {t.u0, t.V2, t.V3};
   CK(cudaMemsetAsync(h->aLV, 0, SV * 8, h->stream));
   const long long n = (long long)SV;
   const unsigned nb = (unsigned)((n + 255) / 256);
   for (int st = 2; st >= 0; --st) {
     const double cA = st >= 1 ? rk.c[st][0] / dt : 0.0, cB = st == 2 ? rk.c[st][1] / dt : 0.0;
     const double *mu = st == 2 ? L : h->aLk[st];
-    rc = column_adj(h, mu, st == 2 ? rk.m[2] : 1.0, ks[st], Ud, fac, h->aAR, h->aLV);
+    int rc = column_adj(h, mu, st == 2 ? rk.m[2] : 1.0, t.k[st], t.jbg, t.u0, fac, h->aAR, h->aLV);
     if (rc) return rc;
-    rc = rhs_adjoint_core(h, Vs[st], h->aAR, h->aLt, h->sT1[st], h->sP[st]);
+    rc = rhs_adjoint_core(h, Vs[st], h->aAR, h->aLt, t.T1[st], t.P[st]);
     if (rc) return rc;
     // r_st = F(V_st) + c_st0/dt k1 + c_st1/dt k2; V_st = U0 + a_st0 k1 + a_st1 k2
     if (st == 2)
@@ -935,9 +971,95 @@ int cgd_ros_step_adjoint(cgd_handle *h, const double *U0, const double *Lout, do
                                                0.0, 0.0, 0.0);
     CK(cudaGetLastError());
   }
+  return CGD_OK;
+}
+
+int adjoint_out(cgd_handle *h, double *Lin)
+{
+  const size_t SV = (size_t)h->nz * h->NumG * h->NV;
   if (is_device_ptr(Lin)) CK(cudaMemcpyAsync(Lin, h->aLV, SV * 8, cudaMemcpyDeviceToDevice, h->stream));
   else CK(cudaMemcpyAsync(Lin, h->aLV, SV * 8, cudaMemcpyDeviceToHost, h->stream));
   return finish(h);
+}
+
+const double *adjoint_in(cgd_handle *h, const double *Lout)
+{
+  if (is_device_ptr(Lout)) return Lout;
+  const size_t SV = (size_t)h->nz * h->NumG * h->NV;
+  if (cudaMemcpyAsync(h->aLF, Lout, SV * 8, cudaMemcpyHostToDevice, h->stream) != cudaSuccess) return nullptr;
+  return h->aLF;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cgd_ros_step_adjoint(cgd_handle *h, const double *U0, const double *Lout, double *Lin, double dt)
+{
+  if (!h || !U0 || !Lout || !Lin || !(dt > 0)) return CGD_ERR_INVALID_ARG;
+  if (h->mix || h->NumTr != 0) return CGD_ERR_UNSUPPORTED;
+  int rc = adjoint_alloc(h, true);
+  if (!rc) rc = tape_alloc(h, h->work_tape, false);
+  if (!rc) rc = enter(h);
+  if (rc) return rc;
+  double *Ud;
+  rc = stage_in(h, U0, h->Ubuf, true, &Ud);
+  if (rc) return rc;
+  const double *L = adjoint_in(h, Lout);
+  if (!L) return cuda_fail(h, cudaGetLastError(), "cgd_ros_step_adjoint");
+  rc = record_step(h, h->work_tape, Ud, dt, nullptr);   // U1 itself is not needed
+  if (!rc) rc = reverse_step(h, h->work_tape, L);
+  if (rc) return rc;
+  return adjoint_out(h, Lin);
+}
+
+int cgd_tape_record_step(cgd_handle *h, int32_t slot, double *U, double dt)
+{
+  if (!h || !U || !(dt > 0) || slot < 0 || slot >= CGD_TAPE_MAX_SLOTS) return CGD_ERR_INVALID_ARG;
+  if (h->mix || h->NumTr != 0) return CGD_ERR_UNSUPPORTED;
+  if ((size_t)slot >= h->tapes.size()) h->tapes.resize(slot + 1);
+  int rc = adjoint_alloc(h, true);
+  if (!rc) rc = tape_alloc(h, h->tapes[slot], true);
+  if (!rc) rc = enter(h);
+  if (rc) return rc;
+  double *Ud;
+  rc = stage_in(h, U, h->Ubuf, true, &Ud);
+  if (rc) return rc;
+  rc = record_step(h, h->tapes[slot], Ud, dt, Ud);
+  if (rc) return rc;
+  if (Ud != U)
+    CK(cudaMemcpyAsync(U, Ud, (size_t)h->nz * h->NumG * h->NV * 8, cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
+}
+
+int cgd_tape_step_adjoint(cgd_handle *h, int32_t slot, const double *Lout, double *Lin)
+{
+  if (!h || !Lout || !Lin || slot < 0 || (size_t)slot >= h->tapes.size()) return CGD_ERR_INVALID_ARG;
+  if (!h->tapes[slot].recorded) return CGD_ERR_INVALID_ARG;
+  int rc = enter(h);
+  if (rc) return rc;
+  const double *L = adjoint_in(h, Lout);
+  if (!L) return cuda_fail(h, cudaGetLastError(), "cgd_tape_step_adjoint");
+  rc = reverse_step(h, h->tapes[slot], L);
+  if (rc) return rc;
+  return adjoint_out(h, Lin);
+}
+
+int cgd_tape_release(cgd_handle *h)
+{
+  if (!h) return CGD_ERR_INVALID_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  for (auto &t : h->tapes)
+    for (void *q : t.mem) cudaFree(q);
+  h->tapes.clear();
+  return CGD_OK;
+}
+
+int64_t cgd_tape_bytes_per_step(const cgd_handle *h)
+{
+  if (!h) return CGD_ERR_INVALID_ARG;
+  const int64_t S = (int64_t)h->nz * h->NumG, SV = S * h->NV, SJ = (int64_t)8 * (h->nz - 1) * h->NumG;
+  return 8 * (6 * SV + 15 * S + 3 * S + SJ);
 }
 
 }  // extern "C"
@@ -1113,14 +1235,13 @@ template <int N, int NT, typename R>
 void batch_enqueue_t(cgd_batch *b, WItem *const *w)
 {
   using CF = P2Cfg<N, NT, R>;
-  static bool attr = false;
+  static std::atomic<unsigned long long> attr{0};
   const size_t csmem = (size_t)COL_WARPS * COL_ARR * b->nzmax * sizeof(double);
-  if (!attr) {
+  if (first_on_device(attr)) {
     cudaFuncSetAttribute(kb_phase2<N, NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
     constexpr bool C32 = sizeof(R) == sizeof(float);
     for (auto f : {kb_column<0, C32>, kb_column<1, C32>, kb_column<2, C32>})
       cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, COL_WARPS * COL_ARR * 64 * (int)sizeof(double));
-    attr = true;
   }
   kb_pressure<<<b->n[1], 256, 0, b->stream>>>(w[1], 0);
   for (int stage = 0; stage < 3; ++stage) {

@@ -132,6 +132,23 @@ int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps);
  * states.  No counterpart in the reference (it has no adjoint). */
 int cgd_ros_step_adjoint(cgd_handle *h, const double *U0, const double *Lout, double *Lin, double dt);
 
+/* Recorded steps for multi-step gradients.  cgd_tape_record_step advances U
+ * by one step in place (as cgd_ros_step, but not as a captured graph) and
+ * keeps in tape slot `slot` what the step's reverse reads: a copy of the
+ * initial state, the stage states, their phase-1 caches and pressures, the
+ * stage k and the Jacobian bands (cgd_tape_bytes_per_step bytes of device
+ * memory per slot, allocated on first use of the slot).
+ * cgd_tape_step_adjoint then gives Lin = (dU1/dU0)^T Lout for the step in
+ * that slot without replaying it.  A checkpointed gradient records each
+ * segment's steps into slots 0..k-1 and runs their adjoints backwards.
+ * cgd_tape_release frees every slot.  FP64 handles without tracers
+ * (CGD_ERR_UNSUPPORTED otherwise).  No counterpart in the reference. */
+#define CGD_TAPE_MAX_SLOTS 4096
+int cgd_tape_record_step(cgd_handle *h, int32_t slot, double *U, double dt);
+int cgd_tape_step_adjoint(cgd_handle *h, int32_t slot, const double *Lout, double *Lin);
+int cgd_tape_release(cgd_handle *h);
+int64_t cgd_tape_bytes_per_step(const cgd_handle *h);
+
 /* sum(rho * MMass) over all DOFs, reduced in FP64 on the device (MMass is
  * the caller's lumped quadrature mass (nz, NumG)).
  * Replaces Parallels.GlobalIntegral (src/Parallels/Exchange.jl:1163-1166). */

@@ -181,10 +181,13 @@ def test_checkpointed_gradient_of_a_functional(oracle_mod, built_lib, cuda_ok):
 
     Un = _step(d, U, dt, n)
     grad = d.steps_adjoint(U, np.asfortranarray(w * Un), dt, n, every=2)
-    # the same gradient without recomputation (every step kept); the adjoint
-    # sums are atomic, so the two agree to rounding
+    # the same gradient without recomputation (every step kept) and with
+    # replayed instead of recorded steps; the adjoint sums are atomic, so
+    # they agree to rounding
     g1 = d.steps_adjoint(U, np.asfortranarray(w * Un), dt, n, every=1)
     assert np.abs(grad - g1).max() <= 1e-10 * np.abs(g1).max()
+    g2 = d.steps_adjoint(U, np.asfortranarray(w * Un), dt, n, every=2, tape=False)
+    assert np.abs(grad - g2).max() <= 1e-10 * np.abs(g2).max()
     rng = np.random.default_rng(5)
     nodes = []
     for f in range(NV):
@@ -227,6 +230,25 @@ def test_box_pressure_functional_gradient(oracle_mod, built_lib, cuda_ok):
     # its direct term uses 1e-5
     _assert_entries(*_entry_check(U, scale, Jf.diff, G, nodes, rels=(1e-3, 1e-4, 1e-5, 1e-6), tol=1e-5),
                     nodes)
+    d.close()
+
+
+def test_recorded_step_matches_replayed_step(oracle_mod, built_lib, cuda_ok):
+    """cgd_tape_record_step advances the state exactly as cgd_ros_step does,
+    and the adjoint read from its record equals cgd_ros_step_adjoint's."""
+    d, U, scale = _evolved(oracle_mod, (3, 3, 6, "quadratic"))
+    rng = np.random.default_rng(3)
+    lam = np.asfortranarray(rng.standard_normal(U.shape))
+    V = U.copy(order="F")
+    d.tape_record_step(0, V, 300.0)
+    assert np.array_equal(V, _step(d, U, 300.0, 1))
+    a = d.tape_step_adjoint(0, lam)
+    b = d.ros_step_adjoint(U, lam, 300.0)
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+    d.tape_release()
+    from cgd_b200 import CgdError
+    with pytest.raises(CgdError):
+        d.tape_step_adjoint(0, lam)
     d.close()
 
 
