@@ -21,6 +21,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 NOALLOC_SCRATCH_DOUBLES = 4 * 1024 * 1024
 FLAG_CHECK_FINITE = 1
 BATCH_AUTOTUNE = 1
+BATCH_FUSED = 2
 
 # every symbol declared in include/cgd_b200.h
 EXPORTS = [

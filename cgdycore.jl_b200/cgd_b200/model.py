@@ -295,17 +295,20 @@ class Dycore:
 
 class Ensemble:
     """Batched ensemble of Dycore members (same OrdPoly, NumTr and precision;
-    any nPanel and nz): one ensemble step is one CUDA graph of 15 launches over
-    flat work lists spanning every member (cgd_batch_step).  States are CUDA
-    torch tensors, one per member, stepped in place."""
+    any nPanel and nz): one ensemble step is one CUDA graph over flat work
+    lists spanning every member (cgd_batch_step), either 15 launches or, with
+    fused=True (OrdPoly 4), one persistent cooperative launch per stage.
+    autotune=True times every work-list order in both forms and keeps the
+    fastest.  States are CUDA torch tensors, one per member, stepped in
+    place."""
 
-    def __init__(self, members, autotune=False):
+    def __init__(self, members, autotune=False, fused=False):
         self.members = list(members)
         self._L = self.members[0]._L
         arr = (ctypes.c_void_p * len(self.members))(*[m.h for m in self.members])
         b = ctypes.c_void_p()
-        _lib.check(self._L.cgd_batch_create(arr, len(self.members), _lib.BATCH_AUTOTUNE if autotune else 0,
-                                            ctypes.byref(b)), "cgd_batch_create")
+        flags = (_lib.BATCH_AUTOTUNE if autotune else 0) | (_lib.BATCH_FUSED if fused else 0)
+        _lib.check(self._L.cgd_batch_create(arr, len(self.members), flags, ctypes.byref(b)), "cgd_batch_create")
         self.b = b
 
     def step(self, states, dts, nsteps=1):

@@ -1151,15 +1151,25 @@ struct cgd_batch {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t order_ev = nullptr;   // orders a step after the first member's caller stream
-  // work lists, one set per candidate order; order[ci] names it
+  // work lists, one set per candidate order; a candidate is (order, form):
+  // candidate c runs order c % NORD, split into 15 launches (c < NORD) or as
+  // three fused stage launches (c >= NORD)
   static constexpr int NORD = 3;
-  WItem *w[NORD][4] = {};
-  int n[4] = {};
-  cudaGraph_t graph[NORD] = {};
-  cudaGraphExec_t gexec[NORD] = {};
+  static constexpr int NCAND = 2 * NORD;
+  WItem *w[NORD][5] = {};
+  int n[5] = {};
+  cudaGraph_t graph[NCAND] = {};
+  cudaGraphExec_t gexec[NCAND] = {};
+  bool use[NCAND] = {};
   int chosen = 0;
   bool tuned = false, autotune = false;
-  double tune_ms[NORD] = {};
+  double tune_ms[NCAND] = {};
+  // fused form: grid (CTAs resident on the device), dynamic shared memory,
+  // barrier state, second contribution and stage buffers per member
+  int fgrid = 0;
+  size_t fsmem = 0;
+  GridBar *bar = nullptr;
+  std::vector<double *> C2, Vst2;
   std::vector<GP> gps;
   std::vector<BMember> bms;
   std::vector<void *> scratch;
@@ -1169,6 +1179,7 @@ struct cgd_batch {
 namespace {
 
 const char *const ORDER_NAME[cgd_batch::NORD] = {"member-major", "largest-member-first", "members-interleaved"};
+const char *const FORM_NAME[2] = {"split", "fused"};
 
 int batch_fail(cgd_batch *b, cudaError_t e, const char *what)
 {
@@ -1187,19 +1198,19 @@ int batch_fail(cgd_batch *b, cudaError_t e, const char *what)
 // Work items of every kernel of a stage for every member, in one of three
 // orders: members one after the other, the largest member first, or the
 // members' items interleaved one by one.
-void batch_lists(const cgd_batch *b, int order, std::vector<WItem> out[4])
+void batch_lists(const cgd_batch *b, int order, std::vector<WItem> out[5])
 {
   const int nm = (int)b->mem.size();
-  std::vector<std::vector<WItem>> per[4];
-  for (int k = 0; k < 4; ++k) per[k].resize(nm);
+  std::vector<std::vector<WItem>> per[5];
+  for (int k = 0; k < 5; ++k) per[k].resize(nm);
   const int DoF = b->N * b->N;
   const int LT = 256 / DoF;
-  int LC = 0;
+  int LC = 0, LCF = 0;   // phase-2 levels per CTA: split form, fused form
   switch (b->N) {
-    case 2: LC = P2Cfg<2, 0, double>::LC; break;
-    case 3: LC = P2Cfg<3, 0, double>::LC; break;
-    case 4: LC = P2Cfg<4, 0, double>::LC; break;
-    default: LC = P2Cfg<5, 0, double>::LC; break;
+    case 2: LC = P2Cfg<2, 0, double>::LC; LCF = P2Cfg<2, 0, double, FUSED_P2_WARPS>::LC; break;
+    case 3: LC = P2Cfg<3, 0, double>::LC; LCF = P2Cfg<3, 0, double, FUSED_P2_WARPS>::LC; break;
+    case 4: LC = P2Cfg<4, 0, double>::LC; LCF = P2Cfg<4, 0, double, FUSED_P2_WARPS>::LC; break;
+    default: LC = P2Cfg<5, 0, double>::LC; LCF = P2Cfg<5, 0, double, FUSED_P2_WARPS>::LC; break;
   }
   for (int m = 0; m < nm; ++m) {
     const cgd_handle *h = b->mem[m];
@@ -1210,6 +1221,8 @@ void batch_lists(const cgd_batch *b, int order, std::vector<WItem> out[4])
     for (int IF = 0; IF < h->NF; ++IF)
       for (int c = 0; c < (h->nz + LC - 1) / LC; ++c) per[2][m].push_back({m, c, IF});
     for (int c = 0; c < (h->NumG + COL_WARPS - 1) / COL_WARPS; ++c) per[3][m].push_back({m, c, 0});
+    for (int IF = 0; IF < h->NF; ++IF)
+      for (int c = 0; c < (h->nz + LCF - 1) / LCF; ++c) per[4][m].push_back({m, c, IF});
   }
   std::vector<int> ord(nm);
   for (int m = 0; m < nm; ++m) ord[m] = m;
@@ -1217,7 +1230,7 @@ void batch_lists(const cgd_batch *b, int order, std::vector<WItem> out[4])
     std::stable_sort(ord.begin(), ord.end(), [&](int a, int c) {
       return (long long)b->mem[a]->NF * b->mem[a]->nz > (long long)b->mem[c]->NF * b->mem[c]->nz;
     });
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < 5; ++k) {
     out[k].clear();
     if (order == 2) {
       size_t mx = 0;
@@ -1279,10 +1292,95 @@ void batch_enqueue_r(cgd_batch *b, WItem *const *w)
   }
 }
 
-void batch_enqueue(cgd_batch *b, int order)
+// The fused form (p = 4): three cooperative launches of kb_stage per step.
+// The barrier counter is cleared before each (a launch that timed out may
+// have left it non-zero).
+template <int NT, typename R>
+cudaError_t batch_enqueue_fused_t(cgd_batch *b, WItem *const *w)
 {
-  if (b->mix) batch_enqueue_r<float>(b, b->w[order]);
-  else batch_enqueue_r<double>(b, b->w[order]);
+  FusedArgs fa{};
+  for (int k = 0; k < 5; ++k) {
+    fa.w[k] = w[k];
+    fa.n[k] = b->n[k];
+  }
+  fa.bar = b->bar;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  for (int stage = 0; stage < 3; ++stage) {
+    cudaError_t e = cudaMemsetAsync(&b->bar->count, 0, sizeof(unsigned int), b->stream);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)b->fgrid);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = b->fsmem;
+    cfg.stream = b->stream;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, kb_stage<5, NT, R>, fa, stage);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+template <typename R>
+cudaError_t batch_enqueue_fused_r(cgd_batch *b, WItem *const *w)
+{
+  switch (b->NT) {
+    case 0: return batch_enqueue_fused_t<0, R>(b, w);
+    case 1: return batch_enqueue_fused_t<1, R>(b, w);
+    case 2: return batch_enqueue_fused_t<2, R>(b, w);
+    case 3: return batch_enqueue_fused_t<3, R>(b, w);
+    default: return batch_enqueue_fused_t<4, R>(b, w);
+  }
+}
+
+// Launch limits of the fused kernel on this device: dynamic shared memory
+// (the larger of phase 2's and the column's) and the CTAs that fit at once.
+template <int NT, typename R>
+cudaError_t fused_setup_t(cgd_batch *b)
+{
+  using CF = P2Cfg<5, NT, R, FUSED_P2_WARPS>;
+  const size_t csm = (size_t)COL_WARPS * COL_ARR * b->nzmax * sizeof(double);
+  b->fsmem = std::max(std::max(CF::SMEM, csm), HV1Smem<5, NT, R>::BYTES);
+  cudaError_t e = cudaFuncSetAttribute(kb_stage<5, NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->fsmem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0, sms = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb_stage<5, NT, R>, 256, b->fsmem);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  b->fgrid = per_sm * sms;
+  return e;
+}
+
+template <typename R>
+cudaError_t fused_setup_r(cgd_batch *b)
+{
+  switch (b->NT) {
+    case 0: return fused_setup_t<0, R>(b);
+    case 1: return fused_setup_t<1, R>(b);
+    case 2: return fused_setup_t<2, R>(b);
+    case 3: return fused_setup_t<3, R>(b);
+    default: return fused_setup_t<4, R>(b);
+  }
+}
+
+cudaError_t batch_enqueue(cgd_batch *b, int cand)
+{
+  WItem *const *w = b->w[cand % cgd_batch::NORD];
+  if (cand >= cgd_batch::NORD) return b->mix ? batch_enqueue_fused_r<float>(b, w) : batch_enqueue_fused_r<double>(b, w);
+  if (b->mix) batch_enqueue_r<float>(b, w);
+  else batch_enqueue_r<double>(b, w);
+  return cudaSuccess;
+}
+
+// 1 if a fused launch timed out at a grid barrier (the flag is cleared)
+int fused_timed_out(cgd_batch *b)
+{
+  if (!b->bar) return 0;
+  int t = 0;
+  if (cudaMemcpy(&t, &b->bar->timeout, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+  if (t) cudaMemset(&b->bar->timeout, 0, sizeof(int));
+  return t != 0;
 }
 
 int batch_upload(cgd_batch *b)
@@ -1317,6 +1415,11 @@ int cgd_batch_create(cgd_handle *const *members, int32_t nmembers, int32_t flags
   b->mix = members[0]->mix;
   b->device = members[0]->device;
   b->autotune = (flags & CGD_BATCH_AUTOTUNE) != 0;
+  const bool want_fused = (flags & CGD_BATCH_FUSED) != 0;
+  if (want_fused && b->N != 5) {
+    delete b;
+    return CGD_ERR_UNSUPPORTED;
+  }
   for (auto h : b->mem) b->nzmax = std::max(b->nzmax, h->nz);
   int rc = CGD_OK;
   do {
@@ -1324,11 +1427,45 @@ int cgd_batch_create(cgd_handle *const *members, int32_t nmembers, int32_t flags
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->order_ev, cudaEventDisableTiming);
     if (e != cudaSuccess) { rc = batch_fail(b, e, "cgd_batch_create stream"); break; }
+    // candidates: the autotuner times every order, split and (p = 4, when
+    // the device launches cooperative kernels) fused; otherwise the first
+    // order, split or fused as asked
+    bool fused_ok = false;
+    if (b->N == 5 && (b->autotune || want_fused)) {
+      int coop = 0;
+      e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, b->device);
+      if (e == cudaSuccess && coop) e = b->mix ? fused_setup_r<float>(b) : fused_setup_r<double>(b);
+      if (e != cudaSuccess) { rc = batch_fail(b, e, "cgd_batch_create fused setup"); break; }
+      fused_ok = coop && b->fgrid > 0;
+    }
+    if (want_fused && !fused_ok) { rc = CGD_ERR_UNSUPPORTED; break; }
+    for (int c = 0; c < cgd_batch::NCAND; ++c) {
+      const bool fused = c >= cgd_batch::NORD;
+      b->use[c] = b->autotune ? (!fused || fused_ok) : c == (want_fused ? cgd_batch::NORD : 0);
+    }
+    if (!b->autotune) b->chosen = want_fused ? cgd_batch::NORD : 0;
+    if (fused_ok) {
+      void *p = nullptr;
+      e = cudaMalloc(&p, sizeof(GridBar));
+      if (e == cudaSuccess) e = cudaMemset(p, 0, sizeof(GridBar));
+      b->bar = static_cast<GridBar *>(p);
+      for (int m = 0; m < nmembers && e == cudaSuccess; ++m) {
+        const cgd_handle *h = members[m];
+        const size_t S = (size_t)h->nz * h->NumG;
+        const size_t ENL = (size_t)h->N * h->N * h->nz * h->NF;
+        void *c2 = nullptr, *v2 = nullptr;
+        e = cudaMalloc(&c2, ENL * (h->NV + 1) * sizeof(double));
+        b->C2.push_back(static_cast<double *>(c2));
+        if (e == cudaSuccess) e = cudaMalloc(&v2, S * h->NV * sizeof(double));
+        b->Vst2.push_back(static_cast<double *>(v2));
+      }
+      if (e != cudaSuccess) { rc = batch_fail(b, e, "cgd_batch_create fused buffers"); break; }
+    }
     const int nord = b->autotune ? cgd_batch::NORD : 1;
     for (int o = 0; o < nord && !rc; ++o) {
-      std::vector<WItem> lists[4];
+      std::vector<WItem> lists[5];
       batch_lists(b, o, lists);
-      for (int k = 0; k < 4; ++k) {
+      for (int k = 0; k < 5; ++k) {
         b->n[k] = (int)lists[k].size();
         void *p = nullptr;
         e = cudaMalloc(&p, lists[k].size() * sizeof(WItem));
@@ -1351,13 +1488,17 @@ void cgd_batch_destroy(cgd_batch *b)
 {
   if (!b) return;
   if (b->stream) cudaStreamSynchronize(b->stream);
-  for (int o = 0; o < cgd_batch::NORD; ++o) {
-    if (b->gexec[o]) cudaGraphExecDestroy(b->gexec[o]);
-    if (b->graph[o]) cudaGraphDestroy(b->graph[o]);
-    for (int k = 0; k < 4; ++k)
-      if (b->w[o][k]) cudaFree(b->w[o][k]);
+  for (int c = 0; c < cgd_batch::NCAND; ++c) {
+    if (b->gexec[c]) cudaGraphExecDestroy(b->gexec[c]);
+    if (b->graph[c]) cudaGraphDestroy(b->graph[c]);
   }
+  for (int o = 0; o < cgd_batch::NORD; ++o)
+    for (int k = 0; k < 5; ++k)
+      if (b->w[o][k]) cudaFree(b->w[o][k]);
   for (void *p : b->scratch) cudaFree(p);
+  for (double *p : b->C2) if (p) cudaFree(p);
+  for (double *p : b->Vst2) if (p) cudaFree(p);
+  if (b->bar) cudaFree(b->bar);
   if (b->order_ev) cudaEventDestroy(b->order_ev);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
@@ -1386,17 +1527,18 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
   auto set_members = [&](double *const *state) {
     for (int m = 0; m < nm; ++m) {
       const cgd_handle *h = b->mem[m];
-      b->bms[m] = BMember{state[m], h->Vst, h->k1, h->k2, h->C, h->T1, h->jbg, h->pres, h->pres_st, dt[m]};
+      b->bms[m] = BMember{state[m], h->Vst, h->k1, h->k2, h->C, h->T1, h->jbg, h->pres, h->pres_st, dt[m],
+                          b->C2.empty() ? nullptr : b->C2[m], b->Vst2.empty() ? nullptr : b->Vst2[m]};
     }
   };
-  const int nord = b->autotune ? cgd_batch::NORD : 1;
-  for (int o = 0; o < nord; ++o) {
-    if (b->gexec[o]) continue;
+  for (int c = 0; c < cgd_batch::NCAND; ++c) {
+    if (!b->use[c] || b->gexec[c]) continue;
     BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    batch_enqueue(b, o);
-    cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph[o]);
+    const cudaError_t le = batch_enqueue(b, c);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph[c]);
+    if (le != cudaSuccess) return batch_fail(b, le, "cgd_batch_step fused launch");
     if (e != cudaSuccess) return batch_fail(b, e, "cgd_batch_step capture");
-    BCK(cudaGraphInstantiate(&b->gexec[o], b->graph[o], 0));
+    BCK(cudaGraphInstantiate(&b->gexec[c], b->graph[c], 0));
   }
   if (b->autotune && !b->tuned) {
     // each candidate order advances copies of the states by one step after one
@@ -1413,7 +1555,8 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
     cudaEvent_t e0, e1;
     BCK(cudaEventCreate(&e0));
     BCK(cudaEventCreate(&e1));
-    for (int o = 0; o < nord; ++o) {
+    for (int c = 0; c < cgd_batch::NCAND; ++c) {
+      if (!b->use[c]) continue;
       for (int m = 0; m < nm; ++m) {
         const cgd_handle *h = b->mem[m];
         BCK(cudaMemcpyAsync(copies[m], U[m], (size_t)h->nz * h->NumG * h->NV * sizeof(double),
@@ -1422,20 +1565,24 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
       set_members(copies.data());
       int rc = batch_upload(b);
       if (rc) return rc;
-      BCK(cudaGraphLaunch(b->gexec[o], b->stream));
+      BCK(cudaGraphLaunch(b->gexec[c], b->stream));
       BCK(cudaEventRecord(e0, b->stream));
-      BCK(cudaGraphLaunch(b->gexec[o], b->stream));
+      BCK(cudaGraphLaunch(b->gexec[c], b->stream));
       BCK(cudaEventRecord(e1, b->stream));
       BCK(cudaEventSynchronize(e1));
       float ms = 0.f;
       BCK(cudaEventElapsedTime(&ms, e0, e1));
-      b->tune_ms[o] = ms;
+      b->tune_ms[c] = ms;
+      if (c >= cgd_batch::NORD && fused_timed_out(b)) {
+        g_last_error = "cgd_batch_step: a fused stage launch timed out at a grid barrier";
+        return CGD_ERR_TIMEOUT;
+      }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b->chosen = 0;
-    for (int o = 1; o < nord; ++o)
-      if (b->tune_ms[o] < b->tune_ms[b->chosen]) b->chosen = o;
+    for (int c = 1; c < cgd_batch::NCAND; ++c)
+      if (b->use[c] && b->tune_ms[c] < b->tune_ms[b->chosen]) b->chosen = c;
     b->tuned = true;
   }
   set_members(U);
@@ -1444,17 +1591,24 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
   for (int s = 0; s < nsteps; ++s) BCK(cudaGraphLaunch(b->gexec[b->chosen], b->stream));
   BCK(cudaStreamSynchronize(b->stream));
   BCK(cudaGetLastError());
+  if (b->chosen >= cgd_batch::NORD && fused_timed_out(b)) {
+    g_last_error = "cgd_batch_step: a fused stage launch timed out at a grid barrier";
+    return CGD_ERR_TIMEOUT;
+  }
   return CGD_OK;
 }
 
 int cgd_batch_tuning(cgd_batch *b, char *desc, int32_t len)
 {
   if (!b || !desc || len < 1) return CGD_ERR_INVALID_ARG;
-  std::string s = std::string("order=") + ORDER_NAME[b->chosen];
+  std::string s = std::string("order=") + ORDER_NAME[b->chosen % cgd_batch::NORD] + ";stage=" +
+                  FORM_NAME[b->chosen >= cgd_batch::NORD];
   if (b->tuned) {
-    char buf[64];
-    for (int o = 0; o < cgd_batch::NORD; ++o) {
-      snprintf(buf, sizeof buf, ";%s=%.3fms", ORDER_NAME[o], b->tune_ms[o]);
+    char buf[96];
+    for (int c = 0; c < cgd_batch::NCAND; ++c) {
+      if (!b->use[c]) continue;
+      snprintf(buf, sizeof buf, ";%s/%s=%.3fms", ORDER_NAME[c % cgd_batch::NORD], FORM_NAME[c >= cgd_batch::NORD],
+               b->tune_ms[c]);
       s += buf;
     }
   }

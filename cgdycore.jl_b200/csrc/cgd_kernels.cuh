@@ -118,16 +118,32 @@ __device__ __forceinline__ void recu4(double cLL, double cL, double cR, double c
 // mixed form, where theta enters as its perturbation from the level's FP64
 // reference value.
 // ---------------------------------------------------------------------------
+// shared arrays of phase 1: planes 0-3 curl/contra of (u,v), 4 theta, 5-8
+// the first derivatives, then per tracer its ratio and the two components of
+// its gradient, each LT levels x DoF nodes
+template <int N, int NT, typename R>
+struct HV1Smem {
+  static constexpr int DoF = N * N, LT = 256 / DoF;
+  static constexpr int PLANES = 9 + 3 * NT;
+  static constexpr size_t BYTES = (size_t)PLANES * LT * DoF * sizeof(R);
+};
+template <int N, int NT, typename R>
+__device__ __forceinline__ R *hv1_static_smem()
+{
+  using S = HV1Smem<N, NT, R>;
+  __shared__ R s[S::PLANES * S::LT * S::DoF];
+  return s;
+}
+
+// sbuf: the shared arrays (hv1_static_smem, or a kernel's dynamic buffer)
 template <int N, int NT, typename R>
 __device__ __forceinline__ void hypervisc1_body(const GP &P, const double *__restrict__ U, double *__restrict__ C,
-                                                const int tile, const int IF)
+                                                const int tile, const int IF, R *sbuf)
 {
   constexpr bool MIX = sizeof(R) == sizeof(float);
   constexpr int DoF = N * N;
   constexpr int LT = 256 / DoF;
-  // planes: 0-3 curl/contra of (u,v), 4 theta, 5-8 the first derivatives,
-  // then per tracer its ratio and the two components of its gradient
-  __shared__ R s[9 + 3 * NT][LT * DoF];
+  R(*s)[LT * DoF] = reinterpret_cast<R(*)[LT * DoF]>(sbuf);
   const int t = threadIdx.x;
   const int lvl = t % LT, ID = t / LT;
   const int I = ID % N, Jn = ID / N;
@@ -251,7 +267,7 @@ template <int N, int NT, typename R>
 __global__ void __launch_bounds__(256, 4) k_hypervisc1(const GP P, const double *__restrict__ U,
                                                       double *__restrict__ C)
 {
-  hypervisc1_body<N, NT, R>(P, U, C, blockIdx.x, blockIdx.y);
+  hypervisc1_body<N, NT, R>(P, U, C, blockIdx.x, blockIdx.y, hv1_static_smem<N, NT, R>());
 }
 
 // Contributions and the phase-1 cache: double, or float in the mixed form

@@ -59,11 +59,12 @@ enum {
 // 128 registers a thread fill the register file (a deeper chunk re-stages
 // fewer halo planes: measured 1.65 ms against 1.81 ms with 8 warps at the
 // nPanel 30, nz 45 size); 8 for p < 4, whose deeper chunks would not fit in
-// shared memory.
-template <int N, int NT, typename R>
+// shared memory.  W > 0 sets the warps instead (the fused ensemble stage
+// kernel runs 256-thread CTAs).
+template <int N, int NT, typename R, int W = 0>
 struct P2Cfg {
-  static constexpr int WARPS = N == 5 ? 16 : 8;
-  static constexpr int MINB = N == 5 ? 1 : 2;     // CTAs per SM the registers are sized for
+  static constexpr int WARPS = W > 0 ? W : (N == 5 ? 16 : 8);
+  static constexpr int MINB = WARPS >= 16 ? 1 : 2;   // CTAs per SM the registers are sized for
   static constexpr int DoF = N * N;
   static constexpr int LPW = 32 / DoF;           // levels per warp
   static constexpr int LC = WARPS * LPW;         // levels per CTA
@@ -78,12 +79,12 @@ struct P2Cfg {
                                   (size_t)WARPS * NSCR * SCS * sizeof(R);
 };
 
-template <int N, int NT, typename R>
+template <int N, int NT, typename R, int W = 0>
 __device__ __forceinline__ void phase2_body(const GP &P, const double *__restrict__ U, const double *__restrict__ Pr,
                                             const double *__restrict__ T1, double *__restrict__ C, const int chunk,
                                             const int IF)
 {
-  using CF = P2Cfg<N, NT, R>;
+  using CF = P2Cfg<N, NT, R, W>;
   constexpr bool MIX = sizeof(R) == sizeof(float);
   constexpr int DoF = CF::DoF, LPW = CF::LPW, LC = CF::LC, RP = CF::RP;
   extern __shared__ double sm[];

@@ -180,21 +180,30 @@ int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const do
 /* Batched ensemble.  Members are handles that share OrdPoly, NumTr, the
  * precision and the device; their grids (nPanel, nz) may differ.  One
  * ensemble step advances every member by one Rosenbrock-W step of its own
- * dt, as one CUDA graph of 15 launches over flat work lists spanning all
- * members (the kernels of one stage read each member's parameters from
- * constant memory).  Calls on different batches must not run concurrently:
- * they share those constant tables.  The member handles must stay alive and
- * must not be stepped on their own while their batch steps.
- * With CGD_BATCH_AUTOTUNE the first cgd_batch_step times the candidate
- * work-list orders (member-major, largest member first, interleaved) on
- * copies of the states and keeps the fastest; cgd_batch_tuning reports it.
+ * dt, as one CUDA graph over flat work lists spanning all members (the
+ * kernels of one stage read each member's parameters from constant memory):
+ * either 15 launches (split form) or, with CGD_BATCH_FUSED (OrdPoly 4 only,
+ * CGD_ERR_UNSUPPORTED otherwise), three persistent cooperative launches, one
+ * per stage, each running pressure, both tendency phases with their DSS and
+ * the column solve and update with a grid barrier between them (fused form;
+ * it allocates a second contribution buffer and a second stage state per
+ * member; a barrier wait that exceeds a few seconds ends the launch and the
+ * step returns CGD_ERR_TIMEOUT).  Calls on different batches must not run
+ * concurrently: they share those constant tables.  The member handles must
+ * stay alive and must not be stepped on their own while their batch steps.
+ * With CGD_BATCH_AUTOTUNE the first cgd_batch_step times the candidates -
+ * each work-list order (member-major, largest member first, interleaved) in
+ * the split form and, for OrdPoly 4, in the fused form - on copies of the
+ * states and keeps the fastest; cgd_batch_tuning reports it.
  * No counterpart in the reference, which runs one configuration per job. */
 #define CGD_BATCH_AUTOTUNE 1
+#define CGD_BATCH_FUSED 2
 typedef struct cgd_batch cgd_batch;
 int cgd_batch_create(cgd_handle *const *members, int32_t nmembers, int32_t flags, cgd_batch **out);
 /* U[m] device pointers, dt[m] step sizes; nsteps ensemble steps, in place. */
 int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nsteps);
-/* The chosen work-list order and the timed candidates ("order=...;...=..ms"). */
+/* The chosen candidate and the timed ones
+ * ("order=...;stage=split|fused;<order>/<form>=..ms;..."). */
 int cgd_batch_tuning(cgd_batch *b, char *desc, int32_t len);
 int cgd_batch_get_stream(cgd_batch *b, void **stream);
 void cgd_batch_destroy(cgd_batch *b);

@@ -1,8 +1,10 @@
 """Batched ensemble on the GPU: members on different grids (nPanel, nz) and
-with different dt advance together through cgd_batch_step, one graph of 12
-launches per ensemble step.  The batch runs the single-member kernels on the
-same data in the same order, so every member must come out bit-identical to
-stepping it on its own, with or without the work-order autotuner."""
+with different dt advance together through cgd_batch_step, one graph per
+ensemble step: 15 launches (split form) or one persistent cooperative launch
+per stage (fused form).  Both forms run the single-member kernel bodies on
+the same data in the same order, so every member must come out bit-identical
+to stepping it on its own, in either form and with or without the
+autotuner."""
 import numpy as np
 import pytest
 
@@ -31,9 +33,10 @@ def _host(t):
     return t.cpu().numpy().transpose(2, 1, 0)
 
 
-@pytest.mark.parametrize("exact,autotune,precision", [(True, False, "fp64"), (False, True, "fp64"),
-                                                      (False, False, "mixed")])
-def test_batch_matches_members(oracle_mod, built_lib, cuda_ok, exact, autotune, precision):
+@pytest.mark.parametrize("exact,autotune,precision,fused", [(True, False, "fp64", False), (False, True, "fp64", False),
+                                                            (False, False, "mixed", False), (True, False, "fp64", True),
+                                                            (False, False, "fp64", True), (False, False, "mixed", True)])
+def test_batch_matches_members(oracle_mod, built_lib, cuda_ok, exact, autotune, precision, fused):
     import torch
     from cgd_b200 import Ensemble
     mem = _members(oracle_mod, exact, precision)
@@ -46,7 +49,7 @@ def test_batch_matches_members(oracle_mod, built_lib, cuda_ok, exact, autotune, 
     # fresh handles for the batch (a mixed handle keeps the reference profile
     # of its first state, the same here)
     mem2 = _members(oracle_mod, exact, precision)
-    ens = Ensemble([d for d, _, _ in mem2], autotune=autotune)
+    ens = Ensemble([d for d, _, _ in mem2], autotune=autotune, fused=fused)
     states = [_dev(U) for _, U, _ in mem2]
     ens.step(states, [dt for _, _, dt in mem2], 2)
     ens.step(states, [dt for _, _, dt in mem2], 1)
@@ -55,8 +58,9 @@ def test_batch_matches_members(oracle_mod, built_lib, cuda_ok, exact, autotune, 
         assert np.array_equal(_host(s), r)
     desc = ens.tuning()
     assert desc.startswith("order=")
-    if autotune:
-        assert desc.count("ms") == 3
+    assert ("stage=fused" in desc) == fused or autotune
+    if autotune:   # three orders, split and fused (OrdPoly 4)
+        assert desc.count("ms") == 6, desc
     ens.close()
     for d, _, _ in mem + mem2:
         d.close()
@@ -72,3 +76,13 @@ def test_batch_rejects_mismatched_members(oracle_mod, built_lib, cuda_ok):
     assert e.value.code == -2
     a.close()
     b.close()
+
+
+def test_batch_fused_needs_p4(oracle_mod, built_lib, cuda_ok):
+    from cgd_b200 import CgdError, Dycore, Ensemble
+    o, g, U, nu = make_case(oracle_mod, 3, 3, 6, 0)
+    a = Dycore(g, 0, nu)
+    with pytest.raises(CgdError) as e:
+        Ensemble([a], fused=True)
+    assert e.value.code == -7
+    a.close()
