@@ -450,10 +450,22 @@ __device__ __forceinline__ Mat2 mat2_mul(const Mat2 &x, const Mat2 &y)
 {
   return {x.a * y.a + x.b * y.c, x.a * y.b + x.b * y.d, x.c * y.a + x.d * y.c, x.c * y.b + x.d * y.d};
 }
+// m scaled by 2^-e, e the binary exponent of its largest entry (largest |entry|
+// = f 2^e, 0.5 <= f < 1).  When that entry is a normal number whose 2^-e is
+// normal too (biased exponent 1 .. 2044), the scaling is one multiply by 2^-e,
+// assembled from the exponent bits: a multiply by an exact power of two is
+// the single correctly rounded x 2^-e, so it equals ldexp(x, -e) bit for bit.
+// Other magnitudes (zero, subnormal, near overflow, not finite) take
+// frexp/ldexp.
 __device__ __forceinline__ Mat2 mat2_scaled(Mat2 m)
 {
   const double mx = fmax(fmax(fabs(m.a), fabs(m.b)), fmax(fabs(m.c), fabs(m.d)));
-  if (mx > 0.0) {
+  const int be = (int)((unsigned long long)__double_as_longlong(mx) >> 52);   // mx >= 0: no sign bit
+  if (be >= 1 && be <= 2044) {
+    // e = be - 1022; 2^-e has the biased exponent 1023 - e = 2045 - be
+    const double sc = __longlong_as_double((long long)(2045 - be) << 52);
+    m.a *= sc; m.b *= sc; m.c *= sc; m.d *= sc;
+  } else if (mx > 0.0) {
     int e;
     frexp(mx, &e);
     m.a = ldexp(m.a, -e); m.b = ldexp(m.b, -e); m.c = ldexp(m.c, -e); m.d = ldexp(m.d, -e);
