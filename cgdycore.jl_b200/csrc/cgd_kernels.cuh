@@ -284,12 +284,43 @@ __device__ __forceinline__ void cstore(double *C, long long i, double v)
   else C[i] = v;
 }
 
+// Sum over the NQ contributors (element-node offsets o) of one global DOF at
+// one level, for every field, each sum from 0.0 in ascending order.
+// WSPLIT (the phase-2 tendency): a node's contribution to w at interface l is
+// its upper part (slot 3, level l) plus its lower part (slot NV, stored at
+// level l), zero at the top level.
+template <int NQ, bool WSPLIT, bool C32>
+__device__ __forceinline__ void gather_nq(const GP &P, const double *__restrict__ C, const long long *o, bool wtop,
+                                          size_t fstr, double *acc)
+{
+  double wlo[NQ];
+  if (WSPLIT) {
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) wlo[j] = !wtop ? cload<C32>(C, o[j] + P.NV * fstr) : 0.0;
+  }
+#pragma unroll
+  for (int f = 0; f < MAXNV; ++f) {
+    if (f < P.NV) {
+      double x[NQ];
+#pragma unroll
+      for (int j = 0; j < NQ; ++j) x[j] = !(WSPLIT && f == 3 && wtop) ? cload<C32>(C, o[j] + f * fstr) : 0.0;
+      if (WSPLIT && f == 3) {
+#pragma unroll
+        for (int j = 0; j < NQ; ++j) x[j] = wtop ? 0.0 : x[j] + wlo[j];
+      }
+      double a = 0.0;
+#pragma unroll
+      for (int j = 0; j < NQ; ++j) a += x[j];
+      acc[f] = a;
+    }
+  }
+}
+
 // Sum the contributions of the element nodes sharing global DOF g at level l
-// (ascending element, node order) for every field.  Up to four contributors
-// (every cubed-sphere node) are loaded with independent loads.  WSPLIT (the
-// phase-2 tendency): a node's contribution to w at interface l is its upper
-// part (slot 3, level l) plus its lower part (slot NV, stored at level l),
-// zero at the top level.
+// (ascending element, node order) for every field.  Every cubed-sphere node
+// has 1 to 4 contributors; each count has its own fully unrolled path (the
+// count is uniform over a column, so over a warp of the column kernel), whose
+// loads are all independent.
 template <bool WSPLIT, bool C32>
 __device__ __forceinline__ void gather_node(const GP &P, const double *__restrict__ C, int g, int l, size_t fstr,
                                             double *acc)
@@ -297,45 +328,41 @@ __device__ __forceinline__ void gather_node(const GP &P, const double *__restric
   const int q0 = P.inv_ptr[g], q1 = P.inv_ptr[g + 1];
   const int nq = q1 - q0;
   const bool wtop = WSPLIT && l == P.nz - 1;
-  if (nq <= 4) {
-    long long o[4];
+  long long o[4];
+  switch (nq) {
+    case 1:
+      o[0] = P.inv_off[q0] + l;
+      gather_nq<1, WSPLIT, C32>(P, C, o, wtop, fstr, acc);
+      return;
+    case 2:
 #pragma unroll
-    for (int j = 0; j < 4; ++j) o[j] = j < nq ? P.inv_off[q0 + j] + l : 0;
-    double wlo[4];
-    if (WSPLIT) {
+      for (int j = 0; j < 2; ++j) o[j] = P.inv_off[q0 + j] + l;
+      gather_nq<2, WSPLIT, C32>(P, C, o, wtop, fstr, acc);
+      return;
+    case 3:
 #pragma unroll
-      for (int j = 0; j < 4; ++j) wlo[j] = j < nq && !wtop ? cload<C32>(C, o[j] + P.NV * fstr) : 0.0;
-    }
+      for (int j = 0; j < 3; ++j) o[j] = P.inv_off[q0 + j] + l;
+      gather_nq<3, WSPLIT, C32>(P, C, o, wtop, fstr, acc);
+      return;
+    case 4:
 #pragma unroll
-    for (int f = 0; f < MAXNV; ++f) {
-      if (f < P.NV) {
-        double x[4];
+      for (int j = 0; j < 4; ++j) o[j] = P.inv_off[q0 + j] + l;
+      gather_nq<4, WSPLIT, C32>(P, C, o, wtop, fstr, acc);
+      return;
+    default:
+      break;
+  }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) x[j] = j < nq && !(WSPLIT && f == 3 && wtop) ? cload<C32>(C, o[j] + f * fstr) : 0.0;
-        if (WSPLIT && f == 3) {
-#pragma unroll
-          for (int j = 0; j < 4; ++j) x[j] = wtop ? 0.0 : x[j] + wlo[j];
-        }
-        double a = 0.0;
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (j < nq) a += x[j];
-        acc[f] = a;
+  for (int f = 0; f < MAXNV; ++f) {
+    if (f < P.NV) {
+      double a = 0.0;
+      for (int q = q0; q < q1; ++q) {
+        const long long oq = P.inv_off[q] + l;
+        double x = cload<C32>(C, oq + f * fstr);
+        if (WSPLIT && f == 3) x = wtop ? 0.0 : x + cload<C32>(C, oq + P.NV * fstr);
+        a += x;
       }
-    }
-  } else {
-#pragma unroll
-    for (int f = 0; f < MAXNV; ++f) {
-      if (f < P.NV) {
-        double a = 0.0;
-        for (int q = q0; q < q1; ++q) {
-          const long long o = P.inv_off[q] + l;
-          double x = cload<C32>(C, o + f * fstr);
-          if (WSPLIT && f == 3) x = wtop ? 0.0 : x + cload<C32>(C, o + P.NV * fstr);
-          a += x;
-        }
-        acc[f] = a;
-      }
+      acc[f] = a;
     }
   }
 }
