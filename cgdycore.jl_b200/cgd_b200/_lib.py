@@ -31,6 +31,7 @@ EXPORTS = [
     "cgd_rhs_adjoint", "cgd_ros_step_adjoint", "cgd_set_caller_stream",
     "cgd_tape_record_step", "cgd_tape_step_adjoint", "cgd_tape_release", "cgd_tape_bytes_per_step",
     "cgd_batch_create", "cgd_batch_step", "cgd_batch_tuning", "cgd_batch_get_stream", "cgd_batch_destroy",
+    "cgd_grid_barrier_check",
 ]
 
 
@@ -81,6 +82,8 @@ def lib(exact=False):
         L.cgd_tape_release.restype = ctypes.c_int
         L.cgd_tape_bytes_per_step.argtypes = [vp]
         L.cgd_tape_bytes_per_step.restype = ctypes.c_int64
+        L.cgd_grid_barrier_check.argtypes = [i32, i32, ctypes.c_double, ctypes.POINTER(i32)]
+        L.cgd_grid_barrier_check.restype = ctypes.c_int
         for f in ("cgd_prepare", "cgd_hypervisc_phase1", "cgd_rhs", "cgd_jac"):
             getattr(L, f).argtypes = [vp, vp, vp]
             getattr(L, f).restype = ctypes.c_int

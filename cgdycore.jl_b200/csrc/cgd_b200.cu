@@ -1598,6 +1598,48 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
   return CGD_OK;
 }
 
+int cgd_grid_barrier_check(int32_t rounds, int32_t absent, double limit_s, int32_t *violations)
+{
+  if (rounds < 1 || !(limit_s > 0) || limit_s > 10.0 || !violations) return CGD_ERR_INVALID_ARG;
+  int dev = 0, sms = 0, per_sm = 0, coop = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_barrier_probe, 256, 0);
+  if (e != cudaSuccess) return batch_fail(nullptr, e, "cgd_grid_barrier_check setup");
+  if (!coop || per_sm < 1) return CGD_ERR_UNSUPPORTED;
+  // one allocation: the barrier, the arrival counter, the violation count
+  struct Probe {
+    GridBar bar;
+    unsigned int arrivals;
+    int violations;
+  };
+  Probe *pd = nullptr;
+  e = cudaMalloc(&pd, sizeof(Probe));
+  if (e != cudaSuccess) return batch_fail(nullptr, e, "cgd_grid_barrier_check alloc");
+  Probe init{};
+  // a participant that never arrives: the counter starts one ahead, so the
+  // last real arrival is never the last one
+  if (absent) init.bar.count = 1u;
+  e = cudaMemcpy(pd, &init, sizeof(Probe), cudaMemcpyHostToDevice);
+  const unsigned grid = (unsigned)(absent ? 1 : std::min(per_sm, 2) * sms);
+  const unsigned long long limit_ns = (unsigned long long)(limit_s * 1e9);
+  if (e == cudaSuccess) {
+    GridBar *gb = &pd->bar;
+    unsigned int *arr = &pd->arrivals;
+    int *vio = &pd->violations;
+    void *args[] = {&gb, const_cast<unsigned long long *>(&limit_ns), &rounds, &arr, &vio};
+    e = cudaLaunchCooperativeKernel((const void *)k_barrier_probe, dim3(grid), dim3(256), args, 0, nullptr);
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  Probe out{};
+  if (e == cudaSuccess) e = cudaMemcpy(&out, pd, sizeof(Probe), cudaMemcpyDeviceToHost);
+  cudaFree(pd);
+  if (e != cudaSuccess) return batch_fail(nullptr, e, "cgd_grid_barrier_check");
+  *violations = out.violations;
+  return out.bar.timeout ? CGD_ERR_TIMEOUT : CGD_OK;
+}
+
 int cgd_batch_tuning(cgd_batch *b, char *desc, int32_t len)
 {
   if (!b || !desc || len < 1) return CGD_ERR_INVALID_ARG;

@@ -127,7 +127,7 @@ __device__ __forceinline__ unsigned long long globaltimer_ns()
   return t;
 }
 
-__device__ __forceinline__ bool grid_sync(GridBar *gb)
+__device__ __forceinline__ bool grid_sync(GridBar *gb, unsigned long long limit_ns = GBAR_NS)
 {
   __shared__ int s_ok;
   __syncthreads();
@@ -142,7 +142,7 @@ __device__ __forceinline__ bool grid_sync(GridBar *gb)
     } else {
       const unsigned long long t0 = globaltimer_ns();
       for (unsigned int it = 0; ld_acquire_u32(&gb->gen) == g0; ++it) {
-        if (it >= GBAR_SPINS || globaltimer_ns() - t0 > GBAR_NS) {
+        if (it >= GBAR_SPINS || globaltimer_ns() - t0 > limit_ns) {
           atomicExch(&gb->timeout, 1);
           ok = 0;
           break;
@@ -155,6 +155,20 @@ __device__ __forceinline__ bool grid_sync(GridBar *gb)
   }
   __syncthreads();
   return s_ok != 0;
+}
+
+// Check of the grid barrier: every CTA counts its arrival before each of
+// `rounds` barriers; after barrier r, thread 0 of each CTA must see at least
+// gridDim.x * (r + 1) arrivals, else it counts a violation.  A CTA whose wait
+// timed out leaves (the barrier records the timeout).
+__global__ void __launch_bounds__(256) k_barrier_probe(GridBar *gb, unsigned long long limit_ns, int rounds,
+                                                       unsigned int *arrivals, int *violations)
+{
+  for (int r = 0; r < rounds; ++r) {
+    if (threadIdx.x == 0) atomicAdd(arrivals, 1u);
+    if (!grid_sync(gb, limit_ns)) return;
+    if (threadIdx.x == 0 && ld_acquire_u32(arrivals) < gridDim.x * (unsigned)(r + 1)) atomicAdd(violations, 1);
+  }
 }
 
 // work lists of the fused kernel: 0 phase-1 tiles, 1 blocks of 256

@@ -202,6 +202,15 @@ typedef struct cgd_batch cgd_batch;
 int cgd_batch_create(cgd_handle *const *members, int32_t nmembers, int32_t flags, cgd_batch **out);
 /* U[m] device pointers, dt[m] step sizes; nsteps ensemble steps, in place. */
 int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nsteps);
+/* Check of the grid barrier that the fused stage kernel uses (a bounded spin
+ * on a generation word).  absent = 0: a cooperative launch of two CTAs per
+ * SM passes `rounds` barriers, and *violations counts the CTAs that got past
+ * a barrier before every CTA had arrived (0 expected).  absent != 0: one CTA
+ * waits for a participant that never arrives; its wait ends after limit_s
+ * seconds (at most 10) and the call returns CGD_ERR_TIMEOUT, leaving the
+ * context usable.  Runs on the current device and synchronises it.  No
+ * counterpart in the reference. */
+int cgd_grid_barrier_check(int32_t rounds, int32_t absent, double limit_s, int32_t *violations);
 /* The chosen candidate and the timed ones
  * ("order=...;stage=split|fused;<order>/<form>=..ms;..."). */
 int cgd_batch_tuning(cgd_batch *b, char *desc, int32_t len);

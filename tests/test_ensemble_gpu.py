@@ -86,3 +86,23 @@ def test_batch_fused_needs_p4(oracle_mod, built_lib, cuda_ok):
         Ensemble([a], fused=True)
     assert e.value.code == -7
     a.close()
+
+
+def test_grid_barrier_holds_and_times_out(built_lib, cuda_ok):
+    """The fused kernel's grid barrier: with every CTA present (two per SM,
+    cooperative launch), no CTA passes any of 50 barriers before all have
+    arrived; with a participant that never arrives, the wait ends after its
+    0.2 s limit with CGD_ERR_TIMEOUT, and the device still runs a normal
+    check afterwards."""
+    import ctypes
+    import time
+    from cgd_b200 import _lib
+    L = _lib.lib()
+    v = ctypes.c_int32(-1)
+    assert L.cgd_grid_barrier_check(50, 0, 2.0, ctypes.byref(v)) == 0
+    assert v.value == 0
+    t0 = time.perf_counter()
+    assert L.cgd_grid_barrier_check(3, 1, 0.2, ctypes.byref(v)) == -5   # CGD_ERR_TIMEOUT
+    assert time.perf_counter() - t0 < 5.0
+    assert L.cgd_grid_barrier_check(50, 0, 2.0, ctypes.byref(v)) == 0
+    assert v.value == 0
