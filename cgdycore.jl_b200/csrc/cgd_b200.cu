@@ -9,7 +9,7 @@
 #include "cgd_kernels.cuh"
 #include "cgd_phase2.cuh"
 #include "cgd_batch.cuh"
-#include "cgd_adjoint.cuh"
+#include "cgd_adjoint_launch.h"
 
 #include <cuda_runtime.h>
 #include <atomic>
@@ -323,24 +323,6 @@ void ensure_ref(cgd_handle *h, const double *Ud)
   if (!h->mix || h->have_ref) return;
   k_refprof<<<h->nz, 256, 0, h->stream>>>(h->gp, Ud, h->pref, h->thref);
   h->have_ref = true;
-}
-
-// Reverse of the tendency (no tracers, FP64): phase 2 into the state and
-// cache adjoints, then phase 1 from the cache adjoint into the state adjoint.
-template <int N>
-int rhs_adjoint_launch(cgd_handle *h, const double *Ud, const double *T1, const double *pres, const double *LF,
-                       double *LU)
-{
-  using CF = AdjCfg<N>;
-  static std::atomic<unsigned long long> attr{0};
-  if (first_on_device(attr)) {
-    cudaFuncSetAttribute(k_phase2_adj<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
-  }
-  dim3 grid((h->nz + CF::LC - 1) / CF::LC, h->NF);
-  k_phase2_adj<N><<<grid, CF::THREADS, CF::SMEM, h->stream>>>(h->gp, Ud, pres, T1, LF, LU, h->aLT1);
-  k_hypervisc1_adj<N><<<grid, CF::THREADS, 0, h->stream>>>(h->gp, Ud, h->aLT1, LU);
-  CK(cudaGetLastError());
-  return CGD_OK;
 }
 
 void free_graph(cgd_handle *h)
@@ -859,23 +841,14 @@ int rhs_adjoint_core(cgd_handle *h, const double *Ud, const double *LFd, double 
   }
   CK(cudaMemsetAsync(LUd, 0, S * h->NV * 8, h->stream));
   CK(cudaMemsetAsync(h->aLT1, 0, S * 5 * 8, h->stream));
-  switch (h->N) {
-    case 2: return rhs_adjoint_launch<2>(h, Ud, T1, pres, LFd, LUd);
-    case 3: return rhs_adjoint_launch<3>(h, Ud, T1, pres, LFd, LUd);
-    case 4: return rhs_adjoint_launch<4>(h, Ud, T1, pres, LFd, LUd);
-    default: return rhs_adjoint_launch<5>(h, Ud, T1, pres, LFd, LUd);
-  }
+  CK(launch_rhs_adjoint(h->gp, Ud, T1, pres, LFd, LUd, h->aLT1, h->stream));
+  return CGD_OK;
 }
 
 int column_adj(cgd_handle *h, const double *mu, double mus, const double *kx, const double *jbg, const double *Vn,
                double fac, double *AR, double *LV)
 {
-  CK(cudaFuncSetAttribute(k_column_adj, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          COL_WARPS * CA_ARR * 64 * (int)sizeof(double)));
-  const size_t smem = (size_t)COL_WARPS * CA_ARR * h->nz * sizeof(double);
-  k_column_adj<<<(h->NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, h->stream>>>(
-      h->gp, mu, mus, kx, jbg, Vn, fac, AR, LV);
-  CK(cudaGetLastError());
+  CK(launch_column_adjoint(h->gp, mu, mus, kx, jbg, Vn, fac, AR, LV, h->stream));
   return CGD_OK;
 }
 
@@ -951,7 +924,6 @@ int reverse_step(cgd_handle *h, const StepTape &t, const double *L)
   const double *Vs[3] = {t.u0, t.V2, t.V3};
   CK(cudaMemsetAsync(h->aLV, 0, SV * 8, h->stream));
   const long long n = (long long)SV;
-  const unsigned nb = (unsigned)((n + 255) / 256);
   for (int st = 2; st >= 0; --st) {
     const double cA = st >= 1 ? rk.c[st][0] / dt : 0.0, cB = st == 2 ? rk.c[st][1] / dt : 0.0;
     const double *mu = st == 2 ? L : h->aLk[st];
@@ -961,15 +933,14 @@ int reverse_step(cgd_handle *h, const StepTape &t, const double *L)
     if (rc) return rc;
     // r_st = F(V_st) + c_st0/dt k1 + c_st1/dt k2; V_st = U0 + a_st0 k1 + a_st1 k2
     if (st == 2)
-      k_adj_update<<<nb, 256, 0, h->stream>>>(n, L, h->aAR, h->aLt, h->aLV, h->aLk[0], h->aLk[1], rk.m[0], rk.m[1],
-                                               cA, cB, rk.a[2][0], rk.a[2][1]);
+      CK(launch_adjoint_update(n, L, h->aAR, h->aLt, h->aLV, h->aLk[0], h->aLk[1], rk.m[0], rk.m[1], cA, cB,
+                               rk.a[2][0], rk.a[2][1], h->stream));
     else if (st == 1)
-      k_adj_update<<<nb, 256, 0, h->stream>>>(n, nullptr, h->aAR, h->aLt, h->aLV, h->aLk[0], nullptr, 0.0, 0.0, cA,
-                                               0.0, rk.a[1][0], 0.0);
+      CK(launch_adjoint_update(n, nullptr, h->aAR, h->aLt, h->aLV, h->aLk[0], nullptr, 0.0, 0.0, cA, 0.0,
+                               rk.a[1][0], 0.0, h->stream));
     else
-      k_adj_update<<<nb, 256, 0, h->stream>>>(n, nullptr, nullptr, h->aLt, h->aLV, nullptr, nullptr, 0.0, 0.0, 0.0,
-                                               0.0, 0.0, 0.0);
-    CK(cudaGetLastError());
+      CK(launch_adjoint_update(n, nullptr, nullptr, h->aLt, h->aLV, nullptr, nullptr, 0.0, 0.0, 0.0, 0.0, 0.0,
+                               0.0, h->stream));
   }
   return CGD_OK;
 }

@@ -789,6 +789,9 @@ __global__ void __launch_bounds__(32 * COL_WARPS, MODE == 2 ? 3 : 4) k_column(co
   column_body<MODE, C32>(P, A, blockIdx.x);
 }
 
+// The kernels below are defined by the forward translation unit only (the
+// adjoint's, cgd_adjoint.cu, includes this header for its device functions).
+#ifndef CGD_ADJOINT_TU
 // Mixed form: the FP64 reference profile of pressure and theta, the
 // horizontal mean of each level of a state (one CTA per level, fixed-order
 // tree reduction, so the profile is reproducible).
@@ -891,5 +894,7 @@ __global__ void k_mass_final(const double *__restrict__ part, int nb, double *__
     out[0] = acc;
   }
 }
+
+#endif  // CGD_ADJOINT_TU
 
 } // namespace cgd

@@ -42,7 +42,10 @@ def test_library_is_sm100a(built_lib):
     from cgd_b200 import build
     flags = " ".join(build.NVCC_FLAGS)
     assert "arch=compute_100a,code=sm_100a" in flags
-    assert build.VARIANTS[build.LIB_PATH_EXACT] == ["-fmad=false"]
+    # the forward kernels without multiply-add contraction (the exact build
+    # matches the restatement bit for bit), the adjoint's unit with it
+    assert build.VARIANTS[build.LIB_PATH_EXACT] == [] and build.FWD_FLAGS == ["-fmad=false"]
+    assert build.ADJ_FLAGS == ["-fmad=true"]
     from cgd_b200 import _lib
     assert b"sm_100a" in _lib.lib().cgd_version() and b"fast" in _lib.lib().cgd_version()
     assert b"exact" in _lib.lib(exact=True).cgd_version()
