@@ -490,7 +490,7 @@ def run_ensemble(args, rank, world, local):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (baroclinic wave + seeded member perturbations)",
             "config": {"workload": "batched ensemble: 48 members on 3 grids, one CUDA graph per ensemble step "
                                    "(15 launches split, or 3 fused persistent stage launches; the autotuner picks "
-                                   "the order and the form)", "grids": E["grids"], "per_grid": E["per_grid"],
+                                   "the work-list order, the form and the levels per phase-2 CTA)", "grids": E["grids"], "per_grid": E["per_grid"],
                        "dt": E["dt"], "hours": E["hours"], "steps_total": nsteps,
                        "perturbation": f"theta +-{E['theta_amp']} K, u,v +-{E['wind_amp']} m/s, seed "
                                        f"{E['seed0']}+member",

@@ -1123,10 +1123,12 @@ struct cgd_batch {
   cudaStream_t stream = nullptr;
   cudaEvent_t order_ev = nullptr;   // orders a step after the first member's caller stream
   // work lists, one set per candidate order; a candidate is (order, form):
-  // candidate c runs order c % NORD, split into 15 launches (c < NORD) or as
-  // three fused stage launches (c >= NORD)
+  // candidate c runs order c % NORD in form c / NORD: split into 15 launches
+  // (FORM_SPLIT), split with phase 2 in 8-level chunks (FORM_SPLIT8, p = 4),
+  // or as three fused stage launches (FORM_FUSED)
   static constexpr int NORD = 3;
-  static constexpr int NCAND = 2 * NORD;
+  static constexpr int FORM_SPLIT = 0, FORM_SPLIT8 = 1, FORM_FUSED = 2, NFORM = 3;
+  static constexpr int NCAND = NFORM * NORD;
   WItem *w[NORD][5] = {};
   int n[5] = {};
   cudaGraph_t graph[NCAND] = {};
@@ -1150,7 +1152,19 @@ struct cgd_batch {
 namespace {
 
 const char *const ORDER_NAME[cgd_batch::NORD] = {"member-major", "largest-member-first", "members-interleaved"};
-const char *const FORM_NAME[2] = {"split", "fused"};
+const char *const FORM_NAME[cgd_batch::NFORM] = {"split", "split8", "fused"};
+int form_of(int cand) { return cand / cgd_batch::NORD; }
+// levels per phase-2 CTA of a form
+int phase2_levels(int N, int form)
+{
+  if (form != cgd_batch::FORM_SPLIT) return P2Cfg<5, 0, double, FUSED_P2_WARPS>::LC;
+  switch (N) {
+    case 2: return P2Cfg<2, 0, double>::LC;
+    case 3: return P2Cfg<3, 0, double>::LC;
+    case 4: return P2Cfg<4, 0, double>::LC;
+    default: return P2Cfg<5, 0, double>::LC;
+  }
+}
 
 int batch_fail(cgd_batch *b, cudaError_t e, const char *what)
 {
@@ -1216,13 +1230,17 @@ void batch_lists(const cgd_batch *b, int order, std::vector<WItem> out[5])
 }
 
 template <int N, int NT, typename R>
-void batch_enqueue_t(cgd_batch *b, WItem *const *w)
+void batch_enqueue_t(cgd_batch *b, WItem *const *w, bool p2w8)
 {
   using CF = P2Cfg<N, NT, R>;
+  using CF8 = P2Cfg<N, NT, R, FUSED_P2_WARPS>;
   static std::atomic<unsigned long long> attr{0};
   const size_t csmem = (size_t)COL_WARPS * COL_ARR * b->nzmax * sizeof(double);
   if (first_on_device(attr)) {
     cudaFuncSetAttribute(kb_phase2<N, NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
+    if constexpr (N == 5)
+      cudaFuncSetAttribute(kb_phase2<N, NT, R, FUSED_P2_WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)CF8::SMEM);
     constexpr bool C32 = sizeof(R) == sizeof(float);
     for (auto f : {kb_column<0, C32>, kb_column<1, C32>, kb_column<2, C32>})
       cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, COL_WARPS * COL_ARR * 64 * (int)sizeof(double));
@@ -1231,7 +1249,12 @@ void batch_enqueue_t(cgd_batch *b, WItem *const *w)
   for (int stage = 0; stage < 3; ++stage) {
     kb_hypervisc1<N, NT, R><<<b->n[0], 256, 0, b->stream>>>(w[0], stage);
     kb_gather<sizeof(R) == sizeof(float)><<<b->n[1], 256, 0, b->stream>>>(w[1]);
-    kb_phase2<N, NT, R><<<b->n[2], CF::THREADS, CF::SMEM, b->stream>>>(w[2], stage);
+    if constexpr (N == 5) {
+      if (p2w8) kb_phase2<N, NT, R, FUSED_P2_WARPS><<<b->n[4], CF8::THREADS, CF8::SMEM, b->stream>>>(w[4], stage);
+      else kb_phase2<N, NT, R><<<b->n[2], CF::THREADS, CF::SMEM, b->stream>>>(w[2], stage);
+    } else {
+      kb_phase2<N, NT, R><<<b->n[2], CF::THREADS, CF::SMEM, b->stream>>>(w[2], stage);
+    }
     constexpr bool C32 = sizeof(R) == sizeof(float);
     if (stage == 0) kb_column<0, C32><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);
     else if (stage == 1) kb_column<1, C32><<<b->n[3], 32 * COL_WARPS, csmem, b->stream>>>(w[3]);
@@ -1241,25 +1264,25 @@ void batch_enqueue_t(cgd_batch *b, WItem *const *w)
 }
 
 template <int N, typename R>
-void batch_enqueue_n(cgd_batch *b, WItem *const *w)
+void batch_enqueue_n(cgd_batch *b, WItem *const *w, bool p2w8)
 {
   switch (b->NT) {
-    case 0: batch_enqueue_t<N, 0, R>(b, w); break;
-    case 1: batch_enqueue_t<N, 1, R>(b, w); break;
-    case 2: batch_enqueue_t<N, 2, R>(b, w); break;
-    case 3: batch_enqueue_t<N, 3, R>(b, w); break;
-    default: batch_enqueue_t<N, 4, R>(b, w); break;
+    case 0: batch_enqueue_t<N, 0, R>(b, w, p2w8); break;
+    case 1: batch_enqueue_t<N, 1, R>(b, w, p2w8); break;
+    case 2: batch_enqueue_t<N, 2, R>(b, w, p2w8); break;
+    case 3: batch_enqueue_t<N, 3, R>(b, w, p2w8); break;
+    default: batch_enqueue_t<N, 4, R>(b, w, p2w8); break;
   }
 }
 
 template <typename R>
-void batch_enqueue_r(cgd_batch *b, WItem *const *w)
+void batch_enqueue_r(cgd_batch *b, WItem *const *w, bool p2w8)
 {
   switch (b->N) {
-    case 2: batch_enqueue_n<2, R>(b, w); break;
-    case 3: batch_enqueue_n<3, R>(b, w); break;
-    case 4: batch_enqueue_n<4, R>(b, w); break;
-    default: batch_enqueue_n<5, R>(b, w); break;
+    case 2: batch_enqueue_n<2, R>(b, w, p2w8); break;
+    case 3: batch_enqueue_n<3, R>(b, w, p2w8); break;
+    case 4: batch_enqueue_n<4, R>(b, w, p2w8); break;
+    default: batch_enqueue_n<5, R>(b, w, p2w8); break;
   }
 }
 
@@ -1338,9 +1361,11 @@ cudaError_t fused_setup_r(cgd_batch *b)
 cudaError_t batch_enqueue(cgd_batch *b, int cand)
 {
   WItem *const *w = b->w[cand % cgd_batch::NORD];
-  if (cand >= cgd_batch::NORD) return b->mix ? batch_enqueue_fused_r<float>(b, w) : batch_enqueue_fused_r<double>(b, w);
-  if (b->mix) batch_enqueue_r<float>(b, w);
-  else batch_enqueue_r<double>(b, w);
+  const int form = form_of(cand);
+  if (form == cgd_batch::FORM_FUSED)
+    return b->mix ? batch_enqueue_fused_r<float>(b, w) : batch_enqueue_fused_r<double>(b, w);
+  if (b->mix) batch_enqueue_r<float>(b, w, form == cgd_batch::FORM_SPLIT8);
+  else batch_enqueue_r<double>(b, w, form == cgd_batch::FORM_SPLIT8);
   return cudaSuccess;
 }
 
@@ -1410,11 +1435,14 @@ int cgd_batch_create(cgd_handle *const *members, int32_t nmembers, int32_t flags
       fused_ok = coop && b->fgrid > 0;
     }
     if (want_fused && !fused_ok) { rc = CGD_ERR_UNSUPPORTED; break; }
+    const int first = want_fused ? cgd_batch::FORM_FUSED * cgd_batch::NORD : 0;
     for (int c = 0; c < cgd_batch::NCAND; ++c) {
-      const bool fused = c >= cgd_batch::NORD;
-      b->use[c] = b->autotune ? (!fused || fused_ok) : c == (want_fused ? cgd_batch::NORD : 0);
+      const int form = form_of(c);
+      const bool avail = form == cgd_batch::FORM_SPLIT || (form == cgd_batch::FORM_SPLIT8 && b->N == 5) ||
+                         (form == cgd_batch::FORM_FUSED && fused_ok);
+      b->use[c] = b->autotune ? avail : c == first;
     }
-    if (!b->autotune) b->chosen = want_fused ? cgd_batch::NORD : 0;
+    if (!b->autotune) b->chosen = first;
     if (fused_ok) {
       void *p = nullptr;
       e = cudaMalloc(&p, sizeof(GridBar));
@@ -1544,7 +1572,7 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
       float ms = 0.f;
       BCK(cudaEventElapsedTime(&ms, e0, e1));
       b->tune_ms[c] = ms;
-      if (c >= cgd_batch::NORD && fused_timed_out(b)) {
+      if (form_of(c) == cgd_batch::FORM_FUSED && fused_timed_out(b)) {
         g_last_error = "cgd_batch_step: a fused stage launch timed out at a grid barrier";
         return CGD_ERR_TIMEOUT;
       }
@@ -1562,7 +1590,7 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
   for (int s = 0; s < nsteps; ++s) BCK(cudaGraphLaunch(b->gexec[b->chosen], b->stream));
   BCK(cudaStreamSynchronize(b->stream));
   BCK(cudaGetLastError());
-  if (b->chosen >= cgd_batch::NORD && fused_timed_out(b)) {
+  if (form_of(b->chosen) == cgd_batch::FORM_FUSED && fused_timed_out(b)) {
     g_last_error = "cgd_batch_step: a fused stage launch timed out at a grid barrier";
     return CGD_ERR_TIMEOUT;
   }
@@ -1614,13 +1642,15 @@ int cgd_grid_barrier_check(int32_t rounds, int32_t absent, double limit_s, int32
 int cgd_batch_tuning(cgd_batch *b, char *desc, int32_t len)
 {
   if (!b || !desc || len < 1) return CGD_ERR_INVALID_ARG;
+  const int form = form_of(b->chosen);
   std::string s = std::string("order=") + ORDER_NAME[b->chosen % cgd_batch::NORD] + ";stage=" +
-                  FORM_NAME[b->chosen >= cgd_batch::NORD];
+                  (form == cgd_batch::FORM_FUSED ? "fused" : "split") + ";phase2_levels=" +
+                  std::to_string(phase2_levels(b->N, form));
   if (b->tuned) {
     char buf[96];
     for (int c = 0; c < cgd_batch::NCAND; ++c) {
       if (!b->use[c]) continue;
-      snprintf(buf, sizeof buf, ";%s/%s=%.3fms", ORDER_NAME[c % cgd_batch::NORD], FORM_NAME[c >= cgd_batch::NORD],
+      snprintf(buf, sizeof buf, ";%s/%s=%.3fms", ORDER_NAME[c % cgd_batch::NORD], FORM_NAME[form_of(c)],
                b->tune_ms[c]);
       s += buf;
     }

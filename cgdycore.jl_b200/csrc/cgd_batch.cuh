@@ -63,12 +63,14 @@ __global__ void __launch_bounds__(256) kb_gather(const WItem *__restrict__ w)
   gather_body<false, true, C32>(c_bgp[it.m], B.C, B.T1, (long long)it.x * blockDim.x + threadIdx.x);
 }
 
-template <int N, int NT, typename R>
-__global__ void __launch_bounds__(P2Cfg<N, NT, R>::THREADS, P2Cfg<N, NT, R>::MINB) kb_phase2(const WItem *__restrict__ w, const int stage)
+// W > 0: phase 2 in chunks of W warps (levels, for p = 4) instead of the default
+template <int N, int NT, typename R, int W = 0>
+__global__ void __launch_bounds__(P2Cfg<N, NT, R, W>::THREADS, P2Cfg<N, NT, R, W>::MINB)
+    kb_phase2(const WItem *__restrict__ w, const int stage)
 {
   const WItem it = w[blockIdx.x];
   const BMember &B = c_bm[it.m];
-  phase2_body<N, NT, R>(c_bgp[it.m], stage == 0 ? B.U : B.Vst, stage == 0 ? B.P0 : B.Pst, B.T1, B.C, it.x, it.y);
+  phase2_body<N, NT, R, W>(c_bgp[it.m], stage == 0 ? B.U : B.Vst, stage == 0 ? B.P0 : B.Pst, B.T1, B.C, it.x, it.y);
 }
 
 template <int MODE, bool C32>

@@ -193,7 +193,8 @@ int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const do
  * stay alive and must not be stepped on their own while their batch steps.
  * With CGD_BATCH_AUTOTUNE the first cgd_batch_step times the candidates -
  * each work-list order (member-major, largest member first, interleaved) in
- * the split form and, for OrdPoly 4, in the fused form - on copies of the
+ * the split form and, for OrdPoly 4, in the split form with phase 2 in
+ * 8-level instead of 16-level CTAs and in the fused form - on copies of the
  * states and keeps the fastest; cgd_batch_tuning reports it.
  * No counterpart in the reference, which runs one configuration per job. */
 #define CGD_BATCH_AUTOTUNE 1
@@ -211,8 +212,8 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
  * context usable.  Runs on the current device and synchronises it.  No
  * counterpart in the reference. */
 int cgd_grid_barrier_check(int32_t rounds, int32_t absent, double limit_s, int32_t *violations);
-/* The chosen candidate and the timed ones
- * ("order=...;stage=split|fused;<order>/<form>=..ms;..."). */
+/* The chosen candidate and the timed ones ("order=...;stage=split|fused;
+ * phase2_levels=<levels per phase-2 CTA>;<order>/<split|split8|fused>=..ms;..."). */
 int cgd_batch_tuning(cgd_batch *b, char *desc, int32_t len);
 int cgd_batch_get_stream(cgd_batch *b, void **stream);
 void cgd_batch_destroy(cgd_batch *b);

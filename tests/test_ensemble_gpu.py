@@ -59,8 +59,9 @@ def test_batch_matches_members(oracle_mod, built_lib, cuda_ok, exact, autotune, 
     desc = ens.tuning()
     assert desc.startswith("order=")
     assert ("stage=fused" in desc) == fused or autotune
-    if autotune:   # three orders, split and fused (OrdPoly 4)
-        assert desc.count("ms") == 6, desc
+    if autotune:   # three orders x split, split with 8-level phase-2 CTAs, fused (OrdPoly 4)
+        assert desc.count("ms") == 9, desc
+        assert "phase2_levels=" in desc
     ens.close()
     for d, _, _ in mem + mem2:
         d.close()
