@@ -626,7 +626,7 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS, 2) k_phase2_adj(const GP P, co
 // cache, broadcast to the element nodes).  Phase 1 is linear in u, v and
 // theta = rho*theta / rho.
 template <int N>
-__global__ void __launch_bounds__(32 * ADJ_WARPS, 3) k_hypervisc1_adj(const GP P, const double *__restrict__ U,
+__global__ void __launch_bounds__(32 * ADJ_WARPS, 5) k_hypervisc1_adj(const GP P, const double *__restrict__ U,
                                                                   const double *__restrict__ LT1,
                                                                   double *__restrict__ LU)
 {
@@ -764,7 +764,7 @@ __global__ void __launch_bounds__(256) k_adj_update(long long n, const double *_
 // column throughout.
 constexpr int CA_ARR = 18;   // per-warp arrays of nz entries
 
-__global__ void __launch_bounds__(32 * COL_WARPS, 3) k_column_adj(const GP P, const double *__restrict__ mu, double mus,
+__global__ void __launch_bounds__(32 * COL_WARPS, 4) k_column_adj(const GP P, const double *__restrict__ mu, double mus,
                                                                  const double *__restrict__ kx,
                                                                  const double *__restrict__ jbg,
                                                                  const double *__restrict__ Vn, double fac,
@@ -847,9 +847,16 @@ __global__ void __launch_bounds__(32 * COL_WARPS, 3) k_column_adj(const GP P, co
   // dp/d(rho*theta) of every level and its derivative factor kappa/(1-kappa) dp/(rho*theta)
   const double ex = P.kappa / (1.0 - P.kappa);
   double *dP = tri, *dPd = tri + 2 * LS;   // t0, t2 are dead after the sweep
+  // dp/d(rho*theta) is recovered from the step's bands, JWRhoTh = +-dp / (RhoF h)
+  // (h = (dzL + dzR) / 2): level l < n from interface l (its lower level), the
+  // top level from interface n - 1 (its upper level); no pow per level
+  const double *V0c = Vn + (size_t)nz * g;
   for (int l = lane; l < nz; l += 32) {
-    const double Th = Vn[l + (size_t)nz * g + 4 * fs] + 0.0;
-    const double d = dpdrhoth(P, Th);
+    const double Th = V0c[l + 4 * fs] + 0.0;
+    const int li = l < n ? l : n - 1;
+    const double dzL = P.dz[li + (size_t)nz * g], dzR = P.dz[li + 1 + (size_t)nz * g], dzs = dzL + dzR;
+    const double RhoF = (V0c[li] * dzL + V0c[li + 1] * dzR) / dzs;
+    const double d = (l < n ? JB(2, 1, li) : -JB(2, 0, li)) * RhoF * (0.5 * dzs);
     dP[l] = d;
     dPd[l] = ex * d / Th;
   }

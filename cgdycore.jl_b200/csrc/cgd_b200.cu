@@ -1124,10 +1124,10 @@ struct cgd_batch {
   cudaEvent_t order_ev = nullptr;   // orders a step after the first member's caller stream
   // work lists, one set per candidate order; a candidate is (order, form):
   // candidate c runs order c % NORD in form c / NORD: split into 15 launches
-  // (FORM_SPLIT), split with phase 2 in 8-level chunks (FORM_SPLIT8, p = 4),
+  // (FORM_SPLIT), split with phase 2 in 16-level CTAs (FORM_SPLIT16, p = 4),
   // or as three fused stage launches (FORM_FUSED)
   static constexpr int NORD = 3;
-  static constexpr int FORM_SPLIT = 0, FORM_SPLIT8 = 1, FORM_FUSED = 2, NFORM = 3;
+  static constexpr int FORM_SPLIT = 0, FORM_SPLIT16 = 1, FORM_FUSED = 2, NFORM = 3;
   static constexpr int NCAND = NFORM * NORD;
   WItem *w[NORD][5] = {};
   int n[5] = {};
@@ -1152,12 +1152,12 @@ struct cgd_batch {
 namespace {
 
 const char *const ORDER_NAME[cgd_batch::NORD] = {"member-major", "largest-member-first", "members-interleaved"};
-const char *const FORM_NAME[cgd_batch::NFORM] = {"split", "split8", "fused"};
+const char *const FORM_NAME[cgd_batch::NFORM] = {"split", "split16", "fused"};
 int form_of(int cand) { return cand / cgd_batch::NORD; }
 // levels per phase-2 CTA of a form
 int phase2_levels(int N, int form)
 {
-  if (form != cgd_batch::FORM_SPLIT) return P2Cfg<5, 0, double, FUSED_P2_WARPS>::LC;
+  if (form == cgd_batch::FORM_SPLIT16) return P2Cfg<5, 0, double, P2_ALT_WARPS>::LC;
   switch (N) {
     case 2: return P2Cfg<2, 0, double>::LC;
     case 3: return P2Cfg<3, 0, double>::LC;
@@ -1190,12 +1190,12 @@ void batch_lists(const cgd_batch *b, int order, std::vector<WItem> out[5])
   for (int k = 0; k < 5; ++k) per[k].resize(nm);
   const int DoF = b->N * b->N;
   const int LT = 256 / DoF;
-  int LC = 0, LCF = 0;   // phase-2 levels per CTA: split form, fused form
+  int LC = 0, LCA = 0;   // phase-2 levels per CTA: default, alternative (p = 4 only)
   switch (b->N) {
-    case 2: LC = P2Cfg<2, 0, double>::LC; LCF = P2Cfg<2, 0, double, FUSED_P2_WARPS>::LC; break;
-    case 3: LC = P2Cfg<3, 0, double>::LC; LCF = P2Cfg<3, 0, double, FUSED_P2_WARPS>::LC; break;
-    case 4: LC = P2Cfg<4, 0, double>::LC; LCF = P2Cfg<4, 0, double, FUSED_P2_WARPS>::LC; break;
-    default: LC = P2Cfg<5, 0, double>::LC; LCF = P2Cfg<5, 0, double, FUSED_P2_WARPS>::LC; break;
+    case 2: LC = LCA = P2Cfg<2, 0, double>::LC; break;
+    case 3: LC = LCA = P2Cfg<3, 0, double>::LC; break;
+    case 4: LC = LCA = P2Cfg<4, 0, double>::LC; break;
+    default: LC = P2Cfg<5, 0, double>::LC; LCA = P2Cfg<5, 0, double, P2_ALT_WARPS>::LC; break;
   }
   for (int m = 0; m < nm; ++m) {
     const cgd_handle *h = b->mem[m];
@@ -1207,7 +1207,7 @@ void batch_lists(const cgd_batch *b, int order, std::vector<WItem> out[5])
       for (int c = 0; c < (h->nz + LC - 1) / LC; ++c) per[2][m].push_back({m, c, IF});
     for (int c = 0; c < (h->NumG + COL_WARPS - 1) / COL_WARPS; ++c) per[3][m].push_back({m, c, 0});
     for (int IF = 0; IF < h->NF; ++IF)
-      for (int c = 0; c < (h->nz + LCF - 1) / LCF; ++c) per[4][m].push_back({m, c, IF});
+      for (int c = 0; c < (h->nz + LCA - 1) / LCA; ++c) per[4][m].push_back({m, c, IF});
   }
   std::vector<int> ord(nm);
   for (int m = 0; m < nm; ++m) ord[m] = m;
@@ -1230,17 +1230,17 @@ void batch_lists(const cgd_batch *b, int order, std::vector<WItem> out[5])
 }
 
 template <int N, int NT, typename R>
-void batch_enqueue_t(cgd_batch *b, WItem *const *w, bool p2w8)
+void batch_enqueue_t(cgd_batch *b, WItem *const *w, bool p2alt)
 {
   using CF = P2Cfg<N, NT, R>;
-  using CF8 = P2Cfg<N, NT, R, FUSED_P2_WARPS>;
+  using CFA = P2Cfg<N, NT, R, P2_ALT_WARPS>;
   static std::atomic<unsigned long long> attr{0};
   const size_t csmem = (size_t)COL_WARPS * COL_ARR * b->nzmax * sizeof(double);
   if (first_on_device(attr)) {
     cudaFuncSetAttribute(kb_phase2<N, NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
     if constexpr (N == 5)
-      cudaFuncSetAttribute(kb_phase2<N, NT, R, FUSED_P2_WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)CF8::SMEM);
+      cudaFuncSetAttribute(kb_phase2<N, NT, R, P2_ALT_WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)CFA::SMEM);
     constexpr bool C32 = sizeof(R) == sizeof(float);
     for (auto f : {kb_column<0, C32>, kb_column<1, C32>, kb_column<2, C32>})
       cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, COL_WARPS * COL_ARR * 64 * (int)sizeof(double));
@@ -1250,7 +1250,7 @@ void batch_enqueue_t(cgd_batch *b, WItem *const *w, bool p2w8)
     kb_hypervisc1<N, NT, R><<<b->n[0], 256, 0, b->stream>>>(w[0], stage);
     kb_gather<sizeof(R) == sizeof(float)><<<b->n[1], 256, 0, b->stream>>>(w[1]);
     if constexpr (N == 5) {
-      if (p2w8) kb_phase2<N, NT, R, FUSED_P2_WARPS><<<b->n[4], CF8::THREADS, CF8::SMEM, b->stream>>>(w[4], stage);
+      if (p2alt) kb_phase2<N, NT, R, P2_ALT_WARPS><<<b->n[4], CFA::THREADS, CFA::SMEM, b->stream>>>(w[4], stage);
       else kb_phase2<N, NT, R><<<b->n[2], CF::THREADS, CF::SMEM, b->stream>>>(w[2], stage);
     } else {
       kb_phase2<N, NT, R><<<b->n[2], CF::THREADS, CF::SMEM, b->stream>>>(w[2], stage);
@@ -1264,25 +1264,25 @@ void batch_enqueue_t(cgd_batch *b, WItem *const *w, bool p2w8)
 }
 
 template <int N, typename R>
-void batch_enqueue_n(cgd_batch *b, WItem *const *w, bool p2w8)
+void batch_enqueue_n(cgd_batch *b, WItem *const *w, bool p2alt)
 {
   switch (b->NT) {
-    case 0: batch_enqueue_t<N, 0, R>(b, w, p2w8); break;
-    case 1: batch_enqueue_t<N, 1, R>(b, w, p2w8); break;
-    case 2: batch_enqueue_t<N, 2, R>(b, w, p2w8); break;
-    case 3: batch_enqueue_t<N, 3, R>(b, w, p2w8); break;
-    default: batch_enqueue_t<N, 4, R>(b, w, p2w8); break;
+    case 0: batch_enqueue_t<N, 0, R>(b, w, p2alt); break;
+    case 1: batch_enqueue_t<N, 1, R>(b, w, p2alt); break;
+    case 2: batch_enqueue_t<N, 2, R>(b, w, p2alt); break;
+    case 3: batch_enqueue_t<N, 3, R>(b, w, p2alt); break;
+    default: batch_enqueue_t<N, 4, R>(b, w, p2alt); break;
   }
 }
 
 template <typename R>
-void batch_enqueue_r(cgd_batch *b, WItem *const *w, bool p2w8)
+void batch_enqueue_r(cgd_batch *b, WItem *const *w, bool p2alt)
 {
   switch (b->N) {
-    case 2: batch_enqueue_n<2, R>(b, w, p2w8); break;
-    case 3: batch_enqueue_n<3, R>(b, w, p2w8); break;
-    case 4: batch_enqueue_n<4, R>(b, w, p2w8); break;
-    default: batch_enqueue_n<5, R>(b, w, p2w8); break;
+    case 2: batch_enqueue_n<2, R>(b, w, p2alt); break;
+    case 3: batch_enqueue_n<3, R>(b, w, p2alt); break;
+    case 4: batch_enqueue_n<4, R>(b, w, p2alt); break;
+    default: batch_enqueue_n<5, R>(b, w, p2alt); break;
   }
 }
 
@@ -1364,8 +1364,8 @@ cudaError_t batch_enqueue(cgd_batch *b, int cand)
   const int form = form_of(cand);
   if (form == cgd_batch::FORM_FUSED)
     return b->mix ? batch_enqueue_fused_r<float>(b, w) : batch_enqueue_fused_r<double>(b, w);
-  if (b->mix) batch_enqueue_r<float>(b, w, form == cgd_batch::FORM_SPLIT8);
-  else batch_enqueue_r<double>(b, w, form == cgd_batch::FORM_SPLIT8);
+  if (b->mix) batch_enqueue_r<float>(b, w, form == cgd_batch::FORM_SPLIT16);
+  else batch_enqueue_r<double>(b, w, form == cgd_batch::FORM_SPLIT16);
   return cudaSuccess;
 }
 
@@ -1438,7 +1438,7 @@ int cgd_batch_create(cgd_handle *const *members, int32_t nmembers, int32_t flags
     const int first = want_fused ? cgd_batch::FORM_FUSED * cgd_batch::NORD : 0;
     for (int c = 0; c < cgd_batch::NCAND; ++c) {
       const int form = form_of(c);
-      const bool avail = form == cgd_batch::FORM_SPLIT || (form == cgd_batch::FORM_SPLIT8 && b->N == 5) ||
+      const bool avail = form == cgd_batch::FORM_SPLIT || (form == cgd_batch::FORM_SPLIT16 && b->N == 5) ||
                          (form == cgd_batch::FORM_FUSED && fused_ok);
       b->use[c] = b->autotune ? avail : c == first;
     }

@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(256) kb_gather(const WItem *__restrict__ w)
   gather_body<false, true, C32>(c_bgp[it.m], B.C, B.T1, (long long)it.x * blockDim.x + threadIdx.x);
 }
 
-// W > 0: phase 2 in chunks of W warps (levels, for p = 4) instead of the default
+// W > 0: phase 2 in CTAs of W warps (levels, for p = 4) instead of the default
 template <int N, int NT, typename R, int W = 0>
 __global__ void __launch_bounds__(P2Cfg<N, NT, R, W>::THREADS, P2Cfg<N, NT, R, W>::MINB)
     kb_phase2(const WItem *__restrict__ w, const int stage)
@@ -174,9 +174,11 @@ __global__ void __launch_bounds__(256) k_barrier_probe(GridBar *gb, unsigned lon
 }
 
 // work lists of the fused kernel: 0 phase-1 tiles, 1 blocks of 256
-// column-levels (DSS gather, pressure), 3 blocks of COL_WARPS columns, 4
-// phase-2 chunks of FUSED_P2_WARPS levels
+// column-levels (DSS gather, pressure), 2 phase-2 chunks (the default
+// FUSED_P2_WARPS-warp CTAs), 3 blocks of COL_WARPS columns
 constexpr int FUSED_P2_WARPS = 8;
+// the split form's alternative phase-2 CTA for p = 4 (autotuner), work list 4
+constexpr int P2_ALT_WARPS = 16;
 struct FusedArgs {
   const WItem *w[5];
   int n[5];
@@ -195,6 +197,7 @@ __global__ void __launch_bounds__(256, 2) kb_stage(const FusedArgs A, const int 
 {
   constexpr bool C32 = sizeof(R) == sizeof(float);
   static_assert(P2Cfg<N, NT, R, FUSED_P2_WARPS>::THREADS == 256, "phase-2 chunks of 256 threads");
+  static_assert(P2Cfg<N, NT, R, FUSED_P2_WARPS>::LC == P2Cfg<N, NT, R>::LC, "the default phase-2 work list");
   static_assert(32 * COL_WARPS == 256, "column blocks of 256 threads");
   extern __shared__ double fsm[];   // each part's shared arrays in turn (phase 1, phase 2, column)
   if (stage == 0) {   // pressure of the step's state
@@ -221,8 +224,8 @@ __global__ void __launch_bounds__(256, 2) kb_stage(const FusedArgs A, const int 
   }
   if (!grid_sync(A.bar)) return;
   // phase 2 -> C2
-  for (int i = blockIdx.x; i < A.n[4]; i += gridDim.x) {
-    const WItem it = A.w[4][i];
+  for (int i = blockIdx.x; i < A.n[2]; i += gridDim.x) {
+    const WItem it = A.w[2][i];
     const BMember &B = c_bm[it.m];
     phase2_body<N, NT, R, FUSED_P2_WARPS>(c_bgp[it.m], fused_stage_state(B, stage), stage == 0 ? B.P0 : B.Pst,
                                           B.T1, B.C2, it.x, it.y);

@@ -55,15 +55,14 @@ enum {
   O_T1    // + 5 + NumTr: the DSS'd hyperviscosity cache
 };
 
-// Warps (levels) per CTA: 16 for p = 4, one 512-thread CTA per SM, whose
-// 128 registers a thread fill the register file (a deeper chunk re-stages
-// fewer halo planes: measured 1.65 ms against 1.81 ms with 8 warps at the
-// nPanel 30, nz 45 size); 8 for p < 4, whose deeper chunks would not fit in
-// shared memory.  W > 0 sets the warps instead (the fused ensemble stage
-// kernel runs 256-thread CTAs).
+// Warps (levels for p = 4) per CTA: 8, two 256-thread CTAs per SM at 128
+// registers a thread, so that one CTA's staging overlaps the other's
+// arithmetic (at nPanel 30, nz 45: 1.415 ms against 1.533 ms for one
+// 512-thread CTA of 16 levels, which re-stages fewer halo planes).  W > 0
+// sets the warps instead (the batched ensemble's autotuner also tries 16).
 template <int N, int NT, typename R, int W = 0>
 struct P2Cfg {
-  static constexpr int WARPS = W > 0 ? W : (N == 5 ? 16 : 8);
+  static constexpr int WARPS = W > 0 ? W : 8;
   static constexpr int MINB = WARPS >= 16 ? 1 : 2;   // CTAs per SM the registers are sized for
   static constexpr int DoF = N * N;
   static constexpr int LPW = 32 / DoF;           // levels per warp
