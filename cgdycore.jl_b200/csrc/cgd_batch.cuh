@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(P2Cfg<N, NT, R, W>::THREADS, P2Cfg<N, NT, R, W
 }
 
 template <int MODE, bool C32>
-__global__ void __launch_bounds__(32 * COL_WARPS, MODE == 2 ? 3 : 4) kb_column(const WItem *__restrict__ w)
+__global__ void __launch_bounds__(32 * COL_WARPS, 4) kb_column(const WItem *__restrict__ w)
 {
   const WItem it = w[blockIdx.x];
   const BMember &B = c_bm[it.m];

@@ -784,7 +784,7 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
 }
 
 template <int MODE, bool C32>
-__global__ void __launch_bounds__(32 * COL_WARPS, MODE == 2 ? 3 : 4) k_column(const GP P, const ColArgs A)
+__global__ void __launch_bounds__(32 * COL_WARPS, 4) k_column(const GP P, const ColArgs A)
 {
   column_body<MODE, C32>(P, A, blockIdx.x);
 }
