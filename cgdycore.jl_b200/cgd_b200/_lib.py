@@ -26,7 +26,7 @@ BATCH_FUSED = 2
 # every symbol declared in include/cgd_b200.h
 EXPORTS = [
     "cgd_create", "cgd_destroy", "cgd_prepare", "cgd_hypervisc_phase1", "cgd_rhs", "cgd_jac",
-    "cgd_schur_solve", "cgd_ros_step", "cgd_mass_integral", "cgd_jac_schur_solve_noalloc", "cgd_get_stream",
+    "cgd_jac_bands", "cgd_schur_solve", "cgd_schur_solve_bands", "cgd_ros_step", "cgd_mass_integral", "cgd_jac_schur_solve_noalloc", "cgd_get_stream",
     "cgd_kernel_times", "cgd_strerror", "cgd_version",
     "cgd_rhs_adjoint", "cgd_ros_step_adjoint", "cgd_set_caller_stream",
     "cgd_tape_record_step", "cgd_tape_step_adjoint", "cgd_tape_release", "cgd_tape_bytes_per_step",
@@ -89,6 +89,10 @@ def lib(exact=False):
             getattr(L, f).restype = ctypes.c_int
         L.cgd_schur_solve.argtypes = [vp, vp, vp, dbl]
         L.cgd_schur_solve.restype = ctypes.c_int
+        L.cgd_jac_bands.argtypes = [vp] * 6
+        L.cgd_jac_bands.restype = ctypes.c_int
+        L.cgd_schur_solve_bands.argtypes = [vp] * 7 + [dbl]
+        L.cgd_schur_solve_bands.restype = ctypes.c_int
         L.cgd_ros_step.argtypes = [vp, vp, dbl, i32]
         L.cgd_ros_step.restype = ctypes.c_int
         L.cgd_mass_integral.argtypes = [vp, vp, vp, vp]

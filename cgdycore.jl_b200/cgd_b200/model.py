@@ -13,7 +13,9 @@ libcgd_b200.so:
   fcn(U)                      GPU.FcnGPU!(::CompressibleShallow) (FcnGPU.jl:552)
   hypervisc_phase1(U)         first phase of FcnGPU! (FcnGPU.jl:744-802)
   jac(U)                      DyCore.JacSchurGPU! (JacSchur.jl:3)
+  jac_bands(J, U)             JacSchurGPU!(J, U, ...) filling the JCache bands
   schur_solve(v, fac)         Integration.SchurSolveGPU! (SchurSolve.jl:149)
+  schur_solve_bands(k,v,J,f)  SchurSolveGPU!(k, v, J, fac, ...) with J's bands
   rosenbrock_schur(U, dt)     Integration.RosenbrockSchur! (RosenbrockSchur.jl:1)
   time_stepper(U, dt, n)      the Rosenbrock branch of TimeStepper! (TimeStepper.jl:103-124)
   mass_integral(U)            Parallels.GlobalIntegral (Exchange.jl:1163)
@@ -54,6 +56,19 @@ def _ptr(a, shape=None, writable=False):
             raise ValueError("tensor has the wrong number of elements")
         return a.data_ptr()
     raise TypeError("expected a numpy array or a torch tensor")
+
+
+class JacBands(tuple):
+    """The four Jacobian band arrays of the reference's JStruct, in its field
+    order for the solve: JRhoW, JWRho, JWRhoTh, JRhoThW."""
+
+    def __new__(cls, JRhoW, JWRho, JWRhoTh, JRhoThW):
+        return super().__new__(cls, (JRhoW, JWRho, JWRhoTh, JRhoThW))
+
+    JRhoW = property(lambda self: self[0])
+    JWRho = property(lambda self: self[1])
+    JWRhoTh = property(lambda self: self[2])
+    JRhoThW = property(lambda self: self[3])
 
 
 def _copy(a):
@@ -246,6 +261,28 @@ class Dycore:
         b = np.zeros(4 * 2 * (self.nz - 1) * self.NumG)
         _lib.check(self._L.cgd_jac(self.h, _ptr(U, self.shape), b.ctypes.data), "cgd_jac")
         return b.reshape((4, self.NumG, self.nz - 1, 2)).transpose(0, 3, 2, 1)
+
+    def new_bands(self):
+        """The reference's JCache band arrays JRhoW, JWRho, JWRhoTh, JRhoThW,
+        each (2, nz-1, NumG) in column-major order (src/Integration/JacCache.jl:62-70)."""
+        return JacBands(*[np.zeros((2, self.nz - 1, self.NumG), order="F") for _ in range(4)])
+
+    def jac_bands(self, J, U):
+        """Fill the four band arrays of J (JacBands of Fortran-ordered numpy
+        arrays or of contiguous CUDA torch tensors of shape (NumG, nz-1, 2))
+        from U, as JacSchurGPU!(J, U, ...) does."""
+        shp = (2, self.nz - 1, self.NumG)
+        _lib.check(self._L.cgd_jac_bands(self.h, _ptr(U, self.shape), *[_ptr(b, shp, True) for b in J]),
+                   "cgd_jac_bands")
+        return J
+
+    def schur_solve_bands(self, k, v, J, fac):
+        """k = (I/fac - J)^-1 v with the bands of J (SchurSolveGPU!(k, v, J, fac,
+        Cache, Global)); v is updated in place as by the reference."""
+        shp = (2, self.nz - 1, self.NumG)
+        _lib.check(self._L.cgd_schur_solve_bands(self.h, _ptr(k, self.shape, True), _ptr(v, self.shape, True),
+                                                 *[_ptr(b, shp) for b in J], float(fac)), "cgd_schur_solve_bands")
+        return k
 
     def schur_solve(self, v, fac, k=None):
         """k = (I/fac - J)^-1 v with the bands of the last jac(); v is updated

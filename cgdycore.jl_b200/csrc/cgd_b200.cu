@@ -645,6 +645,19 @@ int cgd_rhs(cgd_handle *h, const double *U, double *F)
   return finish(h);
 }
 
+// The four band arrays inside the handle's contiguous (4, 2, nz-1, NumG) buffer.
+static Bands4 handle_bands(cgd_handle *h)
+{
+  const size_t bs = (size_t)2 * (h->nz - 1) * h->NumG;
+  return Bands4{{h->bands, h->bands + bs, h->bands + 2 * bs, h->bands + 3 * bs}};
+}
+
+static void launch_jac(cgd_handle *h, const double *Ud, const Bands4 &out)
+{
+  const long long n = (long long)(h->nz - 1) * h->NumG;
+  k_jac<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->gp, Ud, out);
+}
+
 int cgd_jac(cgd_handle *h, const double *U, double *bands)
 {
   if (!h || !U) return CGD_ERR_INVALID_ARG;
@@ -652,8 +665,7 @@ int cgd_jac(cgd_handle *h, const double *U, double *bands)
   double *Ud;
   int rc = stage_in(h, U, h->Ubuf, true, &Ud);
   if (rc) return rc;
-  long long n = (long long)(h->nz - 1) * h->NumG;
-  k_jac<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->gp, Ud, h->bands);
+  launch_jac(h, Ud, handle_bands(h));
   if (bands) {
     size_t bytes = (size_t)8 * (h->nz - 1) * h->NumG * 8;
     CK(cudaMemcpyAsync(bands, h->bands, bytes, is_device_ptr(bands) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
@@ -664,11 +676,31 @@ int cgd_jac(cgd_handle *h, const double *U, double *bands)
   return rc;
 }
 
-int cgd_schur_solve(cgd_handle *h, double *k, double *v, double fac)
+int cgd_jac_bands(cgd_handle *h, const double *U, double *JRhoW, double *JWRho, double *JWRhoTh, double *JRhoThW)
 {
-  if (!h || !k || !v || !(fac > 0)) return CGD_ERR_INVALID_ARG;
-  if (!h->have_bands) return CGD_ERR_INVALID_ARG;
+  if (!h || !U || !JRhoW || !JWRho || !JWRhoTh || !JRhoThW) return CGD_ERR_INVALID_ARG;
   if (int erc = enter(h)) return erc;
+  double *Ud;
+  int rc = stage_in(h, U, h->Ubuf, true, &Ud);
+  if (rc) return rc;
+  double *user[4] = {JRhoW, JWRho, JWRhoTh, JRhoThW};
+  bool dev[4];
+  for (int i = 0; i < 4; ++i) dev[i] = is_device_ptr(user[i]);
+  // the handle's own bands (for cgd_schur_solve) and the caller's arrays
+  const Bands4 hb = handle_bands(h);
+  launch_jac(h, Ud, hb);
+  const size_t bytes = (size_t)2 * (h->nz - 1) * h->NumG * 8;
+  for (int i = 0; i < 4; ++i)
+    CK(cudaMemcpyAsync(user[i], hb.b[i], bytes, dev[i] ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                       h->stream));
+  rc = finish(h);
+  if (!rc) h->have_bands = true;
+  return rc;
+}
+
+// The column Schur solve (MODE 3) with the given band arrays.
+static int schur_solve_with(cgd_handle *h, double *k, double *v, const Bands4 &b, double fac)
+{
   double *vd, *kd;
   int rc = stage_in(h, v, h->Ubuf, true, &vd);
   if (rc) return rc;
@@ -677,7 +709,7 @@ int cgd_schur_solve(cgd_handle *h, double *k, double *v, double fac)
   ColArgs a{};
   a.v = vd;
   a.kout = kd;
-  a.bands = h->bands;
+  for (int i = 0; i < 4; ++i) a.jb4[i] = b.b[i];
   a.fac = fac;
   a.dt = fac;
   column<3>(h, a);
@@ -685,6 +717,35 @@ int cgd_schur_solve(cgd_handle *h, double *k, double *v, double fac)
   if (!kdev) CK(cudaMemcpyAsync(k, kd, bytes, cudaMemcpyDeviceToHost, h->stream));
   if (vd != v) CK(cudaMemcpyAsync(v, vd, bytes, cudaMemcpyDeviceToHost, h->stream));
   return finish(h);
+}
+
+int cgd_schur_solve(cgd_handle *h, double *k, double *v, double fac)
+{
+  if (!h || !k || !v || !(fac > 0)) return CGD_ERR_INVALID_ARG;
+  if (!h->have_bands) return CGD_ERR_INVALID_ARG;
+  if (int erc = enter(h)) return erc;
+  return schur_solve_with(h, k, v, handle_bands(h), fac);
+}
+
+int cgd_schur_solve_bands(cgd_handle *h, double *k, double *v, const double *JRhoW, const double *JWRho,
+                          const double *JWRhoTh, const double *JRhoThW, double fac)
+{
+  if (!h || !k || !v || !JRhoW || !JWRho || !JWRhoTh || !JRhoThW || !(fac > 0)) return CGD_ERR_INVALID_ARG;
+  if (int erc = enter(h)) return erc;
+  const double *user[4] = {JRhoW, JWRho, JWRhoTh, JRhoThW};
+  Bands4 b = handle_bands(h);
+  const size_t bytes = (size_t)2 * (h->nz - 1) * h->NumG * 8;
+  for (int i = 0; i < 4; ++i) {
+    if (is_device_ptr(user[i])) {
+      b.b[i] = const_cast<double *>(user[i]);   // read only
+    } else {
+      // host bands are staged into the handle's band buffer, which then no
+      // longer holds the last cgd_jac's bands
+      CK(cudaMemcpyAsync(b.b[i], user[i], bytes, cudaMemcpyHostToDevice, h->stream));
+      h->have_bands = false;
+    }
+  }
+  return schur_solve_with(h, k, v, b, fac);
 }
 
 int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps)
@@ -789,17 +850,20 @@ int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const do
   P.nz = cfg->nz; P.NumG = cfg->NumG; P.NumTr = cfg->NumTr; P.NV = 5 + cfg->NumTr; P.NC = P.NV + 1;
   P.dz = dz; P.Grav = cfg->Grav; P.Rd = cfg->Rd; P.p0 = cfg->p0; P.kappa = cfg->Rd / cfg->Cpd;
   const long long n = (long long)(P.nz - 1) * P.NumG;
-  k_jac<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, U, bands);
+  const size_t bs = (size_t)2 * (P.nz - 1) * P.NumG;
+  const Bands4 b4{{bands, bands + bs, bands + 2 * bs, bands + 3 * bs}};
+  k_jac<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, U, b4);
   ColArgs a{};
   a.v = v;
   a.kout = k;
-  a.bands = bands;
+  for (int i = 0; i < 4; ++i) a.jb4[i] = b4.b[i];
   a.fac = fac;
   a.dt = fac;
   const size_t smem = (size_t)COL_WARPS * COL_ARR * P.nz * sizeof(double);
   k_column<3, false><<<(P.NumG + COL_WARPS - 1) / COL_WARPS, 32 * COL_WARPS, smem, st>>>(P, a);
+  // launch errors only: the work stays ordered on the caller's stream, which
+  // the caller synchronises (or orders further work on) itself
   CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(st));
   return CGD_OK;
 }
 
@@ -1551,9 +1615,18 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
       }
     }
     for (int m = 0; m < nm; ++m) copies[m] = static_cast<double *>(b->scratch[m]);
-    cudaEvent_t e0, e1;
-    BCK(cudaEventCreate(&e0));
-    BCK(cudaEventCreate(&e1));
+    // the timing events are destroyed on every way out of this block
+    struct EventPair {
+      cudaEvent_t a = nullptr, b = nullptr;
+      ~EventPair()
+      {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+      }
+    } ev;
+    BCK(cudaEventCreate(&ev.a));
+    BCK(cudaEventCreate(&ev.b));
+    cudaEvent_t e0 = ev.a, e1 = ev.b;
     for (int c = 0; c < cgd_batch::NCAND; ++c) {
       if (!b->use[c]) continue;
       for (int m = 0; m < nm; ++m) {
@@ -1577,8 +1650,6 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
         return CGD_ERR_TIMEOUT;
       }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     b->chosen = 0;
     for (int c = 1; c < cgd_batch::NCAND; ++c)
       if (b->use[c] && b->tune_ms[c] < b->tune_ms[b->chosen]) b->chosen = c;

@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(32 * COL_WARPS, 4) kb_column(const WItem *__re
   a.k2 = B.k2;
   a.jbg = B.jbg;
   a.v = nullptr;
-  a.bands = nullptr;
+  a.jb4[0] = a.jb4[1] = a.jb4[2] = a.jb4[3] = nullptr;
   a.dt = B.dt;
   a.fac = B.dt * c_brk.gamma;
   a.rk = c_brk;
@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(256, 2) kb_stage(const FusedArgs A, const int 
     a.k2 = B.k2;
     a.jbg = B.jbg;
     a.v = nullptr;
-    a.bands = nullptr;
+    a.jb4[0] = a.jb4[1] = a.jb4[2] = a.jb4[3] = nullptr;
     a.dt = B.dt;
     a.fac = B.dt * c_brk.gamma;
     a.rk = c_brk;

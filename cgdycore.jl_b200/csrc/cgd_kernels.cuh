@@ -422,7 +422,9 @@ struct ColArgs {
   double *kout;          // MODE 0,1,3
   double *Vout;          // MODE 0,1 (stage state), 2 (new state)
   double *v;             // MODE 3: right-hand side (overwritten)
-  const double *bands;   // MODE 3: (2, nz-1, NumG) x 4, the reference layout
+  // MODE 3: the four Jacobian bands JRhoW, JWRho, JWRhoTh, JRhoThW, each
+  // (2, nz-1, NumG) in the reference layout (the JCache arrays)
+  const double *jb4[4];
   double *jbg;           // MODE 0 writes, 1-2 read: [8][NumG][nz-1] bands of the step
   double dt, fac;
   RK rk;
@@ -639,9 +641,8 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
       for (int f = 1; f < NV; ++f)
         if (f != 3 && f != 4) A.kout[o0 + f * fs] = fac * A.v[o0 + f * fs];
       if (l < n) {
-        const size_t bs = (size_t)2 * n * NumG;
         for (int arr = 0; arr < 4; ++arr)
-          for (int r = 0; r < 2; ++r) jb[(2 * arr + r) * LS + l] = A.bands[arr * bs + r + 2 * (l + (size_t)n * g)];
+          for (int r = 0; r < 2; ++r) jb[(2 * arr + r) * LS + l] = A.jb4[arr][r + 2 * (l + (size_t)n * g)];
       }
     }
   }
@@ -823,8 +824,14 @@ __global__ void __launch_bounds__(256) k_refprof(const GP P, const double *__res
   }
 }
 
+// The four band arrays of the reference's JCache (JRhoW, JWRho, JWRhoTh,
+// JRhoThW), each (2, nz-1, NumG).
+struct Bands4 {
+  double *b[4];
+};
+
 // Jacobian bands into memory (cgd_jac): one thread per (interface, column)
-__global__ void k_jac(const GP P, const double *__restrict__ U, double *__restrict__ bands)
+__global__ void k_jac(const GP P, const double *__restrict__ U, const Bands4 out)
 {
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int n = P.nz - 1;
@@ -836,9 +843,8 @@ __global__ void k_jac(const GP P, const double *__restrict__ U, double *__restri
   double b[8];
   jac_at(P, V0[l], V0[l + 1], V0[l + 4 * fs], V0[l + 1 + 4 * fs], P.dz[l + (size_t)nz * g],
          P.dz[l + 1 + (size_t)nz * g], b);
-  const size_t bs = (size_t)2 * n * P.NumG;
   for (int arr = 0; arr < 4; ++arr)
-    for (int r = 0; r < 2; ++r) bands[arr * bs + r + 2 * (l + (size_t)n * g)] = b[arr * 2 + r];
+    for (int r = 0; r < 2; ++r) out.b[arr][r + 2 * (l + (size_t)n * g)] = b[arr * 2 + r];
 }
 
 __device__ __forceinline__ void pressure_body(const GP &P, const double *__restrict__ U, double *__restrict__ p,

@@ -45,8 +45,12 @@ check(rc, what) = rc == 0 || error("$what: " * unsafe_string(ccall((:cgd_strerro
 
 hostcopy(a) = Array{eltype(a)}(a)
 
-# One handle per (CG, Metric) pair; created on first use.
-const HANDLES = IdDict{Any,Handle}()
+# One handle per (Global, precision): Global is the reference's per-model
+# struct that every injected function receives (SchurSolveGPU! gets no CG or
+# Metric), so the handle created from (CG, Metric, Phys, Global) on first use
+# is found again from Global alone.  A mixed-form handle and an FP64 handle of
+# the same model are different handles.
+const HANDLES = IdDict{Any,Dict{Bool,Handle}}()
 
 function config(CG, Global, Phys; mixed = false, check_finite = false)
   CgdConfig(CG.OrdPoly, Global.Grid.nz, Global.Model.NumTr, Global.Grid.NumFaces, CG.NumG,
@@ -58,7 +62,10 @@ end
 # mixed = true selects the mixed form (FP32 horizontal derivative sums and DSS
 # around an FP64 per-level reference; FP64 column solve).
 function handle(CG, Metric, Phys, Global; mixed = false)
-  get!(HANDLES, Metric) do
+  byprec = get!(HANDLES, Global) do
+    Dict{Bool,Handle}()
+  end
+  get!(byprec, mixed) do
     cfg = Ref(config(CG, Global, Phys; mixed = mixed))
     glob = Int64.(hostcopy(CG.Glob))
     DS, DW = hostcopy(CG.DS), hostcopy(CG.DW)
@@ -74,6 +81,15 @@ function handle(CG, Metric, Phys, Global; mixed = false)
     finalizer(x -> ccall((:cgd_destroy, libcgd), Cvoid, (Ptr{Cvoid},), x.ptr), h)
     h
   end
+end
+
+# The handle of a model whose handle exists already (the injected functions
+# that receive no CG or Metric).
+function handle(Global; mixed = false)
+  byprec = get(HANDLES, Global, nothing)
+  (byprec === nothing || !haskey(byprec, mixed)) &&
+    error("CGDB200: no handle for this Global; call FcnB200!, FcnPrepareB200! or JacB200! first")
+  byprec[mixed]
 end
 
 # Pointer of a host Array or a CuArray (CUDA.jl converts CuArray to CuPtr;
@@ -102,24 +118,36 @@ function FcnB200!(F, U, CG, Metric, Phys, Cache, Exchange, Global, Param, DiscTy
   end
 end
 
-# Jac!(JCache, U, CG, Metric, Phys, Cache, Global, Param, DiscType): bands stay
-# in the handle for SchurSolveB200!.
+# Jac!(JCache, U, CG, Metric, Phys, Cache, Global, Param, DiscType) =
+# DyCore.JacSchurGPU! (src/DyCore/JacSchur.jl:3-27): fills the four band
+# arrays of the JStruct (src/Integration/JacCache.jl:62-66), each
+# (2, nz-1, NumG), so the reference's own SchurSolveGPU! or SchurSolveB200!
+# can read them.  JCache.CompTri is set as the reference's RosenbrockSchur!
+# expects (the library forms the tridiagonal matrix from the bands itself).
 function JacB200!(JCache, U, CG, Metric, Phys, Cache, Global, Param, DiscType)
   h = handle(CG, Metric, Phys, Global)
-  GC.@preserve U begin
-    check(ccall((:cgd_jac, libcgd), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}),
-                h.ptr, dptr(U), C_NULL), "cgd_jac")
+  GC.@preserve U JCache begin
+    check(ccall((:cgd_jac_bands, libcgd), Cint,
+                (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                h.ptr, dptr(U), dptr(JCache.JRhoW), dptr(JCache.JWRho), dptr(JCache.JWRhoTh),
+                dptr(JCache.JRhoThW)), "cgd_jac_bands")
   end
+  JCache.CompTri = true
 end
 
-# SchurSolveGPU!(k, v, JCache, fac, Cache, Global) with the handle of the
-# last JacB200! call.
-function SchurSolveB200!(k, v, CG, Metric, Phys, Global, fac)
-  h = handle(CG, Metric, Phys, Global)
-  GC.@preserve k v begin
-    check(ccall((:cgd_schur_solve, libcgd), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Cdouble),
-                h.ptr, dptr(k), dptr(v), fac), "cgd_schur_solve")
+# SchurSolve!(k, v, J, fac, Cache, Global) = Integration.SchurSolveGPU!
+# (src/Integration/SchurSolve.jl:149-177) with the reference's signature: the
+# bands come from J (filled by JacB200! or by the reference's JacSchurGPU!).
+function SchurSolveB200!(k, v, J, fac, Cache, Global)
+  h = handle(Global)
+  GC.@preserve k v J begin
+    check(ccall((:cgd_schur_solve_bands, libcgd), Cint,
+                (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+                 Ptr{Float64}, Cdouble),
+                h.ptr, dptr(k), dptr(v), dptr(J.JRhoW), dptr(J.JWRho), dptr(J.JWRhoTh), dptr(J.JRhoThW),
+                fac), "cgd_schur_solve_bands")
   end
+  J.CompTri = false
 end
 
 # RosenbrockSchur!(V, dt, Fcn!, FcnPrepare!, Jac, CG, Metric, Phys, Cache,
@@ -134,8 +162,11 @@ function RosenbrockSchurB200!(V, dt, Fcn!, FcnPrepare!, Jac, CG, Metric, Phys, C
   end
 end
 
-# Allocation-free Jacobian + Schur solve (no counterpart in the reference):
-# bands in a static 32 MiB device array; 8*(nz-1)*NumG <= 4_194_304.
+# Allocation-free Jacobian + Schur solve (no counterpart in the reference),
+# for a caller whose device memory belongs to CUDA.jl's pool allocator:
+# bands in a static 32 MiB device array per library file;
+# 8*(nz-1)*NumG <= 4_194_304.  The work is enqueued on `stream` and not
+# waited for: synchronise that stream before reading k or v.
 function JacSchurSolveNoAlloc!(k, v, U, dz, CG, Global, Phys, fac; stream = C_NULL)
   cfg = Ref(config(CG, Global, Phys))
   GC.@preserve k v U dz begin

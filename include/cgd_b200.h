@@ -109,10 +109,29 @@ int cgd_rhs_adjoint(cgd_handle *h, const double *U, const double *LF, double *LU
  * Replaces DyCore.JacSchurGPU! (src/DyCore/JacSchur.jl:3-75). */
 int cgd_jac(cgd_handle *h, const double *U, double *bands);
 
-/* Column Schur solve with the bands of the last cgd_jac: k from v (v is
- * overwritten as in the reference), fac = dt*gamma.
- * Replaces Integration.SchurSolveGPU! (src/Integration/SchurSolve.jl:149-177). */
+/* The same bands written into the four caller-owned arrays of the
+ * reference's JCache (src/Integration/JacCache.jl:1-20,62-70), each
+ * (2, nz-1, NumG), device or host memory; the handle keeps a copy too.
+ * Replaces JacSchurGPU!(J, U, ...) (src/DyCore/JacSchur.jl:3-27), which
+ * fills J.JRhoW, J.JWRho, J.JWRhoTh and J.JRhoThW. */
+int cgd_jac_bands(cgd_handle *h, const double *U, double *JRhoW, double *JWRho, double *JWRhoTh,
+                  double *JRhoThW);
+
+/* Column Schur solve with the bands of the last cgd_jac/cgd_jac_bands: k
+ * from v (v is overwritten as in the reference), fac = dt*gamma.
+ * Replaces Integration.SchurSolveGPU! (src/Integration/SchurSolve.jl:149-177)
+ * when the bands stay inside the library. */
 int cgd_schur_solve(cgd_handle *h, double *k, double *v, double fac);
+
+/* Column Schur solve with the bands passed explicitly, as the reference's
+ * SchurSolveGPU!(k, v, J, fac, Cache, Global) reads them from J
+ * (src/Integration/SchurSolve.jl:149-177): JRhoW, JWRho, JWRhoTh, JRhoThW
+ * each (2, nz-1, NumG), device memory (read in place) or host memory
+ * (staged through the handle's band buffer, which then no longer holds the
+ * bands of the last cgd_jac).  The tridiagonal matrix (J.tri) is formed
+ * from the bands on every call.  k from v, v overwritten, fac = dt*gamma. */
+int cgd_schur_solve_bands(cgd_handle *h, double *k, double *v, const double *JRhoW, const double *JWRho,
+                          const double *JWRhoTh, const double *JRhoThW, double fac);
 
 /* nsteps SSP-Knoth Rosenbrock-W steps of size dt, in place.  One step is a
  * captured CUDA graph (3 stages x {hyperviscosity+DSS, tendency+DSS,
@@ -154,25 +173,33 @@ int64_t cgd_tape_bytes_per_step(const cgd_handle *h);
  * Replaces Parallels.GlobalIntegral (src/Parallels/Exchange.jl:1163-1166). */
 int cgd_mass_integral(cgd_handle *h, const double *U, const double *MMass, double *out);
 
-/* Allocation-free Jacobian + column Schur solve, for callers that cannot let
- * a library call cudaMalloc/cudaFree: code running inside its own stream
- * capture or a host runtime whose device memory is owned by a pool
- * allocator (CUDA.jl, PyTorch), where an allocation would synchronise the
- * device or is not allowed.  No counterpart in the reference (its solve
- * always uses the JCache arrays allocated with the model).
+/* Allocation-free Jacobian + column Schur solve.  Some callers cannot let a
+ * library allocate device memory: a host runtime whose device memory belongs
+ * to its own pool allocator (CUDA.jl, PyTorch), where a cudaMalloc or
+ * cudaFree behind the pool's back synchronises the device, fragments it or
+ * is forbidden by the embedding application.  This entry point allocates
+ * nothing.  No counterpart in the reference (its solve always uses the
+ * JCache arrays allocated with the model).
  * Computes the vertical acoustic Jacobian bands of U and solves k from v
  * (v is updated as by cgd_schur_solve), with fac = dt*gamma.  Uses only
  * cfg->nz, NumG, NumTr, Grav, Rd, Cpd, p0.  U, dz, k, v must be device
- * memory; the call enqueues on `stream` (a cudaStream_t, NULL = default
- * stream) and waits for it.
+ * memory.  The work is enqueued on `stream` (a cudaStream_t, NULL = the
+ * legacy default stream) and the call returns without waiting for it: the
+ * caller synchronises that stream, or orders later work after it, before
+ * reading k or v.  Launch errors are returned; errors of the running
+ * kernels surface at the caller's next synchronisation.
  * Scratch: the bands live in one file-scope device array of
- * CGD_NOALLOC_SCRATCH_DOUBLES doubles (32 MiB, held by every GPU that loads
- * the library until the process exits); 8*(nz-1)*NumG must not exceed it,
- * otherwise CGD_ERR_SHAPE.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress), so make that first call before any
- * stream capture.  Every call overwrites the whole band region it uses, so
- * nothing needs clearing between calls; calls that overlap on the GPU share
- * the array and race. */
+ * CGD_NOALLOC_SCRATCH_DOUBLES doubles (32 MiB).  Each library file
+ * (libcgd_b200.so and libcgd_b200_exact.so) holds its own array on every
+ * GPU where that file is used, until the process exits.  8*(nz-1)*NumG must
+ * not exceed it, otherwise CGD_ERR_SHAPE.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress, with that device
+ * current) and keeps it for the life of the process, so make that first
+ * call before any stream capture, and do not reset the device
+ * (cudaDeviceReset) between calls.  Every call overwrites the whole band
+ * region it uses, so nothing needs clearing between calls; calls through
+ * the same library file whose work overlaps on one GPU share the array and
+ * race, so order them on one stream. */
 #define CGD_NOALLOC_SCRATCH_DOUBLES (4u * 1024u * 1024u)
 int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const double *dz,
                                 double *k, double *v, double fac, void *stream);

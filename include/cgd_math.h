@@ -19,7 +19,7 @@
  *        s = (m-1)/(m+1), atanh by its Taylor series in s^2 to degree 23;
  *        e*ln2 added in head/tail form.
  *   pow: exp(y*log(x)) (only used for x in (0, 2], |y| < 2 on this path).
- * Accuracy is checked against the C library in tests/test_math.py (<= 2 ulp).
+ * Accuracy is checked against the C library in tests/test_abi_and_math.py (<= 2 ulp).
  *
  * All arithmetic must be compiled without floating-point contraction
  * (host: -ffp-contract=off; device: -fmad=false) for the bit-exactness claim.

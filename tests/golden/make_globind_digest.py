@@ -7,6 +7,9 @@ SHA-256, shape, extrema and a few full columns, so the tests can pin the grid
 chain bit-exactly without the 691 KB file (and without the reference tree).
 
     python tests/golden/make_globind_digest.py [path/to/CGDycore.jl]
+
+The checkout is the argument, else the CGD_REFERENCE_DIR environment
+variable.
 """
 import hashlib
 import json
@@ -15,7 +18,9 @@ import sys
 
 import numpy as np
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CGD_REFERENCE_DIR", "")
+if not ref:
+    sys.exit("usage: make_globind_digest.py path/to/CGDycore.jl (or set CGD_REFERENCE_DIR)")
 raw = open(os.path.join(ref, "TestKernels", "GlobInd"), "rb").read()
 g = np.frombuffer(raw, dtype="<i8").reshape((16, 5400), order="F")
 cols = [0, 1, 29, 30, 899, 900, 1799, 2700, 3599, 4500, 5399]

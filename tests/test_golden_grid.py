@@ -10,7 +10,10 @@ import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = json.load(open(os.path.join(HERE, "golden", "globind_n30_p3.json")))
-REF_FILE = "/root/reference/TestKernels/GlobInd"
+# the reference checkout, when present (CGD_REFERENCE_DIR); the digest above
+# stands in for it everywhere else
+REF_DIR = os.environ.get("CGD_REFERENCE_DIR", "")
+REF_FILE = os.path.join(REF_DIR, "TestKernels", "GlobInd") if REF_DIR else ""
 
 
 def _check_against_digest(glob):

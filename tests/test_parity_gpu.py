@@ -105,6 +105,39 @@ def test_jacobian_and_schur(case):
         assert np.array_equal(bg, bo)
 
 
+def test_jcache_bands_and_explicit_solve(case):
+    """Per-function injection as the reference's RosenbrockSchur! does it:
+    JacSchurGPU!(J, U, ...) fills the caller's four JCache band arrays
+    (cgd_jac_bands), then SchurSolveGPU!(k, v, J, fac, ...) reads them
+    (cgd_schur_solve_bands), on host arrays and on device tensors.  The
+    bands match the oracle's Jacobian and the solve its Schur solve."""
+    import torch
+    name, o, g, U, nu, d = case
+    bo = o.jac(U)                       # (4, 2, nz-1, NumG)
+    J = d.jac_bands(d.new_bands(), U)
+    for i in range(4):
+        assert np.abs(J[i] - bo[i]).max() <= 1e-14 * np.abs(bo).max()
+        if d.exact:
+            assert np.array_equal(J[i], bo[i])
+    rng = np.random.default_rng(12)
+    v = np.asfortranarray(rng.standard_normal(U.shape))
+    ko, vo = o.schur(v, 120.0)
+    d.jac(U * 1.01)                     # the handle's own bands now differ
+    vg = v.copy(order="F")
+    kg = d.schur_solve_bands(d.new_state(), vg, J, 120.0)
+    _same(kg, ko, d.exact, TOL_RHS)
+    _same(vg, vo, d.exact, TOL_RHS)
+    # device arrays: bands and state as CUDA tensors, read in place
+    Jt = [torch.from_numpy(np.ascontiguousarray(b.transpose(2, 1, 0))).cuda() for b in J]
+    vt = torch.from_numpy(np.ascontiguousarray(v.transpose(2, 1, 0))).cuda()
+    kt = torch.empty_like(vt)
+    torch.cuda.synchronize()
+    from cgd_b200.model import JacBands
+    d.schur_solve_bands(kt, vt, JacBands(*Jt), 120.0)
+    assert np.array_equal(kt.cpu().numpy().transpose(2, 1, 0), kg)
+    assert np.array_equal(vt.cpu().numpy().transpose(2, 1, 0), vg)
+
+
 def test_ten_steps(case):
     name, o, g, U, nu, d = case
     dt = 600.0 if name == "small" else 300.0

@@ -1,8 +1,12 @@
 """The allocation-free Jacobian + Schur solve (cgd_jac_schur_solve_noalloc),
-called through the C ABI on device buffers, against the handle-based
-cgd_jac + cgd_schur_solve on the same inputs, two calls in a row (the second
-reuses the static band scratch the first one filled).  Collected last so it
-also runs after every other GPU test in the same process."""
+for callers whose device memory belongs to their own pool allocator and who
+cannot let the library call cudaMalloc.  It is called through the C ABI on
+device buffers and checked against the handle-based cgd_jac +
+cgd_schur_solve on the same inputs, two calls in a row (the second reuses
+the static band scratch the first one filled).  The call only enqueues on
+the given stream, so the test synchronises before it reads the results.
+Collected last so it also runs after every other GPU test in the same
+process."""
 import ctypes
 
 import numpy as np
@@ -56,6 +60,7 @@ def test_noalloc_matches_handle_solve_twice(oracle_mod, built_lib, cuda_ok, exac
         rc = L.cgd_jac_schur_solve_noalloc(ctypes.byref(cfg), U_t.data_ptr(), dz_t.data_ptr(), k_t.data_ptr(),
                                            v_t.data_ptr(), fac, None)
         assert rc == 0, (rc, L.cgd_strerror(rc))
+        torch.cuda.synchronize()
         k_g, v_g = _host(k_t), _host(v_t)
         assert rel_err_per_field(k_g, k_ref).max() <= 1e-12
         assert rel_err_per_field(v_g, v_ref).max() <= 1e-12
