@@ -48,10 +48,18 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision sub-measurement")
     ap.add_argument("--mixed-days", type=float, default=1.0, help="simulated days of the mixed accuracy run")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint sub-measurement")
+    ap.add_argument("--no-mixed-cfg3", action="store_true",
+                    help="skip the mixed form at its own configuration (nPanel 60, nz 64, 1 simulated day)")
+    ap.add_argument("--cfg3-days", type=float, default=1.0, help="simulated days of the nPanel-60 accuracy run")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble sub-measurement")
+    ap.add_argument("--ensemble-steps", type=int, default=10, help="timed ensemble steps per precision")
     ap.add_argument("--adjoint-steps", "--adjoint-window", dest="adjoint_steps", type=int, default=120,
                     help="steps of the adjoint sensitivity study (120 x 120 s = 4 h)")
     ap.add_argument("--adjoint-fd", action="store_true",
                     help="add central-difference checks of the sensitivity gradient (about a minute)")
+    ap.add_argument("--parallel", default="member", choices=["member", "shard"],
+                    help="N > 1: one ensemble member per GPU (weak scaling) or one grid decomposed over the "
+                         "GPUs with halo exchanges of the DSS (strong scaling)")
     return ap.parse_args()
 
 
@@ -312,6 +320,101 @@ def run_mixed(args, cfg, rank, ranks, U0, fp64_value, torch):
                     "profile; FP64 vertical terms, column Jacobian/Schur solve and reductions"}
 
 
+def run_mixed_cfg3(args, rank, ranks, torch):
+    """The mixed form at its own configuration (physics.CONFIGS['mixed']:
+    nPanel 60, p 4, nz 64 quadratic, no tracers): device-resident steps/s of
+    both precisions (timed like the headline) and, over args.cfg3_days
+    simulated days from the same initial state, the lowest-layer pressure
+    (surface-pressure proxy) of the mixed form against the FP64 path of the
+    same configuration, and the mass drift of both."""
+    from cgd_b200 import setup
+    from cgd_b200 import physics as Ph
+    cfg = member_config(Ph.CONFIGS["mixed"], rank)
+    nsteps = max(1, int(round(args.cfg3_days * 86400.0 / cfg.dt)))
+    K = max(3, min(args.steps, 20))
+    out = {}
+    for prec in ("fp64", "mixed"):
+        d, U0, _ = setup(cfg, precision=prec, check_finite=True)
+        stream = torch.cuda.ExternalStream(d.stream())
+        V = torch.from_numpy(np.ascontiguousarray(U0.transpose(2, 1, 0))).cuda()
+        m0 = d.mass_integral(V)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        W = min(3, nsteps)
+        d.time_stepper(V, cfg.dt, W)
+        ranks.barrier()
+        e0.record(stream)
+        d.time_stepper(V, cfg.dt, min(K, nsteps - W))
+        e1.record(stream)
+        e1.synchronize()
+        t = ranks.max(e0.elapsed_time(e1) / 1e3)
+        d.time_stepper(V, cfg.dt, max(0, nsteps - W - K))
+        torch.cuda.synchronize()
+        out[prec] = {"steps_per_s": ranks.world * min(K, nsteps - W) / t, "p1": np.asarray(d.fcn_prepare(V))[0].copy(),
+                     "drift": (d.mass_integral(V) - m0) / m0, "finite": bool(torch.isfinite(V).all().item())}
+        d.close()
+        del V
+        torch.cuda.empty_cache()
+    p64, pm = out["fp64"]["p1"], out["mixed"]["p1"]
+    return {"config": {"workload": "mixed: cubed sphere nPanel 60 (21600 elements), OrdPoly 4, nz 64 quadratic, "
+                                   f"NumTr 0, dt {cfg.dt:g} s", "nPanel": cfg.nPanel, "nz": cfg.nz, "dt": cfg.dt,
+                       "dt_note": "dt 150 s is beyond the explicit horizontal-acoustics limit of this W-method at "
+                                  "nPanel 60 (it halves the grid spacing of nPanel 30, where 150 s already fails); "
+                                  "60 s keeps the drop-in grid's Courant number"},
+            "fp64_steps_per_s": out["fp64"]["steps_per_s"], "mixed_steps_per_s": out["mixed"]["steps_per_s"],
+            "speedup_vs_fp64": out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"],
+            "accuracy": {"simulated_days": nsteps * cfg.dt / 86400.0, "steps": nsteps,
+                         "p1_rel_l2": float(np.sqrt(np.sum((pm - p64) ** 2) / np.sum(p64 ** 2))),
+                         "p1_rel_linf": float(np.abs(pm - p64).max() / np.abs(p64).max()),
+                         "mass_drift_mixed": float(out["mixed"]["drift"]), "mass_drift_fp64": float(out["fp64"]["drift"]),
+                         "finite": out["fp64"]["finite"] and out["mixed"]["finite"],
+                         "p1": "pressure of the lowest layer (surface-pressure proxy), mixed against the FP64 path "
+                               "of the same configuration"}}
+
+
+def adjoint_fd_entries(d, U, dt, nsteps, rng, per_field=8, rels=(1e-5, 1e-6, 1e-7, 1e-8), tol=1e-6):
+    """Entry-wise check of the gradient of L(U0) = <lam, U_n> (U_n after
+    nsteps steps, lam seeded Gaussian) through the step adjoints
+    (steps_adjoint) against central differences: per field, per_field
+    entries at levels spread over the column; each entry's error is the
+    best of the step sizes rels (of the field's scale).  The forward is
+    deterministic, so entries away from the perturbed one cancel exactly in
+    the difference."""
+    import torch
+    lam = torch.from_numpy(rng.standard_normal(tuple(U.shape))).to(U.device)
+    G = d.steps_adjoint(U, lam, dt, nsteps, every=1)
+    NV, NumG, nz = U.shape
+    work = U.clone()
+    rows = []
+    for f in range(NV):
+        scale = max(float(U[f].abs().max()), 1.0)
+        med = float(G[f].abs().median())
+        for i in range(per_field):
+            l, g = int((i * nz) // per_field), int(rng.integers(NumG))
+            a = float(G[f, g, l])
+            fds = []
+            for rel in rels:
+                h = rel * scale
+                work.copy_(U)
+                work[f, g, l] += h
+                d.time_stepper(work, dt, nsteps)
+                jp = float(torch.sum(lam * work))
+                work.copy_(U)
+                work[f, g, l] -= h
+                d.time_stepper(work, dt, nsteps)
+                jm = float(torch.sum(lam * work))
+                fds.append((jp - jm) / (2 * h))
+            den = max(abs(a), med, 1e-300)
+            rows.append({"field": f, "level": l, "err": min(abs(x - a) for x in fds) / den,
+                         "spread": (max(fds) - min(fds)) / den})
+    errs = np.array([r["err"] for r in rows])
+    return {"entries": len(rows), "steps": nsteps, "rel_steps": list(rels), "tol": tol,
+            "pass_fraction": float(np.mean(errs <= tol)), "pass_fraction_1e-5": float(np.mean(errs <= 1e-5)),
+            "err_median": float(np.median(errs)), "err_max": float(errs.max()),
+            "functional": "L = <lam, U_n>, lam ~ N(0,1) seeded; error = min over step sizes |FD - adjoint| / "
+                          "max(|adjoint|, median |gradient| of the field)"}
+
+
 def run_adjoint(args, rank, ranks, torch):
     """The hand-written adjoint on the drop-in grid without tracers
     (physics.CONFIGS['adjoint']), device-resident, timed with CUDA events on
@@ -398,6 +501,8 @@ def run_adjoint(args, rank, ranks, torch):
            "step_adjoint": "forward replay of the step keeping stage states, phase-1 caches, pressures and k; "
                            "reverse: transposed column Schur solve with band derivatives, tendency adjoint "
                            "(phase 2 and phase 1 with their transposed DSS), stage combinations"}
+    # entry-wise central differences of a 4-step gradient on the drop-in grid
+    res["fd_entries"] = adjoint_fd_entries(d, U, dt, 4, np.random.default_rng(20261205 + rank))
     if args.adjoint_fd:
         # central differences along seeded unit directions of the FP64 state space
         rng = np.random.default_rng(study["fd_seed"])
@@ -421,27 +526,20 @@ def run_adjoint(args, rank, ranks, torch):
     return res
 
 
-def run_ensemble(args, rank, world, local):
-    """Batched-ensemble workload (physics.ENSEMBLE): every rank advances its
-    own 48-member ensemble, one CUDA graph per ensemble step.  Times K steps
-    in FP64 and in the mixed form (aggregate DOF-updates/s) and reports each
-    member's lowest-level pressure difference, mixed against FP64, after the
-    full run (6 simulated hours)."""
-    import torch
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+def ensemble_measure(K, warmup, rank, ranks, torch):
+    """The batched ensemble (physics.ENSEMBLE: 48 members, 16 each on
+    (nPanel, nz) = (16, 30), (24, 45), (32, 64)), one CUDA graph per
+    ensemble step, in FP64 and in the mixed form: K timed steps after warmup
+    steps (the first call also runs the autotuner), then the rest of the 6
+    simulated hours, and each member's lowest-level pressure, mixed against
+    FP64, at the end."""
     from cgd_b200 import Dycore, Ensemble
     from cgd_b200 import physics as Ph
     from cgd_b200.model import _grid_and_state
     E = Ph.ENSEMBLE
-    ranks = Ranks(rank, world, torch.device("cuda", local))
     phys = Ph.PhysParameters()
     nsteps = int(round(E["hours"] * 3600.0 / E["dt"]))
-    K = min(args.steps, nsteps - args.warmup)
+    K = max(1, min(K, nsteps - warmup))
     members = []   # (grid, nu, U0)
     for n, nz in E["grids"]:
         rc = Ph.RunConfig(f"ens{n}_{nz}", n, E["OrdPoly"], nz, 0, E["dt"], nsteps, "quadratic")
@@ -459,7 +557,7 @@ def run_ensemble(args, rank, world, local):
         states = [torch.from_numpy(np.ascontiguousarray(U.transpose(2, 1, 0))).cuda() for _, _, U in members]
         dts = [E["dt"]] * len(members)
         m0 = [d.mass_integral(u) for d, u in zip(dycs, states)]
-        ens.step(states, dts, args.warmup)      # the first call also runs the autotuner
+        ens.step(states, dts, warmup)      # the first call also runs the autotuner
         ranks.barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -468,7 +566,7 @@ def run_ensemble(args, rank, world, local):
         e1.record(stream)
         e1.synchronize()
         t = ranks.max(e0.elapsed_time(e1) / 1e3)
-        ens.step(states, dts, nsteps - args.warmup - K)
+        ens.step(states, dts, nsteps - warmup - K)
         torch.cuda.synchronize()
         p1 = [np.asarray(d.fcn_prepare(u))[0].copy() for d, u in zip(dycs, states)]
         drift = [(d.mass_integral(u) - a) / a for d, u, a in zip(dycs, states, m0)]
@@ -479,32 +577,52 @@ def run_ensemble(args, rank, world, local):
             d.close()
         del states
         torch.cuda.empty_cache()
-    v64 = aggregate(world, K, res["fp64"]["t"]) * dof
-    vm = aggregate(world, K, res["mixed"]["t"]) * dof
+    v64 = aggregate(ranks.world, K, res["fp64"]["t"]) * dof
+    vm = aggregate(ranks.world, K, res["mixed"]["t"]) * dof
     errs = [float(np.sqrt(np.sum((b - a) ** 2) / np.sum(a ** 2))) for a, b in zip(res["fp64"]["p1"], res["mixed"]["p1"])]
-    if rank == 0:
-        line = {
-            "metric": "ensemble DOF-updates/s (48 members, p4: 16 x (nPanel 16, nz 30), (24, 45), (32, 64))",
-            "value": v64, "unit": "DOF-updates/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
-            "ms_per_step": res["fp64"]["t"] / K * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (baroclinic wave + seeded member perturbations)",
-            "config": {"workload": "batched ensemble: 48 members on 3 grids, one CUDA graph per ensemble step "
-                                   "(15 launches split, or 3 fused persistent stage launches; the autotuner picks "
-                                   "the work-list order, the form and the levels per phase-2 CTA)", "grids": E["grids"], "per_grid": E["per_grid"],
-                       "dt": E["dt"], "hours": E["hours"], "steps_total": nsteps,
-                       "perturbation": f"theta +-{E['theta_amp']} K, u,v +-{E['wind_amp']} m/s, seed "
-                                       f"{E['seed0']}+member",
-                       "dt_note": "one dt below the explicit-acoustics limit of the finest member grid",
-                       "parallelism": "one ensemble per GPU"},
-            "dof_per_ensemble_step": dof,
-            "tuning_fp64": res["fp64"]["tuning"],
-            "mixed": {"value": vm, "unit": "DOF-updates/s", "speedup_vs_fp64": vm / v64,
+    return {"dof_updates_per_s": v64, "unit": "DOF-updates/s", "steps": K, "warmup": warmup,
+            "ms_per_step": res["fp64"]["t"] / K * 1e3, "dof_per_ensemble_step": dof,
+            "members": len(members), "grids": E["grids"], "per_grid": E["per_grid"], "dt": E["dt"],
+            "hours": E["hours"], "steps_total": nsteps, "tuning_fp64": res["fp64"]["tuning"],
+            "chosen_form_fp64": "fused" if "stage=fused" in res["fp64"]["tuning"] else "split",
+            "mixed": {"dof_updates_per_s": vm, "speedup_vs_fp64": vm / v64,
                       "ms_per_step": res["mixed"]["t"] / K * 1e3, "tuning": res["mixed"]["tuning"],
                       "p1_rel_l2_vs_fp64": {"max": max(errs), "median": float(np.median(errs))},
                       "mass_drift_max": float(max(abs(x) for x in res["mixed"]["drift"]))},
             "mass_drift_fp64_max": float(max(abs(x) for x in res["fp64"]["drift"])),
             "finite": res["fp64"]["finite"] and res["mixed"]["finite"],
-            "gpu_launches": (3 if "stage=fused" in res["fp64"]["tuning"] else 15) * K,
+            "perturbation": f"theta +-{E['theta_amp']} K, u,v +-{E['wind_amp']} m/s, seed {E['seed0']}+member",
+            "gpu_launches": (3 if "stage=fused" in res["fp64"]["tuning"] else 15) * K}
+
+
+def run_ensemble(args, rank, world, local):
+    """Batched-ensemble workload as its own line: every rank advances its
+    own 48-member ensemble (ensemble_measure)."""
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    ranks = Ranks(rank, world, torch.device("cuda", local))
+    r = ensemble_measure(args.steps, args.warmup, rank, ranks, torch)
+    if rank == 0:
+        line = {
+            "metric": "ensemble DOF-updates/s (48 members, p4: 16 x (nPanel 16, nz 30), (24, 45), (32, 64))",
+            "value": r["dof_updates_per_s"], "unit": "DOF-updates/s", "n_gpus": world, "steps": r["steps"],
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (baroclinic wave + seeded member perturbations)",
+            "config": {"workload": "batched ensemble: 48 members on 3 grids, one CUDA graph per ensemble step "
+                                   "(15 launches split, or 3 fused persistent stage launches; the autotuner picks "
+                                   "the work-list order, the form and the levels per phase-2 CTA)",
+                       "grids": r["grids"], "per_grid": r["per_grid"], "dt": r["dt"], "hours": r["hours"],
+                       "steps_total": r["steps_total"], "perturbation": r["perturbation"],
+                       "dt_note": "one dt below the explicit-acoustics limit of the finest member grid",
+                       "parallelism": "one ensemble per GPU"},
+            "dof_per_ensemble_step": r["dof_per_ensemble_step"], "tuning_fp64": r["tuning_fp64"],
+            "mixed": r["mixed"], "mass_drift_fp64_max": r["mass_drift_fp64_max"], "finite": r["finite"],
+            "gpu_launches": r["gpu_launches"],
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -567,6 +685,14 @@ def run_ours(args, cfg, rank, world, local):
     adjoint = None
     if args.precision == "fp64" and not args.no_adjoint:
         adjoint = run_adjoint(args, rank, ranks, torch)
+    mixed_cfg3 = None
+    if args.precision == "fp64" and not args.no_mixed_cfg3:
+        mixed_cfg3 = run_mixed_cfg3(args, rank, ranks, torch)
+    ensemble = None
+    if args.precision == "fp64" and not args.no_ensemble:
+        ensemble = ensemble_measure(args.ensemble_steps, 3, rank, ranks, torch)
+        ensemble["single_member_dof_updates_per_s"] = value * unique_dof(cfg) / world
+        ensemble["vs_single_member"] = ensemble["dof_updates_per_s"] / (value * unique_dof(cfg) / world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -606,13 +732,88 @@ def run_ours(args, cfg, rank, world, local):
             "kernel_share": shares,
             "e2e": e2e,
             "mixed": mixed,
+            "mixed_cfg3": mixed_cfg3,
             "adjoint": adjoint,
+            "ensemble": ensemble,
             "gpu_launches": 15 * args.steps,
             "cpu_baseline": cpu,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
     dyc.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def run_shard(args, cfg, rank, world, local):
+    """One grid decomposed over the ranks (strong scaling): every rank steps
+    its contiguous range of elements; each of the two DSS points of every
+    tendency exchanges the boundary element-node contributions with the
+    neighbouring ranks (NCCL peer sends/receives through torch.distributed),
+    and every rank sums a DOF's contributors in the single-process order.
+    value = whole-grid steps/s over the max-over-ranks time."""
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    from cgd_b200 import Dycore
+    from cgd_b200 import physics as Ph
+    from cgd_b200.model import _grid_and_state
+    from cgd_b200.parallel import TorchTransport, build_plans, partition_elements
+    grid, U0 = _grid_and_state(cfg)
+    plans = build_plans(grid, partition_elements(grid.NF, world))
+    P = plans[rank]
+    d = Dycore(P.local_grid(grid), cfg.NumTr, Ph.hyperdiffusion(cfg.nPanel, cfg.OrdPoly), Ph.PhysParameters(),
+               halo=P)
+    if world > 1:
+        d.set_transport(TorchTransport(P))
+    ranks = Ranks(rank, world, torch.device("cuda", local))
+    stream = torch.cuda.ExternalStream(d.stream())
+    Ut = torch.from_numpy(np.ascontiguousarray(P.restrict(U0).transpose(2, 1, 0))).cuda()
+    d.time_stepper(Ut, cfg.dt, args.warmup)
+    ranks.barrier()
+    clocks = Clocks(local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    d.time_stepper(Ut, cfg.dt, args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    t = ranks.max(e0.elapsed_time(e1) / 1e3)
+    clk = clocks.stop()
+    finite = bool(torch.isfinite(Ut).all().item())
+    # end to end: the rank's part of the state from and to pinned host memory every step
+    Uh = torch.from_numpy(np.ascontiguousarray(P.restrict(U0).transpose(2, 1, 0))).pin_memory()
+    d.time_stepper(Uh, cfg.dt, 1)
+    ranks.barrier()
+    Ke = max(1, args.e2e_steps)
+    e0.record(stream)
+    for _ in range(Ke):
+        d.time_stepper(Uh, cfg.dt, 1)
+    e1.record(stream)
+    e1.synchronize()
+    te = ranks.max(e0.elapsed_time(e1) / 1e3)
+    bytes_local = int(Uh.numel()) * 8
+    tot_bytes = ranks.max(bytes_local) * world if world > 1 else bytes_local
+    if rank == 0:
+        c = workload_config(cfg, "fp64")
+        c["parallelism"] = f"horizontal decomposition over {world} GPU(s): contiguous element ranges, " \
+                           f"halo exchange of DSS contributions (two per tendency)"
+        c["ghost_slots_rank0"] = int(P.n_ghost)
+        line = {"metric": METRIC, "value": args.steps / t, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (baroclinic wave + seeded noise)", "config": c,
+                "dof_updates_per_s": args.steps / t * unique_dof(cfg), "finite": finite,
+                "e2e": {"value": Ke / te, "unit": UNIT, "h2d_bytes_per_step": tot_bytes,
+                        "d2h_bytes_per_step": tot_bytes, "steps": Ke,
+                        "call": "cgd_ros_step(h_rank, host_part, dt, 1) per step on every rank"},
+                "gpu_launches": (15 + (12 if world > 1 else 0)) * args.steps, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    d.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 
@@ -632,6 +833,9 @@ def main():
     cfg = Ph.CONFIGS[args.config]
     if args.impl == "reference":
         run_reference(args, cfg, rank)
+        return
+    if args.parallel == "shard":
+        run_shard(args, cfg, rank, world, local)
         return
     run_ours(args, cfg, rank, world, local)
 

@@ -10,8 +10,10 @@ Host-side modules:
            (fcn_adjoint / ros_step_adjoint / steps_adjoint); Ensemble:
            batched members
   adjoint  gradients of scalar functionals of a run (BoxPressureFunctional)
+  parallel horizontal domain decomposition: element partition, halo plans,
+           the DSS exchange over torch.distributed
   build    compiles libcgd_b200.so for sm_100a
 """
 from . import grid, physics  # noqa: F401
 from ._lib import CgdError, lib  # noqa: F401
-from .model import Dycore, Ensemble, setup  # noqa: F401
+from .model import Dycore, Ensemble, PartGroup, setup  # noqa: F401

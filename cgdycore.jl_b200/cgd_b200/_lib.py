@@ -32,6 +32,7 @@ EXPORTS = [
     "cgd_tape_record_step", "cgd_tape_step_adjoint", "cgd_tape_release", "cgd_tape_bytes_per_step",
     "cgd_batch_create", "cgd_batch_step", "cgd_batch_tuning", "cgd_batch_get_stream", "cgd_batch_destroy",
     "cgd_grid_barrier_check",
+    "cgd_create_part", "cgd_set_exchange", "cgd_halo_buffers", "cgd_group_rhs", "cgd_group_ros_step",
 ]
 
 
@@ -43,6 +44,17 @@ class CgdConfig(ctypes.Structure):
                 ("p0", ctypes.c_double), ("Omega", ctypes.c_double),
                 ("HyperDCurl", ctypes.c_double), ("HyperDGrad", ctypes.c_double),
                 ("HyperDDiv", ctypes.c_double)]
+
+
+class CgdHalo(ctypes.Structure):
+    _fields_ = [("nnb", ctypes.c_int32), ("nb_boundary", ctypes.c_int32), ("nb_rank", ctypes.c_void_p),
+                ("send_ptr", ctypes.c_void_p), ("send_list", ctypes.c_void_p), ("recv_ptr", ctypes.c_void_p),
+                ("contrib_ptr", ctypes.c_void_p), ("contrib", ctypes.c_void_p)]
+
+
+# int (*cgd_exchange_fn)(void *user, void *stream, int32_t nf, const double *send, double *recv)
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                               ctypes.c_void_p)
 
 
 class CgdError(RuntimeError):
@@ -82,6 +94,18 @@ def lib(exact=False):
         L.cgd_tape_release.restype = ctypes.c_int
         L.cgd_tape_bytes_per_step.argtypes = [vp]
         L.cgd_tape_bytes_per_step.restype = ctypes.c_int64
+        L.cgd_create_part.argtypes = [ctypes.POINTER(CgdConfig)] + [vp] * 8 + [ctypes.POINTER(CgdHalo),
+                                                                              ctypes.POINTER(vp)]
+        L.cgd_create_part.restype = ctypes.c_int
+        L.cgd_set_exchange.argtypes = [vp, EXCHANGE_FN, vp]
+        L.cgd_set_exchange.restype = ctypes.c_int
+        L.cgd_halo_buffers.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(vp),
+                                       ctypes.POINTER(ctypes.c_int64)]
+        L.cgd_halo_buffers.restype = ctypes.c_int
+        L.cgd_group_rhs.argtypes = [vp, i32, vp, vp]
+        L.cgd_group_rhs.restype = ctypes.c_int
+        L.cgd_group_ros_step.argtypes = [vp, i32, vp, ctypes.c_double, i32]
+        L.cgd_group_ros_step.restype = ctypes.c_int
         L.cgd_grid_barrier_check.argtypes = [i32, i32, ctypes.c_double, ctypes.POINTER(i32)]
         L.cgd_grid_barrier_check.restype = ctypes.c_int
         for f in ("cgd_prepare", "cgd_hypervisc_phase1", "cgd_rhs", "cgd_jac"):

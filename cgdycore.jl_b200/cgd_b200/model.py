@@ -95,7 +95,9 @@ class Dycore:
     """One model instance on the current CUDA device."""
 
     def __init__(self, grid, NumTr=0, nu=(0.0, 0.0, 0.0), phys=None, precision="fp64",
-                 check_finite=False, exact=False):
+                 check_finite=False, exact=False, halo=None):
+        """grid: the whole grid, or with halo (a parallel.HaloPlan) one
+        rank's part of a decomposed grid (HaloPlan.local_grid)."""
         self.grid = grid
         self.phys = phys or PhysParameters(RadEarth=grid.Rad)
         self.nz, self.NumG, self.NF = grid.nz, grid.NumG, grid.NF
@@ -116,11 +118,49 @@ class Dycore:
             (grid.dXdxI, np.float64), (grid.J, np.float64), (grid.X, np.float64),
             (grid.M, np.float64), (grid.dz, np.float64))]
         h = ctypes.c_void_p()
-        rc = L.cgd_create(ctypes.byref(cfg), *[k.ctypes.data for k in self._keep], ctypes.byref(h))
+        self.halo = halo
+        if halo is None:
+            rc = L.cgd_create(ctypes.byref(cfg), *[k.ctypes.data for k in self._keep], ctypes.byref(h))
+        else:
+            arrs = [np.ascontiguousarray(a, np.int32) for a in (halo.neighbours, halo.send_ptr, halo.send_list,
+                                                               halo.recv_ptr, halo.contrib_ptr, halo.contrib)]
+            hs = _lib.CgdHalo(int(halo.neighbours.size), int(halo.nb_boundary), *[a.ctypes.data for a in arrs])
+            rc = L.cgd_create_part(ctypes.byref(cfg), *[k.ctypes.data for k in self._keep], ctypes.byref(hs),
+                                   ctypes.byref(h))
         self._keep = None
         _lib.check(rc, "cgd_create")
+        self._xfn = None
         self.h = h
         self._mmass = np.asfortranarray(grid.MMass)
+
+    def set_transport(self, transport):
+        """The exchange of a decomposed grid's rank between processes:
+        transport.exchange(send_views, recv_views) (parallel.TorchTransport)
+        is called at every DSS point with device views of the library's
+        packed buffers, on the library's stream."""
+        import torch
+        P = self.halo
+        sp, sn, rp, rn = ctypes.c_void_p(), ctypes.c_int64(), ctypes.c_void_p(), ctypes.c_int64()
+        _lib.check(self._L.cgd_halo_buffers(self.h, ctypes.byref(sp), ctypes.byref(sn), ctypes.byref(rp),
+                                            ctypes.byref(rn)), "cgd_halo_buffers")
+        sbuf = torch.as_tensor(_DevArray(sp.value, max(1, sn.value)), device="cuda")
+        rbuf = torch.as_tensor(_DevArray(rp.value, max(1, rn.value)), device="cuda")
+        nz, nnb = self.nz, P.neighbours.size
+
+        def exchange(user, stream, nf, send, recv):
+            try:
+                per = int(nf) * nz
+                with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+                    sv = [sbuf[P.send_ptr[i] * per:P.send_ptr[i + 1] * per] for i in range(nnb)]
+                    rv = [rbuf[P.recv_ptr[i] * per:P.recv_ptr[i + 1] * per] for i in range(nnb)]
+                    transport.exchange(sv, rv)
+                return 0
+            except Exception:   # noqa: BLE001 - reported to the library as a failed exchange
+                return -1
+
+        self._xfn = _lib.EXCHANGE_FN(exchange)   # kept alive with the handle
+        self._xbufs = (sbuf, rbuf)
+        _lib.check(self._L.cgd_set_exchange(self.h, self._xfn, None), "cgd_set_exchange")
 
     def close(self):
         if getattr(self, "h", None):
@@ -328,6 +368,39 @@ class Dycore:
         if n < 0:
             raise _lib.CgdError(n, "cgd_kernel_times")
         return list(zip(names.value.decode().split(";"), list(ms)[:n]))
+
+
+class _DevArray:
+    """A device buffer of the library seen by torch (zero copy)."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": "<f8", "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+class PartGroup:
+    """The parts of a decomposed grid run together in one process on one GPU
+    (parts[r] is rank r's Dycore): each DSS point exchanges the parts'
+    contributions by device copies.  The multi-process form runs the same
+    kernels and exchanges with one Dycore per process (set_transport)."""
+
+    def __init__(self, parts):
+        self.parts = list(parts)
+        self._L = self.parts[0]._L
+        self._h = (ctypes.c_void_p * len(self.parts))(*[p.h for p in self.parts])
+
+    def _ptrs(self, arrs, writable=False):
+        return (ctypes.c_void_p * len(arrs))(*[_ptr(a, p.shape, writable) for a, p in zip(arrs, self.parts)])
+
+    def fcn(self, U, F):
+        _lib.check(self._L.cgd_group_rhs(self._h, len(self.parts), self._ptrs(U), self._ptrs(F, True)),
+                   "cgd_group_rhs")
+        return F
+
+    def time_stepper(self, U, dt, nsteps):
+        _lib.check(self._L.cgd_group_ros_step(self._h, len(self.parts), self._ptrs(U, True), float(dt),
+                                              int(nsteps)), "cgd_group_ros_step")
+        return U
 
 
 class Ensemble:

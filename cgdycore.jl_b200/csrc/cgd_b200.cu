@@ -60,7 +60,8 @@ struct cgd_handle {
   cudaStream_t caller = cudaStreamLegacy;
   cudaEvent_t order_ev = nullptr;
   std::vector<Buf> bufs;
-  double *met = nullptr, *M = nullptr, *dz = nullptr;
+  double *met = nullptr, *met2 = nullptr, *M = nullptr, *dz = nullptr;
+  int *err_host = nullptr, *err_dev = nullptr;   // host-mapped flag of a kernel's bounded wait
   int *glob = nullptr, *inv_ptr = nullptr;
   long long *inv_off = nullptr;
   double *C = nullptr, *T1 = nullptr, *Vst = nullptr, *k1 = nullptr, *k2 = nullptr;
@@ -90,6 +91,14 @@ struct cgd_handle {
   // profile (the horizontal mean of the first state the handle sees)
   bool mix = false, have_ref = false;
   double *pref = nullptr, *thref = nullptr;
+  // horizontal domain decomposition (cgd_create_part): this rank's halo
+  bool decomposed = false;
+  int nghost = 0, nsend = 0;
+  std::vector<int32_t> nb_rank, send_ptr, recv_ptr;
+  int *send_list = nullptr;                     // device copy
+  double *sbuf = nullptr, *rbuf = nullptr;      // packed contributions, NC*nz per item
+  cgd_exchange_fn xfn = nullptr;
+  void *xuser = nullptr;
   std::string last_error;
 };
 
@@ -272,11 +281,11 @@ void column(cgd_handle *h, const ColArgs &a)
 // profiled step, see cgd_ros_step).
 void rec(cgd_handle *h, int i)
 {
-  if (h->profile && !h->capturing) cudaEventRecord(h->ev[i], h->stream);
+  if (h->profile && !h->capturing && i >= 0 && i <= NPROF) cudaEventRecord(h->ev[i], h->stream);
 }
 
-// One SSP-Knoth step on device state U (in place).
-void enqueue_step(cgd_handle *h, double *U, double dt)
+// Arguments of the column stages of one SSP-Knoth step of U.
+ColArgs step_args(cgd_handle *h, double *U, double dt)
 {
   ColArgs a{};
   a.Vn = U;
@@ -287,18 +296,33 @@ void enqueue_step(cgd_handle *h, double *U, double dt)
   a.rk = h->rk;
   a.C = h->C;
   a.jbg = h->jbg;
-  int e = 0;
-  rec(h, e++);
-  pressure(h, U, h->pres);
-  rec(h, e++);
-  for (int stage = 0; stage < 3; ++stage) {
-    const double *Vsrc = stage == 0 ? U : h->Vst;
+  return a;
+}
+
+// The three pieces of a Rosenbrock-W stage, split at the two direct-stiffness
+// summations (where a decomposed grid exchanges element contributions):
+//   piece 0: (stage 1: the pressure of the step's state) phase 1 -> C
+//   piece 1: DSS of phase 1 -> T1, phase 2 -> C
+//   piece 2: column stage (DSS of phase 2, solve, update), then the pressure
+//            of the next stage state
+// e counts the profiling events of the single-process step.
+void stage_piece(cgd_handle *h, double *U, const ColArgs &a0, int stage, int piece, int &e)
+{
+  const double *Vsrc = stage == 0 ? U : h->Vst;
+  if (piece == 0) {
+    if (stage == 0) {
+      pressure(h, U, h->pres);
+      rec(h, e++);
+    }
     hv1(h, Vsrc, h->C);
     rec(h, e++);
+  } else if (piece == 1) {
     gather(h, h->C, h->T1, false);
     rec(h, e++);
     phase2(h, Vsrc, stage == 0 ? h->pres : h->pres_st, h->T1, h->C);
     rec(h, e++);
+  } else {
+    ColArgs a = a0;
     if (stage == 0) {
       a.kout = h->k1; a.Vout = h->Vst;
       column<0>(h, a);
@@ -315,6 +339,142 @@ void enqueue_step(cgd_handle *h, double *U, double dt)
     }
     rec(h, e++);
   }
+}
+
+// One SSP-Knoth step on device state U (in place).
+void enqueue_step(cgd_handle *h, double *U, double dt)
+{
+  const ColArgs a = step_args(h, U, dt);
+  int e = 0;
+  rec(h, e++);
+  for (int stage = 0; stage < 3; ++stage)
+    for (int piece = 0; piece < 3; ++piece) stage_piece(h, U, a, stage, piece, e);
+}
+
+// ---- decomposed grids: packing, unpacking and the exchange of contributions
+// Pack the first nf contribution slots of the element nodes in send_list
+// (item j at j*nf*nz, field f at +f*nz).
+__global__ void __launch_bounds__(256) k_halo_pack(const double *__restrict__ C, double *__restrict__ sbuf,
+                                                   const int *__restrict__ list, int n, int nf, int DoF, int NC,
+                                                   int nz)
+{
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * nf * nz) return;
+  const int item = (int)(t / ((long long)nf * nz));
+  const int r = (int)(t - (long long)item * nf * nz);
+  const int f = r / nz, l = r - f * nz;
+  const int c = list[item], IF = c / DoF, ID = c - IF * DoF;
+  sbuf[t] = C[(((size_t)IF * NC + f) * DoF + ID) * nz + l];
+}
+// Unpack received contributions into the ghost slots of C: slot j is node
+// j % DoF of the pseudo-element NF + j / DoF.
+__global__ void __launch_bounds__(256) k_halo_unpack(const double *__restrict__ rbuf, double *__restrict__ C, int n,
+                                                     int NF, int nf, int DoF, int NC, int nz)
+{
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * nf * nz) return;
+  const int j = (int)(t / ((long long)nf * nz));
+  const int r = (int)(t - (long long)j * nf * nz);
+  const int f = r / nz, l = r - f * nz;
+  const int pe = NF + j / DoF, node = j % DoF;
+  C[(((size_t)pe * NC + f) * DoF + node) * nz + l] = rbuf[t];
+}
+
+void halo_pack(cgd_handle *h, int nf)
+{
+  const long long n = (long long)h->nsend * nf * h->nz;
+  if (n) k_halo_pack<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->C, h->sbuf, h->send_list, h->nsend, nf,
+                                                                         h->DoF, h->NV + 1, h->nz);
+}
+void halo_unpack(cgd_handle *h, int nf)
+{
+  const long long n = (long long)h->nghost * nf * h->nz;
+  if (n) k_halo_unpack<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->rbuf, h->C, h->nghost, h->NF, nf,
+                                                                           h->DoF, h->NV + 1, h->nz);
+}
+
+// The exchange of one DSS point among the ranks of an in-process group (all
+// on one stream): rank r's ghost slots from neighbour s are s's packed
+// segment for r, copied device to device.
+int group_exchange(cgd_handle *const *parts, int n, int nf, cudaStream_t st)
+{
+  for (int r = 0; r < n; ++r) {
+    cgd_handle *h = parts[r];
+    for (size_t i = 0; i < h->nb_rank.size(); ++i) {
+      const int sr = h->nb_rank[i];
+      const cgd_handle *q = parts[sr];
+      size_t j = 0;
+      while (j < q->nb_rank.size() && q->nb_rank[j] != r) ++j;
+      const size_t per = (size_t)nf * h->nz;
+      const size_t cnt = (size_t)(h->recv_ptr[i + 1] - h->recv_ptr[i]) * per;
+      if (!cnt) continue;
+      cudaError_t e = cudaMemcpyAsync(h->rbuf + (size_t)h->recv_ptr[i] * per, q->sbuf + (size_t)q->send_ptr[j] * per,
+                                      cnt * sizeof(double), cudaMemcpyDeviceToDevice, st);
+      if (e != cudaSuccess) return cuda_fail(h, e, "group exchange");
+    }
+  }
+  return CGD_OK;
+}
+
+// The exchange of one DSS point through the caller's transport (one process
+// per rank).
+int callback_exchange(cgd_handle *h, int nf)
+{
+  if (h->nb_rank.empty()) return CGD_OK;
+  if (!h->xfn) {
+    g_last_error = "decomposed grid without an exchange function (cgd_set_exchange)";
+    return CGD_ERR_INVALID_ARG;
+  }
+  const int rc = h->xfn(h->xuser, (void *)h->stream, nf, h->sbuf, h->rbuf);
+  if (rc) {
+    g_last_error = "the exchange function failed";
+    return CGD_ERR_CUDA;
+  }
+  return CGD_OK;
+}
+
+// One step (or, with rhs_only, one tendency into F) of every part of a
+// decomposed grid, the parts' pieces interleaved with the exchanges.  n > 1:
+// an in-process group on parts[0]'s stream; n == 1: one rank of a
+// multi-process run, exchanging through its callback.
+int part_pieces(cgd_handle *const *parts, int n, double *const *U, double dt, bool rhs_only, double *const *F)
+{
+  cgd_handle *h0 = parts[0];
+  const int nf1 = 5 + h0->NumTr, nf2 = h0->NV + 1;
+  auto xchg = [&](int nf) -> int {
+    for (int r = 0; r < n; ++r) halo_pack(parts[r], nf);
+    int rc = n > 1 ? group_exchange(parts, n, nf, h0->stream) : callback_exchange(h0, nf);
+    if (rc) return rc;
+    for (int r = 0; r < n; ++r) halo_unpack(parts[r], nf);
+    return CGD_OK;
+  };
+  int e = 0;
+  if (rhs_only) {
+    for (int r = 0; r < n; ++r) {
+      cgd_handle *h = parts[r];
+      hv1(h, U[r], h->C);
+    }
+    if (int rc = xchg(nf1)) return rc;
+    for (int r = 0; r < n; ++r) {
+      cgd_handle *h = parts[r];
+      gather(h, h->C, h->T1, false);
+      pressure(h, U[r], h->pres);
+      phase2(h, U[r], h->pres, h->T1, h->C);
+    }
+    if (int rc = xchg(nf2)) return rc;
+    for (int r = 0; r < n; ++r) gather(parts[r], parts[r]->C, F[r], true);
+    return CGD_OK;
+  }
+  std::vector<ColArgs> a(n);
+  for (int r = 0; r < n; ++r) a[r] = step_args(parts[r], U[r], dt);
+  for (int stage = 0; stage < 3; ++stage) {
+    for (int r = 0; r < n; ++r) stage_piece(parts[r], U[r], a[r], stage, 0, e);
+    if (int rc = xchg(nf1)) return rc;
+    for (int r = 0; r < n; ++r) stage_piece(parts[r], U[r], a[r], stage, 1, e);
+    if (int rc = xchg(nf2)) return rc;
+    for (int r = 0; r < n; ++r) stage_piece(parts[r], U[r], a[r], stage, 2, e);
+  }
+  return CGD_OK;
 }
 
 // Mixed form: the reference profile from the first state (before any capture).
@@ -375,15 +535,42 @@ const char *cgd_strerror(int code)
   }
 }
 
+static int create_impl(const cgd_config *cfg, const int64_t *glob, const double *DS, const double *DW,
+                       const double *dXdxI, const double *J, const double *X, const double *M, const double *dz,
+                       const cgd_halo *halo, cgd_handle **out);
+
 int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, const double *DW,
                const double *dXdxI, const double *J, const double *X, const double *M,
                const double *dz, cgd_handle **out)
+{
+  return create_impl(cfg, glob, DS, DW, dXdxI, J, X, M, dz, nullptr, out);
+}
+
+int cgd_create_part(const cgd_config *cfg, const int64_t *glob, const double *DS, const double *DW,
+                    const double *dXdxI, const double *J, const double *X, const double *M, const double *dz,
+                    const cgd_halo *halo, cgd_handle **out)
+{
+  if (!halo) return CGD_ERR_INVALID_ARG;
+  return create_impl(cfg, glob, DS, DW, dXdxI, J, X, M, dz, halo, out);
+}
+
+static int create_impl(const cgd_config *cfg, const int64_t *glob, const double *DS, const double *DW,
+                       const double *dXdxI, const double *J, const double *X, const double *M, const double *dz,
+                       const cgd_halo *halo, cgd_handle **out)
 {
   if (!out) return CGD_ERR_INVALID_ARG;
   *out = nullptr;
   int rc = check_cfg(cfg);
   if (rc) return rc;
   if (!glob || !DS || !DW || !dXdxI || !J || !X || !M || !dz) return CGD_ERR_INVALID_ARG;
+  if (halo) {
+    // the decomposed grid exchanges FP64 contributions
+    if (cfg->precision != CGD_PREC_FP64) return CGD_ERR_UNSUPPORTED;
+    if (halo->nnb < 0 || (halo->nnb > 0 && (!halo->nb_rank || !halo->send_ptr || !halo->send_list ||
+                                            !halo->recv_ptr)) ||
+        !halo->contrib_ptr || !halo->contrib)
+      return CGD_ERR_INVALID_ARG;
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -422,6 +609,53 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
       glob0[ID + (size_t)DoF * IF] = g;
       off[fill[g]++] = ((long long)IF * (NV + 1) * DoF + ID) * nz;
     }
+  // a decomposed grid: the contributor lists come from the halo plan, in
+  // ascending global (element, node) order, local element nodes and ghost
+  // slots (the contributions received from the neighbours) interleaved
+  int nghost = 0, nsend = 0;
+  if (halo) {
+    const int nnb = halo->nnb;
+    nghost = nnb ? halo->recv_ptr[nnb] : 0;
+    nsend = nnb ? halo->send_ptr[nnb] : 0;
+    if (nghost < 0 || nsend < 0) { delete h; return CGD_ERR_INVALID_ARG; }
+    for (int i = 0; i < nnb; ++i)
+      if (halo->recv_ptr[i + 1] < halo->recv_ptr[i] || halo->send_ptr[i + 1] < halo->send_ptr[i]) {
+        delete h;
+        return CGD_ERR_INVALID_ARG;
+      }
+    for (int i = 0; i < nsend; ++i)
+      if (halo->send_list[i] < 0 || halo->send_list[i] >= DoF * NF) { delete h; return CGD_ERR_INDEX; }
+    if (halo->contrib_ptr[0] != 0) { delete h; return CGD_ERR_INVALID_ARG; }
+    std::vector<int> p2(NumG + 1);
+    for (int g = 0; g <= NumG; ++g) {
+      p2[g] = halo->contrib_ptr[g];
+      if (g && (p2[g] <= p2[g - 1])) { delete h; return CGD_ERR_INDEX; }   // every DOF has a contributor
+    }
+    std::vector<long long> o2(p2[NumG]);
+    for (int q = 0; q < p2[NumG]; ++q) {
+      const int c = halo->contrib[q];
+      if (c >= 0) {
+        if (c >= DoF * NF) { delete h; return CGD_ERR_INDEX; }
+        o2[q] = ((long long)(c / DoF) * (NV + 1) * DoF + c % DoF) * nz;
+      } else {
+        const int j = -1 - c;
+        if (j >= nghost) { delete h; return CGD_ERR_INDEX; }
+        o2[q] = ((long long)(NF + j / DoF) * (NV + 1) * DoF + j % DoF) * nz;
+      }
+    }
+    ptr.swap(p2);
+    off.swap(o2);
+    h->decomposed = true;
+    h->nghost = nghost;
+    h->nsend = nsend;
+    h->nb_rank.assign(halo->nb_rank, halo->nb_rank + nnb);
+    h->send_ptr.assign(halo->send_ptr, halo->send_ptr + nnb + 1);
+    h->recv_ptr.assign(halo->recv_ptr, halo->recv_ptr + nnb + 1);
+    if (!nnb) {
+      h->send_ptr.assign(1, 0);
+      h->recv_ptr.assign(1, 0);
+    }
+  }
 
   // ---- compact metric [IF][comp][ID][nz]
   const size_t ENL = (size_t)DoF * nz * NF;
@@ -469,6 +703,15 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
         for (int c = 0; c < NCOMP; ++c) met[(((size_t)IF * NCOMP + c) * DoF + ID) * nz + Iz] = v[c];
       }
 
+  // ---- the same metric level-major [IF][lev][comp][ID] (blocks of LVB doubles)
+  const int LVB = (NCOMP * DoF + 1) & ~1;
+  std::vector<double> met2((size_t)NF * nz * LVB, 0.0);
+  for (int IF = 0; IF < NF; ++IF)
+    for (int c = 0; c < NCOMP; ++c)
+      for (int ID = 0; ID < DoF; ++ID)
+        for (int Iz = 0; Iz < nz; ++Iz)
+          met2[((size_t)IF * nz + Iz) * LVB + (size_t)c * DoF + ID] = met[(((size_t)IF * NCOMP + c) * DoF + ID) * nz + Iz];
+
   // ---- device resources
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->order_ev, cudaEventDisableTiming) != cudaSuccess) {
@@ -480,12 +723,33 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
   const size_t S = (size_t)nz * NumG;
 #define TRY(x) do { int r_ = (x); if (r_) { cgd_destroy(h); return r_; } } while (0)
   TRY(dalloc(h, &h->met, met.size()));
+  TRY(dalloc(h, &h->met2, met2.size()));
+  {
+    void *hp = nullptr, *dp = nullptr;
+    if (cudaHostAlloc(&hp, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(&dp, hp, 0) != cudaSuccess) {
+      cuda_fail(h, cudaGetLastError(), "cgd_create error flag");
+      if (hp) cudaFreeHost(hp);
+      cgd_destroy(h);
+      return CGD_ERR_CUDA;
+    }
+    h->err_host = static_cast<int *>(hp);
+    h->err_dev = static_cast<int *>(dp);
+    *h->err_host = 0;
+  }
   TRY(dalloc(h, &h->M, 2 * S));
   TRY(dalloc(h, &h->dz, S));
   TRY(dalloc(h, &h->glob, glob0.size()));
   TRY(dalloc(h, &h->inv_ptr, ptr.size()));
   TRY(dalloc(h, &h->inv_off, off.size()));
-  TRY(dalloc(h, &h->C, ENL * (NV + 1)));
+  // contribution buffer: the local elements, then the ghost pseudo-elements
+  const size_t ghost_elems = ((size_t)nghost + DoF - 1) / DoF;
+  TRY(dalloc(h, &h->C, ENL * (NV + 1) + ghost_elems * DoF * nz * (NV + 1)));
+  if (halo) {
+    TRY(dalloc(h, &h->send_list, (size_t)std::max(nsend, 1)));
+    TRY(dalloc(h, &h->sbuf, (size_t)std::max(nsend, 1) * (NV + 1) * nz));
+    TRY(dalloc(h, &h->rbuf, (size_t)std::max(nghost, 1) * (NV + 1) * nz));
+  }
   TRY(dalloc(h, &h->T1, S * NV));
   TRY(dalloc(h, &h->Vst, S * NV));
   TRY(dalloc(h, &h->k1, S * NV));
@@ -506,9 +770,10 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
   auto up = [&](void *dst, const void *src, size_t bytes) {
     return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
   };
-  if (up(h->met, met.data(), met.size() * 8) || up(h->M, M, 2 * S * 8) || up(h->dz, dz, S * 8) ||
+  if (up(h->met, met.data(), met.size() * 8) || up(h->met2, met2.data(), met2.size() * 8) || up(h->M, M, 2 * S * 8) || up(h->dz, dz, S * 8) ||
       up(h->glob, glob0.data(), glob0.size() * 4) || up(h->inv_ptr, ptr.data(), ptr.size() * 4) ||
-      up(h->inv_off, off.data(), off.size() * 8)) {
+      up(h->inv_off, off.data(), off.size() * 8) ||
+      (halo && nsend && up(h->send_list, halo->send_list, (size_t)nsend * 4))) {
     cudaError_t e = cudaGetLastError();
     cuda_fail(h, e, "cgd_create upload");
     cgd_destroy(h);
@@ -522,7 +787,7 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS, con
 
   GP &P = h->gp;
   P.N = N; P.DoF = DoF; P.nz = nz; P.NF = NF; P.NumG = NumG; P.NumTr = h->NumTr; P.NV = NV; P.NC = NV + 1;
-  P.met = h->met; P.M = h->M; P.dz = h->dz; P.glob = h->glob; P.inv_ptr = h->inv_ptr; P.inv_off = h->inv_off;
+  P.met = h->met; P.met2 = h->met2; P.met2_lvb = LVB; P.err = h->err_dev; P.M = h->M; P.dz = h->dz; P.glob = h->glob; P.inv_ptr = h->inv_ptr; P.inv_off = h->inv_off;
   P.pref = h->pref; P.thref = h->thref;
   for (int i = 0; i < 25; ++i) { P.D[i] = 0.0; P.DW[i] = 0.0; }
   for (int i = 0; i < N * N; ++i) { P.D[i] = DS[i]; P.DW[i] = DW[i]; }
@@ -556,6 +821,7 @@ void cgd_destroy(cgd_handle *h)
   if (h->stream) cudaStreamSynchronize(h->stream);
   free_graph(h);
   for (auto &b : h->bufs) cudaFree(b.p);
+  if (h->err_host) cudaFreeHost(h->err_host);
   for (void *q : h->work_tape.mem) cudaFree(q);
   for (auto &t : h->tapes)
     for (void *q : t.mem) cudaFree(q);
@@ -587,11 +853,25 @@ static int stage_in(cgd_handle *h, const double *p, double *buf, bool copy, doub
   return CGD_OK;
 }
 
+// 0, or CGD_ERR_TIMEOUT once if a kernel's bounded wait gave up since the
+// last check (the flag is cleared)
+static int take_err(cgd_handle *h)
+{
+  if (h->err_host && *reinterpret_cast<volatile int *>(h->err_host)) {
+    *reinterpret_cast<volatile int *>(h->err_host) = 0;
+    const char *m = "a kernel's bounded wait for its metric copy gave up";
+    g_last_error = m;
+    h->last_error = m;
+    return CGD_ERR_TIMEOUT;
+  }
+  return CGD_OK;
+}
+
 static int finish(cgd_handle *h)
 {
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->stream));
-  return CGD_OK;
+  return take_err(h);
 }
 
 int cgd_prepare(cgd_handle *h, const double *U, double *p)
@@ -636,6 +916,11 @@ int cgd_rhs(cgd_handle *h, const double *U, double *F)
   ensure_ref(h, Ud);
   bool fdev = is_device_ptr(F);
   double *fd = fdev ? F : h->Fbuf;
+  if (h->decomposed) {   // one rank of a decomposed grid: exchange through the callback
+    if ((rc = part_pieces(&h, 1, &Ud, 0.0, true, &fd))) return rc;
+    if (!fdev) CK(cudaMemcpyAsync(F, fd, (size_t)h->nz * h->NumG * h->NV * 8, cudaMemcpyDeviceToHost, h->stream));
+    return finish(h);
+  }
   hv1(h, Ud, h->C);
   gather(h, h->C, h->T1, false);
   pressure(h, Ud, h->pres);
@@ -756,6 +1041,13 @@ int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps)
   int rc = stage_in(h, U, h->Ubuf, true, &Ud);
   if (rc) return rc;
   ensure_ref(h, Ud);
+  if (h->decomposed) {   // one rank of a decomposed grid: steps with the callback's exchanges, not captured
+    for (int s = 0; s < nsteps; ++s)
+      if ((rc = part_pieces(&h, 1, &Ud, dt, false, nullptr))) return rc;
+    if (Ud != U)
+      CK(cudaMemcpyAsync(U, Ud, (size_t)h->nz * h->NumG * h->NV * 8, cudaMemcpyDeviceToHost, h->stream));
+    return finish(h);
+  }
   if (!h->gexec || h->graph_U != Ud || h->graph_dt != dt) {
     free_graph(h);
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -789,6 +1081,94 @@ int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps)
     if (f) return CGD_ERR_NONFINITE;
   }
   return CGD_OK;
+}
+
+int cgd_set_exchange(cgd_handle *h, cgd_exchange_fn fn, void *user)
+{
+  if (!h || !h->decomposed) return CGD_ERR_INVALID_ARG;
+  h->xfn = fn;
+  h->xuser = user;
+  return CGD_OK;
+}
+
+int cgd_halo_buffers(cgd_handle *h, double **send, int64_t *send_doubles, double **recv, int64_t *recv_doubles)
+{
+  if (!h || !h->decomposed || !send || !send_doubles || !recv || !recv_doubles) return CGD_ERR_INVALID_ARG;
+  *send = h->sbuf;
+  *recv = h->rbuf;
+  *send_doubles = (int64_t)h->nsend * (h->NV + 1) * h->nz;
+  *recv_doubles = (int64_t)h->nghost * (h->NV + 1) * h->nz;
+  return CGD_OK;
+}
+
+// Checks of an in-process group: parts[r] is rank r, one device, ranks and
+// exchange sizes consistent.  The parts then run on parts[0]'s stream.
+static int group_enter(cgd_handle *const *parts, int32_t n, std::vector<cudaStream_t> &saved)
+{
+  if (!parts || n < 1) return CGD_ERR_INVALID_ARG;
+  for (int r = 0; r < n; ++r) {
+    cgd_handle *h = parts[r];
+    if (!h || !h->decomposed || h->device != parts[0]->device || h->NV != parts[0]->NV || h->nz != parts[0]->nz)
+      return CGD_ERR_INVALID_ARG;
+    for (size_t i = 0; i < h->nb_rank.size(); ++i) {
+      const int sr = h->nb_rank[i];
+      if (sr < 0 || sr >= n || sr == r) return CGD_ERR_INVALID_ARG;
+      const cgd_handle *q = parts[sr];
+      size_t j = 0;
+      while (j < q->nb_rank.size() && q->nb_rank[j] != r) ++j;
+      if (j == q->nb_rank.size()) return CGD_ERR_INVALID_ARG;
+      if (h->recv_ptr[i + 1] - h->recv_ptr[i] != q->send_ptr[j + 1] - q->send_ptr[j]) return CGD_ERR_SHAPE;
+    }
+  }
+  for (int r = 0; r < n; ++r)
+    if (int rc = enter(parts[r])) return rc;
+  saved.resize(n);
+  for (int r = 0; r < n; ++r) {
+    saved[r] = parts[r]->stream;
+    parts[r]->stream = parts[0]->stream;
+  }
+  // work queued on a part's own stream before the call comes first
+  for (int r = 1; r < n; ++r) {
+    cgd_handle *h = parts[r];
+    cudaEventRecord(h->order_ev, saved[r]);
+    cudaStreamWaitEvent(parts[0]->stream, h->order_ev, 0);
+  }
+  return CGD_OK;
+}
+
+static int group_leave(cgd_handle *const *parts, int32_t n, const std::vector<cudaStream_t> &saved, int rc)
+{
+  for (int r = 0; r < n && r < (int)saved.size(); ++r) parts[r]->stream = saved[r];
+  if (rc) return rc;
+  int out = finish(parts[0]);
+  for (int r = 1; r < n; ++r)
+    if (int e = take_err(parts[r])) out = out ? out : e;
+  return out;
+}
+
+int cgd_group_rhs(cgd_handle *const *parts, int32_t n, const double *const *U, double *const *F)
+{
+  if (!U || !F) return CGD_ERR_INVALID_ARG;
+  for (int r = 0; r < n; ++r)
+    if (!U[r] || !F[r] || !is_device_ptr(U[r]) || !is_device_ptr(F[r])) return CGD_ERR_INVALID_ARG;
+  std::vector<cudaStream_t> saved;
+  if (int rc = group_enter(parts, n, saved)) return rc;
+  std::vector<double *> Ud(n);
+  for (int r = 0; r < n; ++r) Ud[r] = const_cast<double *>(U[r]);
+  const int rc = part_pieces(parts, n, Ud.data(), 0.0, true, F);
+  return group_leave(parts, n, saved, rc);
+}
+
+int cgd_group_ros_step(cgd_handle *const *parts, int32_t n, double *const *U, double dt, int32_t nsteps)
+{
+  if (!U || !(dt > 0) || nsteps < 0) return CGD_ERR_INVALID_ARG;
+  for (int r = 0; r < n; ++r)
+    if (!U[r] || !is_device_ptr(U[r])) return CGD_ERR_INVALID_ARG;
+  std::vector<cudaStream_t> saved;
+  if (int rc = group_enter(parts, n, saved)) return rc;
+  int rc = CGD_OK;
+  for (int s = 0; s < nsteps && !rc; ++s) rc = part_pieces(parts, n, U, dt, false, nullptr);
+  return group_leave(parts, n, saved, rc);
 }
 
 int cgd_mass_integral(cgd_handle *h, const double *U, const double *MMass, double *out)
@@ -1665,7 +2045,10 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
     g_last_error = "cgd_batch_step: a fused stage launch timed out at a grid barrier";
     return CGD_ERR_TIMEOUT;
   }
-  return CGD_OK;
+  int werr = CGD_OK;
+  for (int m = 0; m < nm; ++m)
+    if (int e = take_err(b->mem[m])) werr = e;   // clears every member's flag
+  return werr;
 }
 
 int cgd_grid_barrier_check(int32_t rounds, int32_t absent, double limit_s, int32_t *violations)

@@ -74,6 +74,12 @@ struct GP {
   int N, DoF, nz, NF, NumG, NumTr, NV;
   int NC;                   // contribution slots per element node: NV fields + the lower-node w of phase 2
   const double *met;        // [IF][comp][ID][nz]
+  // the same metric level-major for the tendency kernel: [IF][lev][comp][ID],
+  // one block of met2_lvb doubles (a multiple of 16 bytes) per element level,
+  // so the levels a tendency CTA reads are one contiguous 16-byte-aligned range
+  const double *met2;
+  int met2_lvb;
+  int *err;                 // set by a kernel whose bounded wait gave up (host-mapped)
   const double *M;          // (nz, NumG, 2)
   const double *dz;         // (nz, NumG)
   const int *glob;          // [IF*DoF + ID], 0-based

@@ -83,6 +83,62 @@ int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS,
                cgd_handle **out);
 void cgd_destroy(cgd_handle *h);
 
+/* Horizontal domain decomposition.  One rank's part of the grid is a grid of
+ * its own (its elements, the DOFs they touch, numbered locally) plus its
+ * halo: the reference partitions the faces over MPI ranks
+ * (src/Grids/InitGrid.jl:34-43, src/Grids/SubGridGhost.jl:1-239) and sums
+ * each rank's boundary values with its neighbours' after both DSS points of
+ * a tendency (ExchangeData3DSendGPU / ExchangeData3DRecvGPU!,
+ * src/Parallels/Exchange.jl:938-1071; src/GPU/FcnGPU.jl:777-913).  Here the
+ * ranks exchange element-node contributions and every rank sums all
+ * contributors of a DOF in ascending global (element, node) order, so every
+ * rank's DSS'd values, and the column solves that follow, equal the
+ * single-process ones bit for bit.  Element-node indices are IF*DoF + ID of
+ * the local numbering, 0-based. */
+typedef struct cgd_halo {
+  int32_t nnb;                 /* neighbour ranks */
+  int32_t nb_boundary;         /* the first nb_boundary local elements touch another rank */
+  const int32_t *nb_rank;      /* [nnb] ascending */
+  const int32_t *send_ptr;     /* [nnb+1] offsets into send_list */
+  const int32_t *send_list;    /* element nodes whose contributions go to nb_rank[i], in its slot order */
+  const int32_t *recv_ptr;     /* [nnb+1]: ghost slots recv_ptr[i] .. recv_ptr[i+1]-1 come from nb_rank[i] */
+  const int32_t *contrib_ptr;  /* [NumG+1] */
+  const int32_t *contrib;      /* contributors of each local DOF, ascending global (element, node) order:
+                                  c >= 0 a local element node, c < 0 the ghost slot -1-c */
+} cgd_halo;
+
+/* A rank's part of a decomposed grid (arguments as cgd_create, over the
+ * rank's own elements and DOFs; M and dz are the single-process values at
+ * its DOFs).  FP64 only (CGD_ERR_UNSUPPORTED for the mixed form).
+ * cgd_rhs and cgd_ros_step on such a handle exchange contributions through
+ * the function set with cgd_set_exchange; cgd_group_rhs and
+ * cgd_group_ros_step run the parts of one process together instead.
+ * The element partition and the plan come from cgd_b200.parallel (host). */
+int cgd_create_part(const cgd_config *cfg, const int64_t *glob, const double *DS, const double *DW,
+                    const double *dXdxI, const double *J, const double *X, const double *M, const double *dz,
+                    const cgd_halo *halo, cgd_handle **out);
+
+/* The exchange of one DSS point, supplied by the caller (e.g. NCCL peer
+ * sends/receives between processes): nf contribution fields of nz levels per
+ * element node are packed in `send` (neighbour i's items from
+ * send_ptr[i]*nf*nz on) and must be received into `recv` (neighbour i's
+ * items from recv_ptr[i]*nf*nz on) before the function returns, or be
+ * ordered before later work on `stream` (the handle's cudaStream_t, on which
+ * the packing was enqueued).  Returns 0 on success. */
+typedef int (*cgd_exchange_fn)(void *user, void *stream, int32_t nf, const double *send, double *recv);
+int cgd_set_exchange(cgd_handle *h, cgd_exchange_fn fn, void *user);
+/* The device buffers the exchange reads and fills (sizes in doubles, for
+ * nf = NV + 1). */
+int cgd_halo_buffers(cgd_handle *h, double **send, int64_t *send_doubles, double **recv, int64_t *recv_doubles);
+
+/* All parts of a decomposed grid in one process on one device (parts[r] is
+ * rank r): the tendency F[r] = Fcn(U[r]) or nsteps Rosenbrock-W steps of
+ * every U[r] in place, each DSS point exchanging the parts' contributions by
+ * device copies.  Device pointers.  Ordered after the work queued on every
+ * part's caller stream; returns with the work complete. */
+int cgd_group_rhs(cgd_handle *const *parts, int32_t n, const double *const *U, double *const *F);
+int cgd_group_ros_step(cgd_handle *const *parts, int32_t n, double *const *U, double dt, int32_t nsteps);
+
 /* Pressure p (nz, NumG) from the state.
  * Replaces GPU.FcnPrepareGPU! / PressureKernel! (src/GPU/DiagnosticKernel.jl:96-115,180-218). */
 int cgd_prepare(cgd_handle *h, const double *U, double *p);

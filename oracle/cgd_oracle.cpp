@@ -1681,6 +1681,25 @@ int orc_hypervisc1(void *h, const double *U, double *Temp1)
   return 0;
 }
 
+// The element-node contributions before their DSS, layout
+// ((IF*nz + Iz)*nf + f)*DoF + ID: phase 1 (T1 == NULL, nf = 5 + NumTr) or
+// phase 2 at the DSS'd phase-1 cache T1 (nf = NV).  orc_hypervisc1 and
+// orc_rhs are these summed per global DOF in ascending (element, node) order.
+int orc_contributions(void *h, const double *U, const double *T1, double *C)
+{
+  Model *m = static_cast<Model *>(h);
+  Ctx c(*m, U);
+  const int nf = T1 ? m->NV : 5 + m->NumTr;
+  std::vector<double> Cv((size_t)m->NF * m->nz * nf * m->DoF);
+  #pragma omp parallel for schedule(dynamic, 4)
+  for (int IF = 0; IF < m->NF; ++IF) {
+    if (T1) phase2_element(*m, c, T1, IF, Cv);
+    else hypervisc1_element(*m, c, IF, Cv);
+  }
+  memcpy(C, Cv.data(), Cv.size() * sizeof(double));
+  return 0;
+}
+
 int orc_rhs(void *h, const double *U, double *F)
 {
   rhs(*static_cast<Model *>(h), U, F);

@@ -49,6 +49,7 @@ def lib():
         L.orc_init_state.argtypes = [vp, vp, vp]
         for f in ["orc_pressure", "orc_hypervisc1", "orc_rhs", "orc_jac"]:
             getattr(L, f).argtypes = [vp, vp, vp]
+        L.orc_contributions.argtypes = [vp, vp, vp, vp]
         L.orc_schur.argtypes = [vp, vp, vp, ctypes.c_double]
         L.orc_ros_step.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int]
         L.orc_mass_integral.argtypes = [vp, vp]
@@ -156,6 +157,17 @@ class Oracle:
         T = np.zeros((self.nz, self.NumG, 5 + self.NumTr), order="F")
         lib().orc_hypervisc1(self.h, _p(U), _p(T))
         return T
+
+    def contributions(self, U, T1=None):
+        """Element-node contributions before the DSS, shape (DoF, nf, nz, NF)
+        in Fortran order: phase 1 (T1 None, nf = 5 + NumTr) or phase 2 at the
+        DSS'd phase-1 cache T1 (nf = NV)."""
+        U = np.asfortranarray(U)
+        nf = self.NV if T1 is not None else 5 + self.NumTr
+        C = np.zeros(self.DoF * nf * self.nz * self.NF)
+        T = np.asfortranarray(T1) if T1 is not None else None
+        lib().orc_contributions(self.h, _p(U), _p(T) if T is not None else None, _p(C))
+        return C.reshape((self.DoF, nf, self.nz, self.NF), order="F")
 
     def rhs(self, U):
         U = np.asfortranarray(U)
