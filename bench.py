@@ -358,9 +358,9 @@ def run_mixed_cfg3(args, rank, ranks, torch):
     p64, pm = out["fp64"]["p1"], out["mixed"]["p1"]
     return {"config": {"workload": "mixed: cubed sphere nPanel 60 (21600 elements), OrdPoly 4, nz 64 quadratic, "
                                    f"NumTr 0, dt {cfg.dt:g} s", "nPanel": cfg.nPanel, "nz": cfg.nz, "dt": cfg.dt,
-                       "dt_note": "dt 150 s is beyond the explicit horizontal-acoustics limit of this W-method at "
+                       "dt_note": "dt 150 s (and 60 s, NaN within 60 steps) is beyond the explicit horizontal-acoustics limit of this W-method at "
                                   "nPanel 60 (it halves the grid spacing of nPanel 30, where 150 s already fails); "
-                                  "60 s keeps the drop-in grid's Courant number"},
+                                  "50 s is stable for the simulated day"},
             "fp64_steps_per_s": out["fp64"]["steps_per_s"], "mixed_steps_per_s": out["mixed"]["steps_per_s"],
             "speedup_vs_fp64": out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"],
             "accuracy": {"simulated_days": nsteps * cfg.dt / 86400.0, "steps": nsteps,
@@ -384,7 +384,7 @@ def adjoint_fd_entries(d, U, dt, nsteps, rng, per_field=8, rels=(1e-5, 1e-6, 1e-
     lam = torch.from_numpy(rng.standard_normal(tuple(U.shape))).to(U.device)
     G = d.steps_adjoint(U, lam, dt, nsteps, every=1)
     NV, NumG, nz = U.shape
-    work = U.clone()
+    wp, wm = U.clone(), U.clone()
     rows = []
     for f in range(NV):
         scale = max(float(U[f].abs().max()), 1.0)
@@ -395,24 +395,29 @@ def adjoint_fd_entries(d, U, dt, nsteps, rng, per_field=8, rels=(1e-5, 1e-6, 1e-
             fds = []
             for rel in rels:
                 h = rel * scale
-                work.copy_(U)
-                work[f, g, l] += h
-                d.time_stepper(work, dt, nsteps)
-                jp = float(torch.sum(lam * work))
-                work.copy_(U)
-                work[f, g, l] -= h
-                d.time_stepper(work, dt, nsteps)
-                jm = float(torch.sum(lam * work))
-                fds.append((jp - jm) / (2 * h))
+                wp.copy_(U)
+                wp[f, g, l] += h
+                d.time_stepper(wp, dt, nsteps)
+                wm.copy_(U)
+                wm[f, g, l] -= h
+                d.time_stepper(wm, dt, nsteps)
+                # the difference first: away from the perturbed entry's reach the
+                # two runs are identical, so only the affected entries add up
+                fds.append(float(torch.sum(lam * (wp - wm))) / (2 * h))
             den = max(abs(a), med, 1e-300)
-            rows.append({"field": f, "level": l, "err": min(abs(x - a) for x in fds) / den,
-                         "spread": (max(fds) - min(fds)) / den})
+            rows.append({"err": min(abs(x - a) for x in fds) / den, "spread": (max(fds) - min(fds)) / den})
     errs = np.array([r["err"] for r in rows])
+    spread = np.array([r["spread"] for r in rows])
+    smooth = spread <= tol
     return {"entries": len(rows), "steps": nsteps, "rel_steps": list(rels), "tol": tol,
             "pass_fraction": float(np.mean(errs <= tol)), "pass_fraction_1e-5": float(np.mean(errs <= 1e-5)),
+            "smooth_entries": int(smooth.sum()),
+            "pass_fraction_smooth": float(np.mean(errs[smooth] <= tol)) if smooth.any() else None,
             "err_median": float(np.median(errs)), "err_max": float(errs.max()),
             "functional": "L = <lam, U_n>, lam ~ N(0,1) seeded; error = min over step sizes |FD - adjoint| / "
-                          "max(|adjoint|, median |gradient| of the field)"}
+                          "max(|adjoint|, median |gradient| of the field); an entry is smooth when its "
+                          "differences at the step sizes agree with each other within tol (no limiter or "
+                          "upwind kink within reach)"}
 
 
 def run_adjoint(args, rank, ranks, torch):

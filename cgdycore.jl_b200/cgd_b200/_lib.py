@@ -33,6 +33,7 @@ EXPORTS = [
     "cgd_batch_create", "cgd_batch_step", "cgd_batch_tuning", "cgd_batch_get_stream", "cgd_batch_destroy",
     "cgd_grid_barrier_check",
     "cgd_create_part", "cgd_set_exchange", "cgd_halo_buffers", "cgd_group_rhs", "cgd_group_ros_step",
+    "cgd_metric_sphere", "cgd_mass_dz",
 ]
 
 
@@ -106,6 +107,10 @@ def lib(exact=False):
         L.cgd_group_rhs.restype = ctypes.c_int
         L.cgd_group_ros_step.argtypes = [vp, i32, vp, ctypes.c_double, i32]
         L.cgd_group_ros_step.restype = ctypes.c_int
+        L.cgd_metric_sphere.argtypes = [i32, i32, i32, vp, vp, vp, vp, dbl, dbl, vp, vp, vp]
+        L.cgd_metric_sphere.restype = ctypes.c_int
+        L.cgd_mass_dz.argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp]
+        L.cgd_mass_dz.restype = ctypes.c_int
         L.cgd_grid_barrier_check.argtypes = [i32, i32, ctypes.c_double, ctypes.POINTER(i32)]
         L.cgd_grid_barrier_check.restype = ctypes.c_int
         for f in ("cgd_prepare", "cgd_hypervisc_phase1", "cgd_rhs", "cgd_jac"):

@@ -20,12 +20,9 @@ def column_lonlat(grid):
     """Longitude in [0, 2 pi) and latitude (radians) of the lowest-layer
     midpoint of every column; a column's node takes the coordinates of the
     highest-numbered element that holds it, as the initial state does."""
-    DoF, numg = grid.glob.shape[0], grid.NumG
-    g0 = np.asarray(grid.glob, order="F").T.ravel() - 1
-    last = np.zeros(numg, np.int64)
-    last[g0] = np.arange(g0.size)
-    IF, ID = last // DoF, last % DoF
-    mid = 0.5 * (grid.X[ID, 0, :, 0, IF] + grid.X[ID, 1, :, 0, IF])   # (numg, 3)
+    from .grid import node_positions
+    P = node_positions(grid)                                       # (numg, 2, 3, nz)
+    mid = 0.5 * (P[:, 0, :, 0] + P[:, 1, :, 0])                    # (numg, 3)
     lon = np.mod(np.arctan2(mid[:, 1], mid[:, 0]), 2 * np.pi)
     lat = np.arcsin(mid[:, 2] / np.linalg.norm(mid, axis=1))
     return lon, lat

@@ -36,6 +36,8 @@ DEPS = [os.path.join(PKG_DIR, "csrc", f) for f in ("cgd_b200.cu", "cgd_adjoint.c
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC,-ffp-contract=off"]
+# (nvcc --split-compile builds about three times faster here but its code is
+# slower: the tendency kernel took 1.52 instead of 1.41 ms per launch)
 VARIANTS = {LIB_PATH: ["-DCGD_FAST"], LIB_PATH_EXACT: []}
 FWD_FLAGS = ["-fmad=false"]   # the forward translation unit (cgd_b200.cu)
 ADJ_FLAGS = ["-fmad=true"]    # the adjoint translation unit (cgd_adjoint.cu)

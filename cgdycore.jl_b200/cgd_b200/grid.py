@@ -592,3 +592,64 @@ def init_grid_sphere(nPanel, OrdPoly, z, H, Rad):
     M, MM, dz = mass_and_dz(glob, J, X, w, numg)
     return Grid(nPanel, OrdPoly, z.size - 1, FN.shape[0], numg, nnodes, nedges, Rad, H, z, glob, FP,
                 xw, w, DS, DW, X, dXdxI, J, M, MM, dz)
+
+
+def _fortran_tensor(shape, device):
+    """A CUDA float64 tensor holding a Fortran-ordered array of `shape` (the
+    tensor's own shape is reversed, contiguous)."""
+    import torch
+    return torch.empty(tuple(reversed(shape)), dtype=torch.float64, device=device)
+
+
+def init_grid_sphere_device(nPanel, OrdPoly, z, H, Rad, device="cuda"):
+    """init_grid_sphere with the floating-point arrays formed on the GPU: the
+    topology and the Glob numbering on the host (integer work), the metric
+    (cgd_metric_sphere) and the mass and dz (cgd_mass_dz) on the device.
+    X, dXdxI, J, M, MMass and dz are CUDA tensors holding the reference's
+    Fortran-ordered arrays (tensor shapes reversed).  The metric uses the
+    device's trigonometric functions, so it agrees with init_grid_sphere to
+    rounding."""
+    from . import _lib
+    z = np.asarray(z, dtype=np.float64)
+    nz = z.size - 1
+    FN, FE, EN, FP, nnodes, nedges = build_topology(nPanel, Rad)
+    glob, numg = numbering_cg_quad(FN, FE, EN, nnodes, nedges, OrdPoly)
+    xw, w, DS, DW = derivative_matrices(OrdPoly)
+    NF, N = FN.shape[0], OrdPoly + 1
+    DoF = N * N
+    X = _fortran_tensor((DoF, 2, 3, nz, NF), device)
+    dXdxI = _fortran_tensor((3, 3, 2, DoF, nz, NF), device)
+    J = _fortran_tensor((DoF, 2, nz, NF), device)
+    M = _fortran_tensor((nz, numg, 2), device)
+    MM = _fortran_tensor((nz, numg), device)
+    dz = _fortran_tensor((nz, numg), device)
+    L = _lib.lib()
+    fp = np.ascontiguousarray(FP, dtype=np.float64)
+    dsf = np.asfortranarray(DS, dtype=np.float64)
+    xw_, w_, z_ = (np.ascontiguousarray(a, dtype=np.float64) for a in (xw, w, z))
+    _lib.check(L.cgd_metric_sphere(OrdPoly, nz, NF, fp.ctypes.data, xw_.ctypes.data, dsf.ctypes.data,
+                                   z_.ctypes.data, float(H), float(Rad), X.data_ptr(), dXdxI.data_ptr(),
+                                   J.data_ptr()), "cgd_metric_sphere")
+    g64 = np.asfortranarray(glob, dtype=np.int64)
+    _lib.check(L.cgd_mass_dz(OrdPoly, nz, NF, numg, g64.ctypes.data, w_.ctypes.data, J.data_ptr(), X.data_ptr(),
+                             M.data_ptr(), MM.data_ptr(), dz.data_ptr()), "cgd_mass_dz")
+    return Grid(nPanel, OrdPoly, nz, NF, numg, nnodes, nedges, Rad, H, z, glob, FP, xw, w, DS, DW,
+                X, dXdxI, J, M, MM, dz)
+
+
+def node_positions(grid):
+    """(NumG, 2, 3, nz): the bottom and top positions of every column's nodes,
+    taken from the highest-numbered element node holding the DOF (the one the
+    reference's init kernels write last); works on host arrays and on the
+    device tensors of init_grid_sphere_device."""
+    DoF, numg = grid.glob.shape[0], grid.NumG
+    g0 = np.asarray(grid.glob, order="F").T.ravel() - 1            # index IF*DoF + ID
+    last = np.zeros(numg, np.int64)
+    last[g0] = np.arange(g0.size)                                  # later writes overwrite
+    IF, ID = last // DoF, last % DoF
+    X = grid.X
+    if isinstance(X, np.ndarray):
+        return X[ID, :, :, :, IF]                                  # (numg, 2, 3, nz)
+    import torch
+    t = X[torch.as_tensor(IF, device=X.device), :, :, :, torch.as_tensor(ID, device=X.device)]   # (numg, nz, 3, 2)
+    return t.permute(0, 3, 2, 1).cpu().numpy()

@@ -113,25 +113,26 @@ class Dycore:
         ph = self.phys
         cfg.Grav, cfg.Rd, cfg.Cpd, cfg.p0, cfg.Omega = ph.Grav, ph.Rd, ph.Cpd, ph.p0, ph.Omega
         cfg.HyperDCurl, cfg.HyperDGrad, cfg.HyperDDiv = nu
-        self._keep = [np.asfortranarray(x, dtype=t) for x, t in (
+        # host arrays, or the device tensors of grid.init_grid_sphere_device
+        self._keep = [x if hasattr(x, "data_ptr") else np.asfortranarray(x, dtype=t) for x, t in (
             (grid.glob, np.int64), (grid.DS, np.float64), (grid.DW, np.float64),
             (grid.dXdxI, np.float64), (grid.J, np.float64), (grid.X, np.float64),
             (grid.M, np.float64), (grid.dz, np.float64))]
+        ptrs = [k.data_ptr() if hasattr(k, "data_ptr") else k.ctypes.data for k in self._keep]
         h = ctypes.c_void_p()
         self.halo = halo
         if halo is None:
-            rc = L.cgd_create(ctypes.byref(cfg), *[k.ctypes.data for k in self._keep], ctypes.byref(h))
+            rc = L.cgd_create(ctypes.byref(cfg), *ptrs, ctypes.byref(h))
         else:
             arrs = [np.ascontiguousarray(a, np.int32) for a in (halo.neighbours, halo.send_ptr, halo.send_list,
                                                                halo.recv_ptr, halo.contrib_ptr, halo.contrib)]
             hs = _lib.CgdHalo(int(halo.neighbours.size), int(halo.nb_boundary), *[a.ctypes.data for a in arrs])
-            rc = L.cgd_create_part(ctypes.byref(cfg), *[k.ctypes.data for k in self._keep], ctypes.byref(hs),
-                                   ctypes.byref(h))
+            rc = L.cgd_create_part(ctypes.byref(cfg), *ptrs, ctypes.byref(hs), ctypes.byref(h))
         self._keep = None
         _lib.check(rc, "cgd_create")
         self._xfn = None
         self.h = h
-        self._mmass = np.asfortranarray(grid.MMass)
+        self._mmass = grid.MMass if hasattr(grid.MMass, "data_ptr") else np.asfortranarray(grid.MMass)
 
     def set_transport(self, transport):
         """The exchange of a decomposed grid's rank between processes:
@@ -343,8 +344,9 @@ class Dycore:
 
     def mass_integral(self, U):
         out = ctypes.c_double()
-        _lib.check(self._L.cgd_mass_integral(self.h, _ptr(U, self.shape), self._mmass.ctypes.data,
-                                                ctypes.byref(out)), "cgd_mass_integral")
+        mm = self._mmass.data_ptr() if hasattr(self._mmass, "data_ptr") else self._mmass.ctypes.data
+        _lib.check(self._L.cgd_mass_integral(self.h, _ptr(U, self.shape), mm, ctypes.byref(out)),
+                   "cgd_mass_integral")
         return out.value
 
     def set_caller_stream(self, stream=None):
@@ -454,16 +456,19 @@ class Ensemble:
 _SETUP_CACHE = {}
 
 
-def _grid_and_state(cfg):
+def _grid_and_state(cfg, where="host"):
     """Grid and seeded initial state of a configuration, built once per
-    process (the arrays are read-only inputs of the library)."""
+    process (the arrays are read-only inputs of the library).  where="device"
+    forms the grid's floating-point arrays on the GPU
+    (grid.init_grid_sphere_device)."""
     from . import grid as G
     from . import physics as Ph
     key = (cfg.nPanel, cfg.OrdPoly, cfg.nz, cfg.stretch, cfg.H, cfg.NumTr, cfg.Up, cfg.theta_noise,
-           cfg.seed_theta, cfg.seed_tracer)
+           cfg.seed_theta, cfg.seed_tracer, where)
     if key not in _SETUP_CACHE:
         phys = Ph.PhysParameters()
-        grid = G.init_grid_sphere(cfg.nPanel, cfg.OrdPoly, cfg.levels(), cfg.H, phys.RadEarth)
+        init = G.init_grid_sphere_device if where == "device" else G.init_grid_sphere
+        grid = init(cfg.nPanel, cfg.OrdPoly, cfg.levels(), cfg.H, phys.RadEarth)
         tl = Ph.tracer_centres(cfg.NumTr, cfg.seed_tracer) if cfg.NumTr else None
         U = Ph.initial_state(grid, phys, cfg.NumTr, tl, cfg.Up)
         Ph.theta_noise(U, cfg.theta_noise, cfg.seed_theta)
@@ -472,16 +477,17 @@ def _grid_and_state(cfg):
     return _SETUP_CACHE[key]
 
 
-def setup(cfg_name_or_cfg, precision="fp64", check_finite=False, nz=None, nPanel=None, exact=False):
+def setup(cfg_name_or_cfg, precision="fp64", check_finite=False, nz=None, nPanel=None, exact=False, where="host"):
     """Grid + initial state + Dycore for a named configuration
-    (physics.CONFIGS).  Returns (dycore, U0, config); U0 is a fresh copy."""
+    (physics.CONFIGS).  Returns (dycore, U0, config); U0 is a fresh copy.
+    where="device": the grid's floating-point arrays formed on the GPU."""
     from . import physics as Ph
     cfg = Ph.CONFIGS[cfg_name_or_cfg] if isinstance(cfg_name_or_cfg, str) else cfg_name_or_cfg
     if nz is not None or nPanel is not None:
         import dataclasses
         cfg = dataclasses.replace(cfg, nz=nz or cfg.nz, nPanel=nPanel or cfg.nPanel)
     phys = Ph.PhysParameters()
-    grid, U = _grid_and_state(cfg)
+    grid, U = _grid_and_state(cfg, where)
     nu = Ph.hyperdiffusion(cfg.nPanel, cfg.OrdPoly)
     dyc = Dycore(grid, cfg.NumTr, nu, phys, precision=precision, check_finite=check_finite, exact=exact)
     return dyc, U.copy(order="F"), cfg

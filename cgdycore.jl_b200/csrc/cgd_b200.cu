@@ -9,6 +9,7 @@
 #include "cgd_kernels.cuh"
 #include "cgd_phase2.cuh"
 #include "cgd_batch.cuh"
+#include "cgd_init.cuh"
 #include "cgd_adjoint_launch.h"
 
 #include <cuda_runtime.h>
@@ -60,8 +61,7 @@ struct cgd_handle {
   cudaStream_t caller = cudaStreamLegacy;
   cudaEvent_t order_ev = nullptr;
   std::vector<Buf> bufs;
-  double *met = nullptr, *met2 = nullptr, *M = nullptr, *dz = nullptr;
-  int *err_host = nullptr, *err_dev = nullptr;   // host-mapped flag of a kernel's bounded wait
+  double *met = nullptr, *M = nullptr, *dz = nullptr;
   int *glob = nullptr, *inv_ptr = nullptr;
   long long *inv_off = nullptr;
   double *C = nullptr, *T1 = nullptr, *Vst = nullptr, *k1 = nullptr, *k2 = nullptr;
@@ -657,11 +657,14 @@ static int create_impl(const cgd_config *cfg, const int64_t *glob, const double 
     }
   }
 
-  // ---- compact metric [IF][comp][ID][nz]
+  // ---- compact metric [IF][comp][ID][nz]: on the host, or on the device
+  // (k_compact_metric, the same expressions) when the reference-layout
+  // metric is device memory
   const size_t ENL = (size_t)DoF * nz * NF;
-  std::vector<double> met(ENL * NCOMP);
+  const bool dev_metric = is_device_ptr(dXdxI) && is_device_ptr(J) && is_device_ptr(X);
+  std::vector<double> met(dev_metric ? 0 : ENL * NCOMP);
   const double Omega2 = 2.0 * cfg->Omega;
-  for (int IF = 0; IF < NF; ++IF)
+  for (int IF = 0; IF < (dev_metric ? 0 : NF); ++IF)
     for (int ID = 0; ID < DoF; ++ID)
       for (int Iz = 0; Iz < nz; ++Iz) {
         auto dx = [&](int a, int b, int K) {
@@ -703,15 +706,6 @@ static int create_impl(const cgd_config *cfg, const int64_t *glob, const double 
         for (int c = 0; c < NCOMP; ++c) met[(((size_t)IF * NCOMP + c) * DoF + ID) * nz + Iz] = v[c];
       }
 
-  // ---- the same metric level-major [IF][lev][comp][ID] (blocks of LVB doubles)
-  const int LVB = (NCOMP * DoF + 1) & ~1;
-  std::vector<double> met2((size_t)NF * nz * LVB, 0.0);
-  for (int IF = 0; IF < NF; ++IF)
-    for (int c = 0; c < NCOMP; ++c)
-      for (int ID = 0; ID < DoF; ++ID)
-        for (int Iz = 0; Iz < nz; ++Iz)
-          met2[((size_t)IF * nz + Iz) * LVB + (size_t)c * DoF + ID] = met[(((size_t)IF * NCOMP + c) * DoF + ID) * nz + Iz];
-
   // ---- device resources
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->order_ev, cudaEventDisableTiming) != cudaSuccess) {
@@ -722,21 +716,7 @@ static int create_impl(const cgd_config *cfg, const int64_t *glob, const double 
   }
   const size_t S = (size_t)nz * NumG;
 #define TRY(x) do { int r_ = (x); if (r_) { cgd_destroy(h); return r_; } } while (0)
-  TRY(dalloc(h, &h->met, met.size()));
-  TRY(dalloc(h, &h->met2, met2.size()));
-  {
-    void *hp = nullptr, *dp = nullptr;
-    if (cudaHostAlloc(&hp, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
-        cudaHostGetDevicePointer(&dp, hp, 0) != cudaSuccess) {
-      cuda_fail(h, cudaGetLastError(), "cgd_create error flag");
-      if (hp) cudaFreeHost(hp);
-      cgd_destroy(h);
-      return CGD_ERR_CUDA;
-    }
-    h->err_host = static_cast<int *>(hp);
-    h->err_dev = static_cast<int *>(dp);
-    *h->err_host = 0;
-  }
+  TRY(dalloc(h, &h->met, ENL * NCOMP));
   TRY(dalloc(h, &h->M, 2 * S));
   TRY(dalloc(h, &h->dz, S));
   TRY(dalloc(h, &h->glob, glob0.size()));
@@ -767,10 +747,15 @@ static int create_impl(const cgd_config *cfg, const int64_t *glob, const double 
   TRY(dalloc(h, &h->scal, 4));
   TRY(dalloc(h, &h->mmass, S));
   TRY(dalloc(h, &h->flag, 4));
+  // host or device sources (unified addressing tells them apart)
   auto up = [&](void *dst, const void *src, size_t bytes) {
-    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, h->stream);
   };
-  if (up(h->met, met.data(), met.size() * 8) || up(h->met2, met2.data(), met2.size() * 8) || up(h->M, M, 2 * S * 8) || up(h->dz, dz, S * 8) ||
+  if (dev_metric) {
+    const long long n = (long long)ENL;
+    k_compact_metric<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(DoF, nz, NF, Omega2, dXdxI, J, X, h->met);
+  }
+  if ((!dev_metric && up(h->met, met.data(), met.size() * 8)) || cudaGetLastError() != cudaSuccess || up(h->M, M, 2 * S * 8) || up(h->dz, dz, S * 8) ||
       up(h->glob, glob0.data(), glob0.size() * 4) || up(h->inv_ptr, ptr.data(), ptr.size() * 4) ||
       up(h->inv_off, off.data(), off.size() * 8) ||
       (halo && nsend && up(h->send_list, halo->send_list, (size_t)nsend * 4))) {
@@ -787,7 +772,7 @@ static int create_impl(const cgd_config *cfg, const int64_t *glob, const double 
 
   GP &P = h->gp;
   P.N = N; P.DoF = DoF; P.nz = nz; P.NF = NF; P.NumG = NumG; P.NumTr = h->NumTr; P.NV = NV; P.NC = NV + 1;
-  P.met = h->met; P.met2 = h->met2; P.met2_lvb = LVB; P.err = h->err_dev; P.M = h->M; P.dz = h->dz; P.glob = h->glob; P.inv_ptr = h->inv_ptr; P.inv_off = h->inv_off;
+  P.met = h->met; P.M = h->M; P.dz = h->dz; P.glob = h->glob; P.inv_ptr = h->inv_ptr; P.inv_off = h->inv_off;
   P.pref = h->pref; P.thref = h->thref;
   for (int i = 0; i < 25; ++i) { P.D[i] = 0.0; P.DW[i] = 0.0; }
   for (int i = 0; i < N * N; ++i) { P.D[i] = DS[i]; P.DW[i] = DW[i]; }
@@ -821,7 +806,6 @@ void cgd_destroy(cgd_handle *h)
   if (h->stream) cudaStreamSynchronize(h->stream);
   free_graph(h);
   for (auto &b : h->bufs) cudaFree(b.p);
-  if (h->err_host) cudaFreeHost(h->err_host);
   for (void *q : h->work_tape.mem) cudaFree(q);
   for (auto &t : h->tapes)
     for (void *q : t.mem) cudaFree(q);
@@ -853,25 +837,11 @@ static int stage_in(cgd_handle *h, const double *p, double *buf, bool copy, doub
   return CGD_OK;
 }
 
-// 0, or CGD_ERR_TIMEOUT once if a kernel's bounded wait gave up since the
-// last check (the flag is cleared)
-static int take_err(cgd_handle *h)
-{
-  if (h->err_host && *reinterpret_cast<volatile int *>(h->err_host)) {
-    *reinterpret_cast<volatile int *>(h->err_host) = 0;
-    const char *m = "a kernel's bounded wait for its metric copy gave up";
-    g_last_error = m;
-    h->last_error = m;
-    return CGD_ERR_TIMEOUT;
-  }
-  return CGD_OK;
-}
-
 static int finish(cgd_handle *h)
 {
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->stream));
-  return take_err(h);
+  return CGD_OK;
 }
 
 int cgd_prepare(cgd_handle *h, const double *U, double *p)
@@ -1083,6 +1053,79 @@ int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps)
   return CGD_OK;
 }
 
+int cgd_metric_sphere(int32_t OrdPoly, int32_t nz, int32_t NF, const double *FP, const double *xw, const double *DS,
+                      const double *z, double H, double Rad, double *X, double *dXdxI, double *J)
+{
+  cgd_handle *h = nullptr;   // for CK(): errors are reported through g_last_error
+  if (OrdPoly < 1 || OrdPoly > 4 || nz < 1 || NF < 1) return CGD_ERR_UNSUPPORTED;
+  if (!FP || !xw || !DS || !z || !X || !dXdxI || !J || !(H > 0) || !(Rad > 0)) return CGD_ERR_INVALID_ARG;
+  if (!is_device_ptr(X) || !is_device_ptr(dXdxI) || !is_device_ptr(J)) return CGD_ERR_INVALID_ARG;
+  const int N = OrdPoly + 1;
+  const size_t nfp = (size_t)NF * 12, nin = nfp + N + N * N + nz + 1;
+  double *buf = nullptr;
+  CK(cudaMalloc(&buf, nin * sizeof(double)));
+  double *dFP = buf, *dxw = dFP + nfp, *dDS = dxw + N, *dz = dDS + N * N;
+  cudaError_t e = cudaMemcpy(dFP, FP, nfp * 8, cudaMemcpyDefault);
+  if (e == cudaSuccess) e = cudaMemcpy(dxw, xw, (size_t)N * 8, cudaMemcpyDefault);
+  if (e == cudaSuccess) e = cudaMemcpy(dDS, DS, (size_t)N * N * 8, cudaMemcpyDefault);
+  if (e == cudaSuccess) e = cudaMemcpy(dz, z, (size_t)(nz + 1) * 8, cudaMemcpyDefault);
+  if (e == cudaSuccess) {
+    const long long n = (long long)NF * N * N;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    switch (N) {
+      case 2: k_metric_sphere<2><<<nb, 256>>>(nz, NF, dFP, dxw, dDS, dz, H, Rad, X, dXdxI, J); break;
+      case 3: k_metric_sphere<3><<<nb, 256>>>(nz, NF, dFP, dxw, dDS, dz, H, Rad, X, dXdxI, J); break;
+      case 4: k_metric_sphere<4><<<nb, 256>>>(nz, NF, dFP, dxw, dDS, dz, H, Rad, X, dXdxI, J); break;
+      default: k_metric_sphere<5><<<nb, 256>>>(nz, NF, dFP, dxw, dDS, dz, H, Rad, X, dXdxI, J); break;
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  }
+  cudaFree(buf);
+  if (e != cudaSuccess) return cuda_fail(h, e, "cgd_metric_sphere");
+  return CGD_OK;
+}
+
+int cgd_mass_dz(int32_t OrdPoly, int32_t nz, int32_t NF, int32_t NumG, const int64_t *glob, const double *w,
+                const double *J, const double *X, double *M, double *MMass, double *dz)
+{
+  cgd_handle *h = nullptr;
+  if (OrdPoly < 1 || OrdPoly > 4 || nz < 1 || NF < 1 || NumG < 1) return CGD_ERR_UNSUPPORTED;
+  if (!glob || !w || !J || !X || !M || !MMass || !dz) return CGD_ERR_INVALID_ARG;
+  if (!is_device_ptr(J) || !is_device_ptr(X) || !is_device_ptr(M) || !is_device_ptr(MMass) || !is_device_ptr(dz))
+    return CGD_ERR_INVALID_ARG;
+  const int N = OrdPoly + 1, DoF = N * N;
+  // contributors of each DOF in ascending (element, node) order
+  std::vector<int> ptr(NumG + 1, 0), idx((size_t)DoF * NF);
+  for (size_t i = 0; i < (size_t)DoF * NF; ++i) {
+    const int64_t g = glob[i];
+    if (g < 1 || g > NumG) return CGD_ERR_INDEX;
+    ptr[g] += 1;
+  }
+  for (int g = 0; g < NumG; ++g) {
+    if (ptr[g + 1] == 0) return CGD_ERR_INDEX;
+    ptr[g + 1] += ptr[g];
+  }
+  std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+  for (size_t i = 0; i < (size_t)DoF * NF; ++i) idx[fill[glob[i] - 1]++] = (int)i;   // i = IF*DoF + ID, ascending
+  int *dptr = nullptr;
+  CK(cudaMalloc(&dptr, (ptr.size() + idx.size() + 1) * sizeof(int) + (size_t)N * sizeof(double)));
+  int *didx = dptr + ptr.size();
+  double *dw = reinterpret_cast<double *>(didx + idx.size() + (idx.size() + ptr.size()) % 2);
+  cudaError_t e = cudaMemcpy(dptr, ptr.data(), ptr.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(didx, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dw, w, (size_t)N * 8, cudaMemcpyDefault);
+  if (e == cudaSuccess) {
+    const long long n = (long long)nz * NumG;
+    k_mass_dz<<<(unsigned)((n + 255) / 256), 256>>>(N, nz, NumG, dptr, didx, dw, J, X, M, MMass, dz);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  }
+  cudaFree(dptr);
+  if (e != cudaSuccess) return cuda_fail(h, e, "cgd_mass_dz");
+  return CGD_OK;
+}
+
 int cgd_set_exchange(cgd_handle *h, cgd_exchange_fn fn, void *user)
 {
   if (!h || !h->decomposed) return CGD_ERR_INVALID_ARG;
@@ -1140,10 +1183,7 @@ static int group_leave(cgd_handle *const *parts, int32_t n, const std::vector<cu
 {
   for (int r = 0; r < n && r < (int)saved.size(); ++r) parts[r]->stream = saved[r];
   if (rc) return rc;
-  int out = finish(parts[0]);
-  for (int r = 1; r < n; ++r)
-    if (int e = take_err(parts[r])) out = out ? out : e;
-  return out;
+  return finish(parts[0]);
 }
 
 int cgd_group_rhs(cgd_handle *const *parts, int32_t n, const double *const *U, double *const *F)
@@ -2045,10 +2085,7 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
     g_last_error = "cgd_batch_step: a fused stage launch timed out at a grid barrier";
     return CGD_ERR_TIMEOUT;
   }
-  int werr = CGD_OK;
-  for (int m = 0; m < nm; ++m)
-    if (int e = take_err(b->mem[m])) werr = e;   // clears every member's flag
-  return werr;
+  return CGD_OK;
 }
 
 int cgd_grid_barrier_check(int32_t rounds, int32_t absent, double limit_s, int32_t *violations)

@@ -58,6 +58,20 @@ __device__ __forceinline__ float rsum2(float acc, float c1, float x1, float c2, 
   return __fmaf_rn(c1, x1, __fmaf_rn(c2, x2, acc));
 }
 
+// 8- and 4-byte asynchronous copies global -> shared (cp.async, sm_80 and
+// later) and the wait for all of a thread's copies
+__device__ __forceinline__ void cp_async8(double *smem_dst, const double *gsrc)
+{
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async4(float *smem_dst, const float *gsrc)
+{
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 constexpr int NCOMP = 21;
 enum {
   C_D11_0 = 0, C_D11_1, C_D12_0, C_D12_1, C_D21_0, C_D21_1, C_D22_0, C_D22_1,
@@ -74,12 +88,6 @@ struct GP {
   int N, DoF, nz, NF, NumG, NumTr, NV;
   int NC;                   // contribution slots per element node: NV fields + the lower-node w of phase 2
   const double *met;        // [IF][comp][ID][nz]
-  // the same metric level-major for the tendency kernel: [IF][lev][comp][ID],
-  // one block of met2_lvb doubles (a multiple of 16 bytes) per element level,
-  // so the levels a tendency CTA reads are one contiguous 16-byte-aligned range
-  const double *met2;
-  int met2_lvb;
-  int *err;                 // set by a kernel whose bounded wait gave up (host-mapped)
   const double *M;          // (nz, NumG, 2)
   const double *dz;         // (nz, NumG)
   const int *glob;          // [IF*DoF + ID], 0-based
@@ -437,8 +445,10 @@ struct ColArgs {
 };
 
 constexpr int COL_WARPS = 8;
-// per warp: fv of rho, w, rho*theta, 8 bands, tri[3], x; each nz long
-constexpr int COL_ARR = 15;
+// per warp: fv of rho, w, rho*theta, 8 bands, tri[3], x, and the step's
+// initial rho, w, rho*theta (copied in asynchronously at the start and read
+// by the stage update at the end); each nz long
+constexpr int COL_ARR = 18;
 
 // dPresdRhoTh (src/Models/Equation.jl:33-36) of one level
 __device__ __forceinline__ double dpdrhoth(const GP &P, double RhoTh0)
@@ -587,6 +597,7 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
   double *jb = sw + 3 * LS;             // [8][nz]
   double *tri = jb + 8 * LS;            // [3][nz]
   double *xs = tri + 3 * LS;            // [nz]
+  double *vns = xs + LS;                // [3][nz]: Vn of rho, w, rho*theta
   const size_t fs = (size_t)nz * NumG;
   const double fac = A.fac;
   // k1, k2 of the Schur fields (rho, w, rho*theta), kept for the update
@@ -600,6 +611,10 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
     if (!valid || l >= nz) continue;
     const size_t o0 = l + (size_t)nz * g;
     if (MODE <= 2) {
+      // the step's initial rho, w, rho*theta for the update at the end, in flight meanwhile
+      cp_async8(vns + l, A.Vn + o0);
+      cp_async8(vns + LS + l, A.Vn + o0 + 3 * fs);
+      cp_async8(vns + 2 * LS + l, A.Vn + o0 + 4 * fs);
       const size_t fstr = (size_t)P.DoF * nz;
       double gacc[MAXNV];
       gather_node<true, C32>(P, A.C, g, l, fstr, gacc);
@@ -734,6 +749,7 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
   __syncthreads();
 #endif
   if (!valid) return;
+  if (MODE <= 2) cp_async_wait_all();   // this lane's copies of Vn (its own levels only)
   // SchurSolveBKernel! and the stage update of rho, w, rho*theta; each lane
   // owns levels lane and lane + 32
 #pragma unroll
@@ -767,16 +783,16 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
       const size_t o = o0 + f * fs;
       const double k = kk[sf];
       if (MODE == 0) {
-        const double vn = A.Vn[o];
+        const double vn = vns[sf * LS + l];
         A.kout[o] = k;
         A.Vout[o] = vn + A.rk.a[1][0] * k;
       } else if (MODE == 1) {
-        const double vn = A.Vn[o];
+        const double vn = vns[sf * LS + l];
         A.kout[o] = k;
         A.Vout[o] = vn + A.rk.a[2][0] * s1[it][sf] + A.rk.a[2][1] * k;
       } else if (MODE == 2) {
-        // Vout may alias Vn: this lane alone reads and writes index o
-        const double vn = A.Vn[o];
+        // Vout may alias Vn: this lane alone read index o (at the start) and writes it
+        const double vn = vns[sf * LS + l];
         A.Vout[o] = vn + A.rk.m[0] * s1[it][sf] + A.rk.m[1] * s2[it][sf] + A.rk.m[2] * k;
         if (A.kout) A.kout[o] = k;   // the last stage's k of rho, w, rho*theta (adjoint replay only)
       } else {

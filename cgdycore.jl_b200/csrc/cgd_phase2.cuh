@@ -3,21 +3,14 @@
 // One CTA per (element, chunk of LC levels); inside it one warp per level
 // (N = 5: lanes 0..24 are the 25 nodes; for smaller N a warp holds
 // LPW = 32 / N^2 levels).  Grid: (chunks, elements), chunks fastest so the
-// chunks of one element, which share their halo levels, run together.
+// chunks of one element, which share their halo planes, run together.
 //
 // The number of tracers NT is a template parameter.
 //
-//   1. One thread starts a bulk asynchronous copy (cp.async.bulk, completing
-//      on an mbarrier) of the element's metric at the levels L0-1 .. L0+LC:
-//      the level-major metric (GP::met2) keeps every component of a level in
-//      one 16-byte-aligned block, so these levels are one contiguous range.
-//      Meanwhile every thread stages the pointwise state of its LC levels
-//      plus two halo planes on each side (state, lumped mass, pressure -
+//   1. The CTA stages the pointwise quantities of its LC levels plus two halo
+//      planes on each side (state, vertical metric, lumped mass, pressure -
 //      computed beforehand, once per column-level, by the kernel that forms
-//      the state - then theta and tracer ratios) with 8-byte cp.async: the
-//      state is indexed by global DOF, so its rows are scattered.  The wait
-//      for the metric is bounded; a copy that does not land in time sets
-//      GP::err and the CTA leaves.
+//      the state - theta and tracer ratios) in shared memory.  One barrier.
 //   2. One thread per (node, interface) forms the vertical mass flux and the
 //      limited upwind fluxes of the interfaces L0-1 .. L0+LC-1 (the one below
 //      the chunk is formed by both neighbouring chunks, with identical
@@ -41,68 +34,19 @@
 
 namespace cgd {
 
-// pointwise state quantities staged per (plane, node)
+// pointwise quantities per (plane, node)
 enum {
-  Q_RHO = 0, Q_U, Q_V, Q_W, Q_M0, Q_M1, Q_P, Q_CTH,
+  Q_RHO = 0, Q_U, Q_V, Q_W, Q_D310, Q_D311, Q_D320, Q_D321, Q_D330, Q_D331,
+  Q_M0, Q_M1, Q_P, Q_J0, Q_CTH,
   Q_TR0   // + one per tracer: rho*q / rho
 };
 
-// 8-byte asynchronous copy global -> shared (cp.async, sm_80 and later) and
-// the wait for all of a thread's copies
-__device__ __forceinline__ void cp_async8(double *smem_dst, const double *gsrc)
-{
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// Bulk copy global -> shared through the tensor-memory-access unit, completing
-// on an mbarrier (sm_90 and later; this GPU's own memory only, no multicast).
-// Addresses 16-byte aligned, size a multiple of 16 bytes.
-__device__ __forceinline__ void mbar_init(uint64_t *mb, unsigned count)
-{
-  const unsigned a = (unsigned)__cvta_generic_to_shared(mb);
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(a), "r"(count) : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-}
-__device__ __forceinline__ void mbar_inval(uint64_t *mb)
-{
-  const unsigned a = (unsigned)__cvta_generic_to_shared(mb);
-  asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(a) : "memory");
-}
-__device__ __forceinline__ void bulk_load(void *smem_dst, const void *gsrc, unsigned bytes, uint64_t *mb)
-{
-  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-  const unsigned a = (unsigned)__cvta_generic_to_shared(mb);
-  // order earlier generic-proxy accesses of this CTA's shared memory before
-  // the asynchronous writes
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(a), "r"(bytes) : "memory");
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(d),
-               "l"(gsrc), "r"(bytes), "r"(a)
-               : "memory");
-}
-// Wait for phase `parity` of the mbarrier; bounded by ~1 s of %globaltimer
-// and 2^22 polls.  False if the wait gave up.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *mb, unsigned parity)
-{
-  const unsigned a = (unsigned)__cvta_generic_to_shared(mb);
-  unsigned long long t0;
-  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t0));
-  for (unsigned it = 0; it < (1u << 22); ++it) {
-    unsigned done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
-    if (t - t0 > 1000000000ull) break;
-  }
-  return false;
-}
+// quantities of the CTA's own levels per (level, node)
+enum {
+  O_D110 = 0, O_D111, O_D120, O_D121, O_D210, O_D211, O_D220, O_D221, O_J1, O_FC,
+  O_N     // the DSS'd hyperviscosity cache (5 + NumTr fields) has an array of its own, stored like T1
+};
 
 // Warps (levels for p = 4) per CTA: 8, two 256-thread CTAs per SM at 128
 // registers a thread, so that one CTA's staging overlaps the other's
@@ -116,21 +60,18 @@ struct P2Cfg {
   static constexpr int DoF = N * N;
   static constexpr int LPW = 32 / DoF;           // levels per warp
   static constexpr int LC = WARPS * LPW;         // levels per CTA
-  static constexpr int RP = LC + 4;              // staged state planes
-  static constexpr int ML = LC + 2;              // staged metric levels (L0-1 .. L0+LC)
-  static constexpr int LVB = (NCOMP * DoF + 1) & ~1;   // doubles per level block of the level-major metric
-  static constexpr int NQ = Q_TR0 + NT;          // staged state quantities
+  static constexpr int RP = LC + 4;              // staged planes
   static constexpr int THREADS = 32 * WARPS;
   // scratch quantities per warp (the largest derivative round: 5+NT, 4+2NT,
   // 6 for each half of the momentum round, 6+NT) and the scratch row length
   static constexpr int NSCR = (4 + 2 * NT) > (6 + NT) ? (4 + 2 * NT) : (6 + NT);
   static constexpr int SCS = LPW * DoF;
-  static constexpr size_t SCR_BYTES = ((size_t)WARPS * NSCR * SCS * sizeof(R) + 15) & ~(size_t)15;
-  // metric block first (16-byte aligned), state planes, own-level cache,
-  // interface fluxes, scratch; +16 for aligning the dynamic buffer
-  static constexpr size_t SMEM = ((size_t)ML * LVB + (size_t)NQ * RP * DoF + (size_t)(5 + NT) * LC * DoF +
-                                  (size_t)(2 + NT) * (LC + 1) * DoF) * sizeof(double) +
-                                 SCR_BYTES + 16;
+  // the own levels' phase-1 cache: float in the mixed form (as stored), else double
+  using CT = typename std::conditional<sizeof(R) == sizeof(float), float, double>::type;
+  static constexpr size_t SMEM = ((size_t)(Q_TR0 + NT) * RP * DoF + (size_t)O_N * LC * DoF +
+                                   (size_t)(2 + NT) * (LC + 1) * DoF) * sizeof(double) +
+                                  (size_t)(5 + NT) * LC * DoF * sizeof(CT) +
+                                  (size_t)WARPS * NSCR * SCS * sizeof(R);
 };
 
 template <int N, int NT, typename R, int W = 0>
@@ -140,33 +81,25 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
 {
   using CF = P2Cfg<N, NT, R, W>;
   constexpr bool MIX = sizeof(R) == sizeof(float);
-  constexpr int DoF = CF::DoF, LPW = CF::LPW, LC = CF::LC, RP = CF::RP, LVB = CF::LVB;
+  constexpr int DoF = CF::DoF, LPW = CF::LPW, LC = CF::LC, RP = CF::RP;
   extern __shared__ double sm[];
-  __shared__ uint64_t p2_mbar;
   const int nz = P.nz, NumG = P.NumG;
   const int L0 = chunk * LC;
   const size_t cs = (size_t)DoF * nz, fs = (size_t)nz * NumG;
-  // dynamic buffer aligned to 16 bytes for the bulk copy
-  double *mts = reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(sm) + 15) & ~(uintptr_t)15);   // [lev][comp][ID]
-  double *pw = mts + (size_t)CF::ML * LVB;                         // [Q][R][DoF]
-  double *ow = pw + (size_t)CF::NQ * RP * DoF;                     // [5+NT][LC][DoF] own levels' DSS'd cache
-  double *fx = ow + (size_t)(5 + NT) * LC * DoF;                   // [2+NT][LC+1][DoF] interface fluxes
-  R *scr = (R *)(fx + (size_t)(2 + NT) * (LC + 1) * DoF);          // [warp][NSCR][SCS]
-  // metric levels lo .. hi of this chunk (the halo levels L0-1 and L0+LC where they exist)
-  const int mlo = L0 > 0 ? L0 - 1 : 0;
-  const int mhi = L0 + LC < nz - 1 ? L0 + LC : nz - 1;
+  double *pw = sm;                                             // [Q][R][DoF]
+  using CTc = typename CF::CT;
+  double *ow = pw + (size_t)(Q_TR0 + NT) * RP * DoF;             // [O][LC][DoF]
+  double *fx = ow + (size_t)O_N * LC * DoF;                     // [2+NT][LC+1][DoF] interface fluxes
+  CTc *otc = reinterpret_cast<CTc *>(fx + (size_t)(2 + NT) * (LC + 1) * DoF);   // [5+NT][LC][DoF] cache
+  R *scr = reinterpret_cast<R *>(otc + (size_t)(5 + NT) * LC * DoF);            // [warp][NSCR][SCS]
+  const double *mte = P.met + (size_t)IF * NCOMP * cs;
 #define PW(q, p, id) pw[((size_t)(q) * RP + (p)) * DoF + (id)]
-#define MT(c, lev, id) mts[((lev) - mlo) * LVB + (c) * DoF + (id)]
 
-  // ---------------- 1. stage: metric by one bulk copy, state by cp.async ----------------
-  if (threadIdx.x == 0) {
-    mbar_init(&p2_mbar, 1);
-    bulk_load(mts, P.met2 + ((size_t)IF * nz + mlo) * LVB, (unsigned)((mhi - mlo + 1) * LVB * sizeof(double)),
-              &p2_mbar);
-  }
-  // state planes L0-2 .. L0+LC+1 (level fastest: every load is a run of
-  // consecutive levels of one column) and the own levels' cache; at most two
-  // slots per thread (DoF * RP <= 2 * THREADS)
+  // ---------------- 1. stage the pointwise planes L0-2 .. L0+LC+1 ----------------
+  // (level fastest: every load is a run of consecutive levels of one column
+  // or one metric row) and the own levels' metric and cache
+  // at most two slots per thread (DoF * RP <= 2 * THREADS); every value is
+  // copied with cp.async, so all of a thread's copies are in flight at once
   static_assert(DoF * RP <= 2 * CF::THREADS, "two staging slots per thread");
 #pragma unroll
   for (int r = 0; r < 2; ++r) {
@@ -177,17 +110,25 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
     if (lev < 0 || lev >= nz) continue;
     const int g = P.glob[IF * DoF + ID];
     const double *Ug = U + (size_t)nz * g + lev;
+    const double *mt = mte + (size_t)ID * nz + lev;
     if (p >= 2 && p <= LC + 1) {
       double *o = ow + (size_t)(p - 2) * DoF + ID;
       constexpr size_t os = (size_t)LC * DoF;
-      if (MIX) {   // the mixed form's phase-1 cache is stored as float
+      cp_async8(o + O_D110 * os, mt + C_D11_0 * cs); cp_async8(o + O_D111 * os, mt + C_D11_1 * cs);
+      cp_async8(o + O_D120 * os, mt + C_D12_0 * cs); cp_async8(o + O_D121 * os, mt + C_D12_1 * cs);
+      cp_async8(o + O_D210 * os, mt + C_D21_0 * cs); cp_async8(o + O_D211 * os, mt + C_D21_1 * cs);
+      cp_async8(o + O_D220 * os, mt + C_D22_0 * cs); cp_async8(o + O_D221 * os, mt + C_D22_1 * cs);
+      cp_async8(o + O_J1 * os, mt + C_J1 * cs);
+      cp_async8(o + O_FC * os, mt + C_FCOR * cs);
+      CTc *oc = otc + (size_t)(p - 2) * DoF + ID;
+      if (MIX) {   // the mixed form's phase-1 cache is stored as float, and staged as float
         const float *T = reinterpret_cast<const float *>(T1) + (size_t)nz * g + lev;
 #pragma unroll
-        for (int f = 0; f < 5 + NT; ++f) o[f * os] = (double)T[f * fs];
+        for (int f = 0; f < 5 + NT; ++f) cp_async4(reinterpret_cast<float *>(oc) + f * os, T + f * fs);
       } else {
         const double *T = T1 + (size_t)nz * g + lev;
 #pragma unroll
-        for (int f = 0; f < 5 + NT; ++f) cp_async8(o + f * os, T + f * fs);
+        for (int f = 0; f < 5 + NT; ++f) cp_async8(reinterpret_cast<double *>(oc) + f * os, T + f * fs);
       }
     }
     cp_async8(&PW(Q_RHO, p, ID), Ug);
@@ -198,6 +139,10 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
     cp_async8(&PW(Q_U, p, ID), Ug + fs);
     cp_async8(&PW(Q_V, p, ID), Ug + 2 * fs);
     cp_async8(&PW(Q_W, p, ID), Ug + 3 * fs);
+    cp_async8(&PW(Q_D310, p, ID), mt + C_D31_0 * cs); cp_async8(&PW(Q_D311, p, ID), mt + C_D31_1 * cs);
+    cp_async8(&PW(Q_D320, p, ID), mt + C_D32_0 * cs); cp_async8(&PW(Q_D321, p, ID), mt + C_D32_1 * cs);
+    cp_async8(&PW(Q_D330, p, ID), mt + C_D33_0 * cs); cp_async8(&PW(Q_D331, p, ID), mt + C_D33_1 * cs);
+    cp_async8(&PW(Q_J0, p, ID), mt + C_J0 * cs);
     cp_async8(&PW(Q_M0, p, ID), P.M + lev + (size_t)nz * g);
     cp_async8(&PW(Q_M1, p, ID), P.M + lev + (size_t)nz * (g + (size_t)NumG));
     cp_async8(&PW(Q_P, p, ID), Pr + lev + (size_t)nz * g);
@@ -217,16 +162,7 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
 #pragma unroll
     for (int q = 0; q < NT; ++q) PW(Q_TR0 + q, p, ID) = PW(Q_TR0 + q, p, ID) / rho;
   }
-  // the metric copy: every thread waits (bounded), then all agree
-  const bool landed = mbar_wait_bounded(&p2_mbar, 0);
-  if (__syncthreads_or(!landed)) {
-    if (threadIdx.x == 0) {
-      atomicExch(P.err, 1);
-      mbar_wait_bounded(&p2_mbar, 0);   // a last bounded wait for the copy in flight
-    }
-    return;
-  }
-  if (threadIdx.x == 0) mbar_inval(&p2_mbar);
+  __syncthreads();
 
   // ---------------- 2. interface fluxes ----------------
   // wCon and the limited upwind fluxes (RecU4, OperatorKernel.jl:1044-1059,
@@ -239,11 +175,12 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
     const int pl = i + 1;   // plane of level il
     const double wI = PW(Q_W, pl, ID);
     const double wCon =
-        PW(Q_RHO, pl, ID) * (MT(C_D31_1, il, ID) * PW(Q_U, pl, ID) + MT(C_D32_1, il, ID) * PW(Q_V, pl, ID) +
-                             MT(C_D33_1, il, ID) * wI) +
-        PW(Q_RHO, pl + 1, ID) * (MT(C_D31_0, il + 1, ID) * PW(Q_U, pl + 1, ID) +
-                                 MT(C_D32_0, il + 1, ID) * PW(Q_V, pl + 1, ID) + MT(C_D33_0, il + 1, ID) * wI);
-    const double kR1 = MT(C_RK0, il, ID), kL1 = MT(C_RK1, il, ID), kL2 = MT(C_RK2, il, ID), kR2 = MT(C_RK3, il, ID);
+        PW(Q_RHO, pl, ID) * (PW(Q_D311, pl, ID) * PW(Q_U, pl, ID) + PW(Q_D321, pl, ID) * PW(Q_V, pl, ID) +
+                             PW(Q_D331, pl, ID) * wI) +
+        PW(Q_RHO, pl + 1, ID) * (PW(Q_D310, pl + 1, ID) * PW(Q_U, pl + 1, ID) +
+                                 PW(Q_D320, pl + 1, ID) * PW(Q_V, pl + 1, ID) + PW(Q_D330, pl + 1, ID) * wI);
+    const double *mt = mte + (size_t)ID * nz + il;
+    const double kR1 = mt[C_RK0 * cs], kL1 = mt[C_RK1 * cs], kL2 = mt[C_RK2 * cs], kR2 = mt[C_RK3 * cs];
     const int pm = il > 0 ? pl - 1 : pl, pp2 = il + 2 < nz ? pl + 2 : pl + 1;
     const double aw = fabs(wCon);
     auto upwind = [&](int q) {
@@ -282,15 +219,16 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   }
   // own quantities
   const int li = lv - L0;                // own row of the per-level arrays
-#define OT(f) ow[((size_t)(f) * LC + li) * DoF + ID]   // own level's DSS'd phase-1 cache
+#define OW(q) ow[((size_t)(q) * LC + li) * DoF + ID]
+#define OT(f) otc[((size_t)(f) * LC + li) * DoF + ID]   // own level's DSS'd phase-1 cache
   double rho = 1, u = 0, v = 0, wl = 0, wh = 0, M0 = 1, M1 = 0, MC = 1, Js = 1, J0 = 0, J1 = 0;
   double e310 = 0, e311 = 0, e320 = 0, e321 = 0, e330 = 1, e331 = 1;
   if (act) {
-    J1 = MT(C_J1, lv, ID);
+    J1 = OW(O_J1);
     rho = PW(Q_RHO, p0, ID); u = PW(Q_U, p0, ID); v = PW(Q_V, p0, ID); wh = PW(Q_W, p0, ID);
-    e310 = MT(C_D31_0, lv, ID); e311 = MT(C_D31_1, lv, ID); e320 = MT(C_D32_0, lv, ID);
-    e321 = MT(C_D32_1, lv, ID); e330 = MT(C_D33_0, lv, ID); e331 = MT(C_D33_1, lv, ID);
-    J0 = MT(C_J0, lv, ID);
+    e310 = PW(Q_D310, p0, ID); e311 = PW(Q_D311, p0, ID); e320 = PW(Q_D320, p0, ID);
+    e321 = PW(Q_D321, p0, ID); e330 = PW(Q_D330, p0, ID); e331 = PW(Q_D331, p0, ID);
+    J0 = PW(Q_J0, p0, ID);
     M0 = PW(Q_M0, p0, ID); M1 = PW(Q_M1, p0, ID);
     Js = J0 + J1;
     MC = M0 + M1;
@@ -300,10 +238,10 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   const double rJs = 1.0 / Js, rMC = 1.0 / MC;
   (void)rJs; (void)rMC;
   // the horizontal metric of the own level, re-read from shared memory where used
-#define D11 (MT(C_D11_0, lv, ID) + MT(C_D11_1, lv, ID))
-#define D12 (MT(C_D12_0, lv, ID) + MT(C_D12_1, lv, ID))
-#define D21 (MT(C_D21_0, lv, ID) + MT(C_D21_1, lv, ID))
-#define D22 (MT(C_D22_0, lv, ID) + MT(C_D22_1, lv, ID))
+#define D11 (OW(O_D110) + OW(O_D111))
+#define D12 (OW(O_D120) + OW(O_D121))
+#define D21 (OW(O_D210) + OW(O_D211))
+#define D22 (OW(O_D220) + OW(O_D221))
 
   // ---- round 1: first derivatives of the DSS'd hyperviscosity cache ----
   if (act) {
@@ -428,8 +366,8 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   const double tw0 = e320 * u - e310 * v, tw1 = e321 * u - e311 * v;
   R U1 = 0, U2 = 0, V1 = 0, V2 = 0, W1 = 0, W2 = 0;
   if (act) {
-    const R d110 = (R)MT(C_D11_0, lv, ID), d111 = (R)MT(C_D11_1, lv, ID), d120 = (R)MT(C_D12_0, lv, ID), d121 = (R)MT(C_D12_1, lv, ID);
-    const R d210 = (R)MT(C_D21_0, lv, ID), d220 = (R)MT(C_D22_0, lv, ID), d221 = (R)MT(C_D22_1, lv, ID);
+    const R d110 = (R)OW(O_D110), d111 = (R)OW(O_D111), d120 = (R)OW(O_D120), d121 = (R)OW(O_D121);
+    const R d210 = (R)OW(O_D210), d220 = (R)OW(O_D220), d221 = (R)OW(O_D221);
     const R wlR = (R)wl, whR = (R)wh;
     SC(0, ID) = -d120 * wlR;  SC(1, ID) = -d121 * whR;    // tempuZ1
     SC(2, ID) = -d220 * wlR;  SC(3, ID) = -d221 * whR;    // tempuZ2
@@ -451,8 +389,8 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   }
   __syncwarp();
   if (act) {
-    const R d110 = (R)MT(C_D11_0, lv, ID), d111 = (R)MT(C_D11_1, lv, ID), d120 = (R)MT(C_D12_0, lv, ID), d121 = (R)MT(C_D12_1, lv, ID);
-    const R d210 = (R)MT(C_D21_0, lv, ID), d211 = (R)MT(C_D21_1, lv, ID), d220 = (R)MT(C_D22_0, lv, ID), d221 = (R)MT(C_D22_1, lv, ID);
+    const R d110 = (R)OW(O_D110), d111 = (R)OW(O_D111), d120 = (R)OW(O_D120), d121 = (R)OW(O_D121);
+    const R d210 = (R)OW(O_D210), d211 = (R)OW(O_D211), d220 = (R)OW(O_D220), d221 = (R)OW(O_D221);
     const R uR = (R)u, vR = (R)v, whR = (R)wh;
     SC(0, ID) = -d111 * whR;                              // tempvZ1 (upper)
     SC(1, ID) = -d211 * whR;                              // tempvZ2 (upper)
@@ -482,9 +420,9 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
     if (bot) {
       const int pb = p0 - 1;
       const double ub = PW(Q_U, pb, ID), vb = PW(Q_V, pb, ID), wb = PW(Q_W, pb, ID);
-      const double tu1b = MT(C_D33_1, lv - 1, ID) * vb - MT(C_D32_1, lv - 1, ID) * wb;
-      const double tv1b = MT(C_D33_1, lv - 1, ID) * ub - MT(C_D31_1, lv - 1, ID) * wb;
-      const double tw1b = MT(C_D32_1, lv - 1, ID) * ub - MT(C_D31_1, lv - 1, ID) * vb;
+      const double tu1b = PW(Q_D331, pb, ID) * vb - PW(Q_D321, pb, ID) * wb;
+      const double tv1b = PW(Q_D331, pb, ID) * ub - PW(Q_D311, pb, ID) * wb;
+      const double tw1b = PW(Q_D321, pb, ID) * ub - PW(Q_D311, pb, ID) * vb;
       const double FluxUZ = 0.5 * (tu0 - tu1b);
       const double FluxVZ = 0.5 * (tv0 - tv1b);
       const double FluxWZ = 0.5 * (tw0 - tw1b);
@@ -498,9 +436,9 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
       rho1 = PW(Q_RHO, pa, ID);
       const double u1 = PW(Q_U, pa, ID), v1 = PW(Q_V, pa, ID);
       const double wl1 = wh;   // the lower w of level lv+1 is the upper w of lv
-      const double tu0a = MT(C_D33_0, lv + 1, ID) * v1 - MT(C_D32_0, lv + 1, ID) * wl1;
-      const double tv0a = MT(C_D33_0, lv + 1, ID) * u1 - MT(C_D31_0, lv + 1, ID) * wl1;
-      const double tw0a = MT(C_D32_0, lv + 1, ID) * u1 - MT(C_D31_0, lv + 1, ID) * v1;
+      const double tu0a = PW(Q_D330, pa, ID) * v1 - PW(Q_D320, pa, ID) * wl1;
+      const double tv0a = PW(Q_D330, pa, ID) * u1 - PW(Q_D310, pa, ID) * wl1;
+      const double tw0a = PW(Q_D320, pa, ID) * u1 - PW(Q_D310, pa, ID) * v1;
       const double FluxUZt = 0.5 * (tu0a - tu1);
       const double FluxVZt = 0.5 * (tv0a - tv1);
       const double FluxWZt = 0.5 * (tw0a - tw1);
@@ -509,7 +447,7 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
       FW2 += (u * FluxVZt + v * FluxUZt);
       den_hi = rho1 * PW(Q_M0, pa, ID) + rho * M1;
     }
-    const double fc = MT(C_FCOR, lv, ID);
+    const double fc = OW(O_FC);
     const double FuCor = v * fc, FvCor = -u * fc, FwCor = 0.0;
     FU += FuCor * (J0 + J1);
     FV += FvCor * (J0 + J1);
@@ -560,8 +498,8 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
       DXp = rsum1(DXp, DI[k], pa[k + N * Jn]);
       DYp = rsum1(DYp, DJ[k], pa[I + N * k]);
     }
-    const double d110 = MT(C_D11_0, lv, ID), d111 = MT(C_D11_1, lv, ID), d120 = MT(C_D12_0, lv, ID), d121 = MT(C_D12_1, lv, ID);
-    const double d210 = MT(C_D21_0, lv, ID), d211 = MT(C_D21_1, lv, ID), d220 = MT(C_D22_0, lv, ID), d221 = MT(C_D22_1, lv, ID);
+    const double d110 = OW(O_D110), d111 = OW(O_D111), d120 = OW(O_D120), d121 = OW(O_D121);
+    const double d210 = OW(O_D210), d211 = OW(O_D211), d220 = OW(O_D220), d221 = OW(O_D221);
     const double d11 = d110 + d111, d12 = d120 + d121, d21 = d210 + d211, d22 = d220 + d221;
     double GuF1 = -(d110 * DXK1 + d210 * DYK1);
     double GvF1 = -(d120 * DXK1 + d220 * DYK1);
@@ -603,8 +541,8 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
     if (top) {
       const int pa1 = p0 + 1;
       GZ = 0.5 * (PW(Q_P, pa1, ID) - PW(Q_P, p0, ID));
-      const double Gradw = GZ * (e331 + MT(C_D33_0, lv + 1, ID));
-      const double Gradp = -(Gradw + P.Grav * (rho * J1 + rho1 * MT(C_J0, lv + 1, ID)));
+      const double Gradw = GZ * (e331 + PW(Q_D330, pa1, ID));
+      const double Gradp = -(Gradw + P.Grav * (rho * J1 + rho1 * PW(Q_J0, pa1, ID)));
       whi = mwhi + CGD_DIVW(GwF2 + Gradp, den_hi);
     }
     if (bot) {
@@ -656,8 +594,8 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
 #undef D12
 #undef D21
 #undef D22
+#undef OW
 #undef OT
-#undef MT
 #undef SC
 #undef PW
 }

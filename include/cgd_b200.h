@@ -74,7 +74,9 @@ typedef struct cgd_handle cgd_handle;
 
 /* Builds the device-side grid: owner-gather maps from Glob, the compact
  * element metric, lumped mass, dz and the Coriolis parameter at layer
- * midpoints.  Host pointers; nothing is kept after the call.
+ * midpoints.  Host pointers, or device pointers for dXdxI, J, X, M and dz
+ * (e.g. from cgd_metric_sphere / cgd_mass_dz); nothing is kept after the
+ * call.
  * Replaces DyCore.InitSphere's device arrays (src/DyCore/InitDriver.jl:1-55,
  * src/DyCore/DiscretizationCG.jl:1-78) as consumed by the hot path. */
 int cgd_create(const cgd_config *cfg, const int64_t *glob, const double *DS,
@@ -138,6 +140,26 @@ int cgd_halo_buffers(cgd_handle *h, double **send, int64_t *send_doubles, double
  * part's caller stream; returns with the work complete. */
 int cgd_group_rhs(cgd_handle *const *parts, int32_t n, const double *const *U, double *const *F);
 int cgd_group_ros_step(cgd_handle *const *parts, int32_t n, double *const *U, double dt, int32_t nsteps);
+
+/* The grid's floating-point arrays formed on the device (the host keeps the
+ * integer topology and Glob numbering).  Replaces the set-up kernels
+ * JacobiSphere3Kernel! (src/Grids/JacobiSphere3GPU.jl:102-215, shallow
+ * atmosphere, Sleve height at zero orography, src/Grids/Adapt.jl:19-31),
+ * MassCGKernel! (src/DyCore/MassCG.jl:61-75) and GridSizeSphereKernel!
+ * (src/DyCore/DiscretizationCG.jl:119-144).
+ * cgd_metric_sphere: X, dXdxI, J (layouts above; device memory) from the
+ * element corner points FP (NF, 4, 3; row-major), the GLL nodes xw (N),
+ * DS (N, N) and the level heights z (nz + 1), top height H, radius Rad.  The
+ * device's sin/cos/asin/atan2 may differ from a host libm in the last bit.
+ * cgd_mass_dz: M (nz, NumG, 2), MMass (nz, NumG), dz (nz, NumG) (device
+ * memory) from Glob (host), the GLL weights w (N) and the device X and J;
+ * contributors summed in ascending (element, node) order.
+ * cgd_create accepts these device arrays directly and then forms its
+ * element metric on the device too.  Both calls synchronise the device. */
+int cgd_metric_sphere(int32_t OrdPoly, int32_t nz, int32_t NF, const double *FP, const double *xw, const double *DS,
+                      const double *z, double H, double Rad, double *X, double *dXdxI, double *J);
+int cgd_mass_dz(int32_t OrdPoly, int32_t nz, int32_t NF, int32_t NumG, const int64_t *glob, const double *w,
+                const double *J, const double *X, double *M, double *MMass, double *dz);
 
 /* Pressure p (nz, NumG) from the state.
  * Replaces GPU.FcnPrepareGPU! / PressureKernel! (src/GPU/DiagnosticKernel.jl:96-115,180-218). */

@@ -19,6 +19,9 @@ CASES = {
     "p4": dict(nPanel=6, p=4, nz=10, NumTr=0, stretch="uniform"),
     "p3_tracers": dict(nPanel=5, p=3, nz=12, NumTr=2, stretch="quadratic"),
     "p4_nz30": dict(nPanel=8, p=4, nz=30, NumTr=1, stretch="quadratic"),
+    # the mixed form's own configuration, reduced horizontally: p 4, nz 64
+    # stretched quadratically, no tracers (nPanel 60 in the benchmark)
+    "cfg3_shape": dict(nPanel=6, p=4, nz=64, NumTr=0, stretch="quadratic"),
 }
 
 
