@@ -327,14 +327,25 @@ def run_mixed_cfg3(args, rank, ranks, torch):
     simulated days from the same initial state, the lowest-layer pressure
     (surface-pressure proxy) of the mixed form against the FP64 path of the
     same configuration, and the mass drift of both."""
+    from cgd_b200 import grid as G
     from cgd_b200 import setup
     from cgd_b200 import physics as Ph
     cfg = member_config(Ph.CONFIGS["mixed"], rank)
     nsteps = max(1, int(round(args.cfg3_days * 86400.0 / cfg.dt)))
     K = max(3, min(args.steps, 20))
+    # the grid set-up at this size: host (numpy) against device (cgd_metric_sphere, cgd_mass_dz)
+    t0 = time.perf_counter()
+    G.init_grid_sphere(cfg.nPanel, cfg.OrdPoly, cfg.levels(), cfg.H, Ph.PhysParameters().RadEarth)
+    t_host = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    gd = G.init_grid_sphere_device(cfg.nPanel, cfg.OrdPoly, cfg.levels(), cfg.H, Ph.PhysParameters().RadEarth)
+    torch.cuda.synchronize()
+    t_dev = time.perf_counter() - t0
+    del gd
     out = {}
     for prec in ("fp64", "mixed"):
-        d, U0, _ = setup(cfg, precision=prec, check_finite=True)
+        d, U0, _ = setup(cfg, precision=prec, check_finite=True, where="device")
         stream = torch.cuda.ExternalStream(d.stream())
         V = torch.from_numpy(np.ascontiguousarray(U0.transpose(2, 1, 0))).cuda()
         m0 = d.mass_integral(V)
@@ -361,6 +372,9 @@ def run_mixed_cfg3(args, rank, ranks, torch):
                        "dt_note": "dt 150 s (and 60 s, NaN within 60 steps) is beyond the explicit horizontal-acoustics limit of this W-method at "
                                   "nPanel 60 (it halves the grid spacing of nPanel 30, where 150 s already fails); "
                                   "50 s is stable for the simulated day"},
+            "grid_setup_s": {"host": t_host, "device": t_dev,
+                             "what": "metric, mass and dz of the nPanel-60 grid (topology and Glob numbering on the "
+                                     "host in both); the runs below use the device-built grid"},
             "fp64_steps_per_s": out["fp64"]["steps_per_s"], "mixed_steps_per_s": out["mixed"]["steps_per_s"],
             "speedup_vs_fp64": out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"],
             "accuracy": {"simulated_days": nsteps * cfg.dt / 86400.0, "steps": nsteps,

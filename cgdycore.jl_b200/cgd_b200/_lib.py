@@ -33,7 +33,7 @@ EXPORTS = [
     "cgd_batch_create", "cgd_batch_step", "cgd_batch_tuning", "cgd_batch_get_stream", "cgd_batch_destroy",
     "cgd_grid_barrier_check",
     "cgd_create_part", "cgd_set_exchange", "cgd_halo_buffers", "cgd_group_rhs", "cgd_group_ros_step",
-    "cgd_metric_sphere", "cgd_mass_dz",
+    "cgd_metric_sphere", "cgd_mass_dz", "cgd_set_physics",
 ]
 
 
@@ -56,6 +56,12 @@ class CgdHalo(ctypes.Structure):
 # int (*cgd_exchange_fn)(void *user, void *stream, int32_t nf, const double *send, double *recv)
 EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
                                ctypes.c_void_p)
+
+
+class CgdPhysics(ctypes.Structure):
+    _fields_ = [("held_suarez", ctypes.c_int32), ("damping", ctypes.c_int32)] + [
+        (n, ctypes.c_double) for n in ("k_a", "k_f", "k_s", "DeltaT_y", "DeltaTh_z", "T_equator", "T_min",
+                                      "sigma_b", "damp_H", "damp_stride", "damp_relax", "Rad")]
 
 
 class CgdError(RuntimeError):
@@ -107,6 +113,8 @@ def lib(exact=False):
         L.cgd_group_rhs.restype = ctypes.c_int
         L.cgd_group_ros_step.argtypes = [vp, i32, vp, ctypes.c_double, i32]
         L.cgd_group_ros_step.restype = ctypes.c_int
+        L.cgd_set_physics.argtypes = [vp, ctypes.POINTER(CgdPhysics), vp]
+        L.cgd_set_physics.restype = ctypes.c_int
         L.cgd_metric_sphere.argtypes = [i32, i32, i32, vp, vp, vp, vp, dbl, dbl, vp, vp, vp]
         L.cgd_metric_sphere.restype = ctypes.c_int
         L.cgd_mass_dz.argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp]

@@ -134,6 +134,24 @@ class Dycore:
         self.h = h
         self._mmass = grid.MMass if hasattr(grid.MMass, "data_ptr") else np.asfortranarray(grid.MMass)
 
+    def set_physics(self, held_suarez=None, damping=None):
+        """Column physics in the tendency tail: held_suarez = True (the
+        reference's ParamHeldSuarezDrySphere values) or a dict of them;
+        damping = (H, StrideDamp, Relax) for the Rayleigh damping of w in the
+        top StrideDamp metres below H.  None switches a term off."""
+        from .physics import HELD_SUAREZ
+        ph = _lib.CgdPhysics()
+        hs = dict(HELD_SUAREZ, **(held_suarez if isinstance(held_suarez, dict) else {}))
+        ph.held_suarez = int(bool(held_suarez))
+        for k, v in hs.items():
+            setattr(ph, k, float(v))
+        ph.damping = int(damping is not None)
+        ph.damp_H, ph.damp_stride, ph.damp_relax = damping if damping is not None else (0.0, 1.0, 0.0)
+        ph.Rad = float(self.grid.Rad)
+        X = self.grid.X
+        xp = X.data_ptr() if hasattr(X, "data_ptr") else np.asfortranarray(X).ctypes.data
+        _lib.check(self._L.cgd_set_physics(self.h, ctypes.byref(ph), xp), "cgd_set_physics")
+
     def set_transport(self, transport):
         """The exchange of a decomposed grid's rank between processes:
         transport.exchange(send_views, recv_views) (parallel.TorchTransport)

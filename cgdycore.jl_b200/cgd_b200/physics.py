@@ -135,6 +135,14 @@ ENSEMBLE = {"grids": [(16, 30), (24, 45), (32, 64)], "per_grid": 16, "OrdPoly": 
             "hours": 6.0, "theta_amp": 0.1, "wind_amp": 0.5, "seed0": 20261300}
 
 
+# ParamHeldSuarezDrySphere (src/Examples/parameters.jl:122-131): the dry
+# Held-Suarez forcing's rates (1/s) and equilibrium-temperature parameters.
+_DAY = 3600.0 * 24.0
+HELD_SUAREZ = {"k_a": 1.0 / (40.0 * _DAY), "k_f": 1.0 / _DAY, "k_s": 1.0 / (4.0 * _DAY), "DeltaT_y": 60.0,
+               "DeltaTh_z": 10.0, "T_equator": 315.0, "T_min": 200.0, "sigma_b": 7.0 / 10.0}
+HELD_SUAREZ_ORDER = ("k_a", "k_f", "k_s", "DeltaT_y", "DeltaTh_z", "T_equator", "T_min", "sigma_b")
+
+
 def tracer_centres(NumTr, seed):
     """Blob centres uniform on the sphere: lon ~ U[0, 2pi), sin(lat) ~ U[-1, 1]."""
     rng = np.random.Generator(np.random.PCG64(seed))

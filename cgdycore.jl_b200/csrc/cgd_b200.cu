@@ -91,6 +91,9 @@ struct cgd_handle {
   // profile (the horizontal mean of the first state the handle sees)
   bool mix = false, have_ref = false;
   double *pref = nullptr, *thref = nullptr;
+  // column physics (cgd_set_physics)
+  std::vector<int> glob_host;                   // 0-based Glob, kept for the per-column set-up
+  double *coslat = nullptr, *sinlat = nullptr, *dampc = nullptr;
   // horizontal domain decomposition (cgd_create_part): this rank's halo
   bool decomposed = false;
   int nghost = 0, nsend = 0;
@@ -240,6 +243,14 @@ void pressure(cgd_handle *h, const double *U, double *p)
   k_pressure<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->gp, U, p);
 }
 
+// The column physics added to a tendency (no launch when none is set).
+void physics(cgd_handle *h, const double *U, const double *p, double *F)
+{
+  if (!h->gp.held_suarez && !h->gp.damping) return;
+  const long long n = (long long)h->nz * h->NumG;
+  k_physics<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->gp, U, p, F);
+}
+
 // wsplit: the phase-2 tendency (w split into two contributions, FP64 output);
 // otherwise phase 1, whose output is the cache (stored like the contributions)
 // or, with tendency_out, an FP64 array for the caller.
@@ -323,6 +334,8 @@ void stage_piece(cgd_handle *h, double *U, const ColArgs &a0, int stage, int pie
     rec(h, e++);
   } else {
     ColArgs a = a0;
+    a.Vs = Vsrc;
+    a.ps = stage == 0 ? h->pres : h->pres_st;
     if (stage == 0) {
       a.kout = h->k1; a.Vout = h->Vst;
       column<0>(h, a);
@@ -462,7 +475,10 @@ int part_pieces(cgd_handle *const *parts, int n, double *const *U, double dt, bo
       phase2(h, U[r], h->pres, h->T1, h->C);
     }
     if (int rc = xchg(nf2)) return rc;
-    for (int r = 0; r < n; ++r) gather(parts[r], parts[r]->C, F[r], true);
+    for (int r = 0; r < n; ++r) {
+      gather(parts[r], parts[r]->C, F[r], true);
+      physics(parts[r], U[r], parts[r]->pres, F[r]);
+    }
     return CGD_OK;
   }
   std::vector<ColArgs> a(n);
@@ -770,6 +786,7 @@ static int create_impl(const cgd_config *cfg, const int64_t *glob, const double 
     return CGD_ERR_CUDA;
   }
 
+  h->glob_host = glob0;
   GP &P = h->gp;
   P.N = N; P.DoF = DoF; P.nz = nz; P.NF = NF; P.NumG = NumG; P.NumTr = h->NumTr; P.NV = NV; P.NC = NV + 1;
   P.met = h->met; P.M = h->M; P.dz = h->dz; P.glob = h->glob; P.inv_ptr = h->inv_ptr; P.inv_off = h->inv_off;
@@ -896,6 +913,7 @@ int cgd_rhs(cgd_handle *h, const double *U, double *F)
   pressure(h, Ud, h->pres);
   phase2(h, Ud, h->pres, h->T1, h->C);
   gather(h, h->C, fd, true);
+  physics(h, Ud, h->pres, fd);
   if (!fdev) CK(cudaMemcpyAsync(F, fd, (size_t)h->nz * h->NumG * h->NV * 8, cudaMemcpyDeviceToHost, h->stream));
   return finish(h);
 }
@@ -1050,6 +1068,78 @@ int cgd_ros_step(cgd_handle *h, double *U, double dt, int32_t nsteps)
     CK(cudaMemcpy(&f, h->flag, sizeof(int), cudaMemcpyDeviceToHost));
     if (f) return CGD_ERR_NONFINITE;
   }
+  return CGD_OK;
+}
+
+int cgd_set_physics(cgd_handle *h, const cgd_physics *ph, const double *X)
+{
+  if (!h || !ph) return CGD_ERR_INVALID_ARG;
+  if (h->mix && (ph->held_suarez || ph->damping)) return CGD_ERR_UNSUPPORTED;
+  if (ph->damping && !(ph->damp_stride > 0)) return CGD_ERR_INVALID_ARG;
+  const int nz = h->nz, NumG = h->NumG, DoF = h->DoF, NF = h->NF;
+  if ((ph->held_suarez || ph->damping) && !X) return CGD_ERR_INVALID_ARG;
+  GP &P = h->gp;
+  if (ph->held_suarez || ph->damping) {
+    // positions (reference layout (N*N, 2, 3, nz, NF)), from the device if need be
+    const size_t nx = (size_t)DoF * 6 * nz * NF;
+    std::vector<double> xh;
+    const double *Xh = X;
+    if (is_device_ptr(X)) {
+      xh.resize(nx);
+      CK(cudaMemcpy(xh.data(), X, nx * 8, cudaMemcpyDeviceToHost));
+      Xh = xh.data();
+    }
+    auto xx = [&](int ID, int K, int c, int Iz, int IF) {
+      return Xh[ID + (size_t)DoF * (K + 2 * (c + 3 * (Iz + (size_t)nz * IF)))];
+    };
+    // per column, from its highest-numbered element node (the last to write
+    // it): the surface latitude (MetricLowerBoundaryKernel!,
+    // src/DyCore/DiscretizationCG.jl:159-178, cart2sphere
+    // src/Grids/Geometry.jl:65-73) and the damping rate at the layer-midpoint
+    // height zP (GridSizeSphereKernel!, DiscretizationCG.jl:119-144; DampingW,
+    // src/GPU/dampingGPU.jl:1-19)
+    std::vector<double> cl(NumG), sl(NumG), dc((size_t)nz * NumG, 0.0);
+    const double pi = 3.141592653589793, Rad = ph->Rad;
+    for (int IF = 0; IF < NF; ++IF)
+      for (int ID = 0; ID < DoF; ++ID) {
+        const int g = h->glob_host[ID + (size_t)DoF * IF];
+        const double x = xx(ID, 0, 0, 0, IF), y = xx(ID, 0, 1, 0, IF), z = xx(ID, 0, 2, 0, IF);
+        const double r = std::sqrt(x * x + y * y + z * z);
+        const double lat = std::asin(z / r);
+        cl[g] = std::cos(lat);
+        sl[g] = std::sin(lat);
+        for (int Iz = 0; Iz < nz; ++Iz) {
+          const double xm = 0.5 * (xx(ID, 0, 0, Iz, IF) + xx(ID, 1, 0, Iz, IF));
+          const double ym = 0.5 * (xx(ID, 0, 1, Iz, IF) + xx(ID, 1, 1, Iz, IF));
+          const double zm = 0.5 * (xx(ID, 0, 2, Iz, IF) + xx(ID, 1, 2, Iz, IF));
+          const double rm = std::sqrt(xm * xm + ym * ym + zm * zm);
+          const double zP = std::max(rm - Rad, 0.0);
+          double c = 0.0;
+          if (ph->damping && zP >= ph->damp_H - ph->damp_stride) {
+            const double sn = std::sin(0.5 * pi * (1.0 - (ph->damp_H - zP) / ph->damp_stride));
+            c = ph->damp_relax * (sn * sn);
+          }
+          dc[Iz + (size_t)nz * g] = c;
+        }
+      }
+    if (!h->coslat) {
+      if (int rc = dalloc(h, &h->coslat, NumG)) return rc;
+      if (int rc = dalloc(h, &h->sinlat, NumG)) return rc;
+      if (int rc = dalloc(h, &h->dampc, (size_t)nz * NumG)) return rc;
+    }
+    CK(cudaMemcpy(h->coslat, cl.data(), NumG * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->sinlat, sl.data(), NumG * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->dampc, dc.data(), dc.size() * 8, cudaMemcpyHostToDevice));
+  }
+  P.held_suarez = ph->held_suarez ? 1 : 0;
+  P.damping = ph->damping ? 1 : 0;
+  const double hs[8] = {ph->k_a, ph->k_f, ph->k_s, ph->DeltaT_y, ph->DeltaTh_z, ph->T_equator, ph->T_min,
+                        ph->sigma_b};
+  for (int i = 0; i < 8; ++i) P.hs[i] = hs[i];
+  P.coslat = h->coslat;
+  P.sinlat = h->sinlat;
+  P.dampc = h->dampc;
+  free_graph(h);   // the captured step holds the old parameters
   return CGD_OK;
 }
 
@@ -1452,7 +1542,7 @@ extern "C" {
 int cgd_ros_step_adjoint(cgd_handle *h, const double *U0, const double *Lout, double *Lin, double dt)
 {
   if (!h || !U0 || !Lout || !Lin || !(dt > 0)) return CGD_ERR_INVALID_ARG;
-  if (h->mix || h->NumTr != 0) return CGD_ERR_UNSUPPORTED;
+  if (h->mix || h->NumTr != 0 || h->gp.held_suarez || h->gp.damping) return CGD_ERR_UNSUPPORTED;
   int rc = adjoint_alloc(h, true);
   if (!rc) rc = tape_alloc(h, h->work_tape, false);
   if (!rc) rc = enter(h);
@@ -1471,7 +1561,7 @@ int cgd_ros_step_adjoint(cgd_handle *h, const double *U0, const double *Lout, do
 int cgd_tape_record_step(cgd_handle *h, int32_t slot, double *U, double dt)
 {
   if (!h || !U || !(dt > 0) || slot < 0 || slot >= CGD_TAPE_MAX_SLOTS) return CGD_ERR_INVALID_ARG;
-  if (h->mix || h->NumTr != 0) return CGD_ERR_UNSUPPORTED;
+  if (h->mix || h->NumTr != 0 || h->gp.held_suarez || h->gp.damping) return CGD_ERR_UNSUPPORTED;
   if ((size_t)slot >= h->tapes.size()) h->tapes.resize(slot + 1);
   int rc = adjoint_alloc(h, true);
   if (!rc) rc = tape_alloc(h, h->tapes[slot], true);
@@ -1524,7 +1614,7 @@ namespace {
 int cgd_rhs_adjoint_impl(cgd_handle *h, const double *U, const double *LF, double *LU)
 {
   if (!h || !U || !LF || !LU) return CGD_ERR_INVALID_ARG;
-  if (h->mix || h->NumTr != 0) return CGD_ERR_UNSUPPORTED;
+  if (h->mix || h->NumTr != 0 || h->gp.held_suarez || h->gp.damping) return CGD_ERR_UNSUPPORTED;
   const size_t S = (size_t)h->nz * h->NumG;
   int arc = adjoint_alloc(h, false);
   if (!arc) arc = enter(h);

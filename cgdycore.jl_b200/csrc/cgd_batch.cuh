@@ -89,6 +89,8 @@ __global__ void __launch_bounds__(32 * COL_WARPS, 4) kb_column(const WItem *__re
   a.dt = B.dt;
   a.fac = B.dt * c_brk.gamma;
   a.rk = c_brk;
+  a.Vs = MODE == 0 ? B.U : B.Vst;
+  a.ps = MODE == 0 ? B.P0 : B.Pst;
   if (MODE == 0) { a.kout = B.k1; a.Vout = B.Vst; }
   else if (MODE == 1) { a.kout = B.k2; a.Vout = B.Vst; }
   else { a.kout = nullptr; a.Vout = B.U; }
@@ -247,6 +249,8 @@ __global__ void __launch_bounds__(256, 2) kb_stage(const FusedArgs A, const int 
     a.dt = B.dt;
     a.fac = B.dt * c_brk.gamma;
     a.rk = c_brk;
+    a.Vs = fused_stage_state(B, stage);
+    a.ps = stage == 0 ? B.P0 : B.Pst;
     if (stage == 0) {
       a.kout = B.k1; a.Vout = B.Vst;
       column_body<0, C32>(c_bgp[it.m], a, it.x);

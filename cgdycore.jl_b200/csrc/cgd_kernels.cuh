@@ -97,6 +97,12 @@ struct GP {
   const double *pref;       // mixed form: per-level FP64 reference pressure and theta
   const double *thref;
   double Grav, Rd, p0, kappa, nuCurl, nuGrad, nuDiv;
+  // column physics of the tendency tail (cgd_set_physics): the dry
+  // Held-Suarez forcing and the Rayleigh damping of w near the top
+  int held_suarez, damping;
+  double hs[8];             // k_a, k_f, k_s, DeltaT_y, DeltaTh_z, T_equator, T_min, sigma_b
+  const double *coslat, *sinlat;   // (NumG) latitude of each column's surface node
+  const double *dampc;             // (nz, NumG) damping rate at the layer midpoint
 };
 
 // Rosenbrock-W coefficients (src/Integration/RosenbrockMethod.jl:26-47).
@@ -108,6 +114,36 @@ __device__ __forceinline__ double pressure_dry(const GP &P, double rhoth)
 {
   // src/Models/Equation.jl:25-38, fast_powGPU (Equation.jl:79)
   return P.p0 * cgd_exp(1.0 / (1.0 - P.kappa) * cgd_log(P.Rd * rhoth / P.p0));
+}
+
+// The column physics of the tendency tail at level l of column g
+// (src/GPU/FcnGPU.jl:953-966): ForceKernel! with the dry Held-Suarez Force
+// (src/GPU/OperatorKernel.jl:1073-1080, src/Examples/initial.jl:513-531) and
+// DampKernel! with DampingW (OperatorKernel.jl:1061-1071,
+// src/GPU/dampingGPU.jl:1-19), for the state values rho, u, v, w, rho*theta
+// and the pressure p there: adds to f[1] (u), f[2] (v), f[3] (w), f[4]
+// (rho*theta).  fast_powGPU(x, y) = exp(y log x) (src/Models/Equation.jl:79).
+__device__ __forceinline__ void physics_terms(const GP &P, int l, int g, double rho, double u, double v, double w,
+                                              double rhoth, double p, double *f)
+{
+  if (P.held_suarez) {
+    const double k_a = P.hs[0], k_f = P.hs[1], k_s = P.hs[2], DeltaT_y = P.hs[3], DeltaTh_z = P.hs[4];
+    const double T_equator = P.hs[5], T_min = P.hs[6], sigma_b = P.hs[7];
+    const double Sigma = p / P.p0;
+    const double SigmaPowKappa = cgd_exp(P.kappa * cgd_log(Sigma));
+    const double height_factor = cgd_max(0.0, (Sigma - sigma_b) / (1.0 - sigma_b));
+    const double coslat = P.coslat[g], sinlat = P.sinlat[g];
+    f[1] += -(k_f * height_factor) * u;
+    f[2] += -(k_f * height_factor) * v;
+    const double kT = k_a + (k_s - k_a) * height_factor * coslat * coslat * coslat * coslat;
+    double Teq = (T_equator - DeltaT_y * sinlat * sinlat - DeltaTh_z * cgd_log(Sigma) * coslat * coslat) *
+                 SigmaPowKappa;
+    Teq = cgd_max(T_min, Teq);
+    const double T = p / (rho * P.Rd);
+    const double DeltaT = kT * (T - Teq);
+    f[4] += -rhoth / T * DeltaT;
+  }
+  if (P.damping) f[3] += -P.dampc[l + (size_t)P.nz * g] * w;
 }
 
 // RecU4: src/GPU/OperatorKernel.jl:1044-1059
@@ -440,6 +476,9 @@ struct ColArgs {
   // (2, nz-1, NumG) in the reference layout (the JCache arrays)
   const double *jb4[4];
   double *jbg;           // MODE 0 writes, 1-2 read: [8][NumG][nz-1] bands of the step
+  // MODE 0..2 with column physics: the stage state the tendency is of and its
+  // pressure (Vs may be Vout: each lane reads its own levels before writing them)
+  const double *Vs, *ps;
   double dt, fac;
   RK rk;
 };
@@ -618,6 +657,10 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
       const size_t fstr = (size_t)P.DoF * nz;
       double gacc[MAXNV];
       gather_node<true, C32>(P, A.C, g, l, fstr, gacc);
+      if (P.held_suarez || P.damping) {   // the tendency tail, at the stage state
+        const double *vs = A.Vs + o0;
+        physics_terms(P, l, g, vs[0], vs[fs], vs[2 * fs], vs[3 * fs], vs[4 * fs], A.ps[o0], gacc);
+      }
 #pragma unroll
       for (int f = 0; f < MAXNV; ++f) {
         if (f >= NV) break;
@@ -851,6 +894,23 @@ __global__ void __launch_bounds__(256) k_refprof(const GP P, const double *__res
 struct Bands4 {
   double *b[4];
 };
+
+// The column physics added to a tendency F of the state U with pressure p
+// (cgd_rhs): one thread per column-level.
+__global__ void __launch_bounds__(256) k_physics(const GP P, const double *__restrict__ U,
+                                                 const double *__restrict__ p, double *__restrict__ F)
+{
+  const long long S = (long long)P.nz * P.NumG;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= S) return;
+  const int g = (int)(t / P.nz), l = (int)(t - (long long)g * P.nz);
+  double f[5] = {0.0, F[t + S], F[t + 2 * S], F[t + 3 * S], F[t + 4 * S]};
+  physics_terms(P, l, g, U[t], U[t + S], U[t + 2 * S], U[t + 3 * S], U[t + 4 * S], p[t], f);
+  F[t + S] = f[1];
+  F[t + 2 * S] = f[2];
+  F[t + 3 * S] = f[3];
+  F[t + 4 * S] = f[4];
+}
 
 // Jacobian bands into memory (cgd_jac): one thread per (interface, column)
 __global__ void k_jac(const GP P, const double *__restrict__ U, const Bands4 out)

@@ -202,6 +202,38 @@ function step!(b::Batch, states, dts::Vector{Float64}; nsteps = 1)
   end
 end
 
+# Column physics in the tendency tail (struct cgd_physics): the dry
+# Held-Suarez forcing with the reference's ParamHeldSuarezDrySphere values
+# (Param) and the Rayleigh damping of w in the top StrideDamp metres below H.
+struct CgdPhysics
+  held_suarez::Int32
+  damping::Int32
+  k_a::Float64
+  k_f::Float64
+  k_s::Float64
+  DeltaT_y::Float64
+  DeltaTh_z::Float64
+  T_equator::Float64
+  T_min::Float64
+  sigma_b::Float64
+  damp_H::Float64
+  damp_stride::Float64
+  damp_relax::Float64
+  Rad::Float64
+end
+
+function set_physics!(h::Handle, Param, Metric, Phys; held_suarez = true, damping = nothing)
+  dH, dS, dR = damping === nothing ? (0.0, 1.0, 0.0) : damping
+  ph = Ref(CgdPhysics(Int32(held_suarez), Int32(damping !== nothing), Param.k_a, Param.k_f, Param.k_s,
+                      Param.DeltaT_y, Param.DeltaTh_z, Param.T_equator, Param.T_min, Param.sigma_b,
+                      dH, dS, dR, Phys.RadEarth))
+  X = hostcopy(Metric.X)
+  GC.@preserve X begin
+    check(ccall((:cgd_set_physics, libcgd), Cint, (Ptr{Cvoid}, Ref{CgdPhysics}, Ptr{Float64}), h.ptr, ph,
+                pointer(X)), "cgd_set_physics")
+  end
+end
+
 # The stream whose queued work every call waits for (a cudaStream_t; a
 # CUDA.jl caller passes CUDA.stream().handle); C_NULL = the legacy default stream.
 function set_caller_stream!(h::Handle, stream)

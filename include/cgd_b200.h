@@ -161,6 +161,30 @@ int cgd_metric_sphere(int32_t OrdPoly, int32_t nz, int32_t NF, const double *FP,
 int cgd_mass_dz(int32_t OrdPoly, int32_t nz, int32_t NF, int32_t NumG, const int64_t *glob, const double *w,
                 const double *J, const double *X, double *M, double *MMass, double *dz);
 
+/* Column physics in the tendency tail, after the DSS (src/GPU/FcnGPU.jl:953-966):
+ *   held_suarez  the dry Held-Suarez forcing, ForceKernel! with
+ *                HeldSuarezDryExample's Force (src/GPU/OperatorKernel.jl:1073-1080,
+ *                src/Examples/initial.jl:513-531; default parameters
+ *                ParamHeldSuarezDrySphere, src/Examples/parameters.jl:122-131):
+ *                Rayleigh friction of u, v below sigma_b and Newtonian
+ *                relaxation of the temperature to Teq(lat, sigma);
+ *   damping      DampKernel! with DampingW (OperatorKernel.jl:1061-1071,
+ *                src/GPU/dampingGPU.jl:1-19): w relaxed at the rate
+ *                damp_relax sin^2(pi/2 (1 - (damp_H - zP)/damp_stride)) in the top
+ *                damp_stride metres below damp_H (zP the layer-midpoint height).
+ * X is the node positions (N*N, 2, 3, nz, NF) (host or device) and Rad the
+ * radius: each column's latitude (of its surface node) and zP are formed
+ * once here, on the host.  Every later tendency (cgd_rhs) and step includes
+ * the terms.  FP64 handles (CGD_ERR_UNSUPPORTED for the mixed form); the
+ * adjoints do not differentiate them (CGD_ERR_UNSUPPORTED while set). */
+typedef struct cgd_physics {
+  int32_t held_suarez, damping;
+  double k_a, k_f, k_s, DeltaT_y, DeltaTh_z, T_equator, T_min, sigma_b;
+  double damp_H, damp_stride, damp_relax;
+  double Rad;
+} cgd_physics;
+int cgd_set_physics(cgd_handle *h, const cgd_physics *phys, const double *X);
+
 /* Pressure p (nz, NumG) from the state.
  * Replaces GPU.FcnPrepareGPU! / PressureKernel! (src/GPU/DiagnosticKernel.jl:96-115,180-218). */
 int cgd_prepare(cgd_handle *h, const double *U, double *p);

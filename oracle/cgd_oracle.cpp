@@ -507,6 +507,11 @@ struct Model {
   std::vector<int> inv_ptr, inv_idx;    // contributors (IF*DoF+ID) of each global id
   std::vector<double> bands;            // JRhoW, JWRho, JWRhoTh, JRhoThW (2, nz-1, NumG) each
   double rk_a[3][3], rk_c[3][3], rk_m[3], rk_gamma;
+  // column physics in the tendency tail (off unless orc_set_physics)
+  int held_suarez = 0, damping = 0;
+  double hs[8] = {};                    // k_a, k_f, k_s, DeltaT_y, DeltaTh_z, T_equator, T_min, sigma_b
+  std::vector<double> coslat, sinlat;   // (NumG) of the surface node
+  std::vector<double> dampc;            // (nz, NumG) Relax sin^2(...) above H - StrideDamp, else 0
 };
 
 inline double &DXI(Model &m, int a, int b, int K, int ID, int Iz, int IF)
@@ -1295,6 +1300,44 @@ static void phase2_element(Model &m, const Ctx &c, const double *T1, int IF, std
   }
 }
 
+// The column physics of the tendency tail (src/GPU/FcnGPU.jl:953-966), after
+// the DSS: ForceKernel! with the dry Held-Suarez Force
+// (src/GPU/OperatorKernel.jl:1073-1080, src/Examples/initial.jl:513-531,
+// parameters src/Examples/parameters.jl:122-131) and DampKernel! with
+// DampingW (src/GPU/OperatorKernel.jl:1061-1071, src/GPU/dampingGPU.jl:1-19).
+// fast_powGPU(x, y) = exp(y log x) (src/Models/Equation.jl:79).
+static void physics_tail(const Model &m, const double *U, double *F)
+{
+  if (!m.held_suarez && !m.damping) return;
+  const int nz = m.nz, NumG = m.NumG;
+  const size_t S = (size_t)nz * NumG;
+  const Phys &ph = m.phys;
+  #pragma omp parallel for schedule(static)
+  for (int g = 0; g < NumG; ++g)
+    for (int Iz = 0; Iz < nz; ++Iz) {
+      const size_t o = Iz + (size_t)nz * g;
+      if (m.held_suarez) {
+        const double k_a = m.hs[0], k_f = m.hs[1], k_s = m.hs[2], DeltaT_y = m.hs[3], DeltaTh_z = m.hs[4];
+        const double T_equator = m.hs[5], T_min = m.hs[6], sigma_b = m.hs[7];
+        const double p = pressure(ph, U[o + 4 * S]);
+        const double Sigma = p / ph.p0;
+        const double SigmaPowKappa = cgd_exp(ph.kappa * cgd_log(Sigma));
+        const double height_factor = std::max(0.0, (Sigma - sigma_b) / (1.0 - sigma_b));
+        const double coslat = m.coslat[g], sinlat = m.sinlat[g];
+        F[o + S] += -(k_f * height_factor) * U[o + S];
+        F[o + 2 * S] += -(k_f * height_factor) * U[o + 2 * S];
+        const double kT = k_a + (k_s - k_a) * height_factor * coslat * coslat * coslat * coslat;
+        double Teq = (T_equator - DeltaT_y * sinlat * sinlat - DeltaTh_z * cgd_log(Sigma) * coslat * coslat) *
+                     SigmaPowKappa;
+        Teq = std::max(T_min, Teq);
+        const double T = p / (U[o] * ph.Rd);
+        const double DeltaT = kT * (T - Teq);
+        F[o + 4 * S] += -U[o + 4 * S] / T * DeltaT;
+      }
+      if (m.damping) F[o + 3 * S] += -m.dampc[o] * U[o + 3 * S];
+    }
+}
+
 static void rhs(Model &m, const double *U, double *F)
 {
   Ctx c(m, U);
@@ -1309,6 +1352,7 @@ static void rhs(Model &m, const double *U, double *F)
   #pragma omp parallel for schedule(dynamic, 4)
   for (int IF = 0; IF < m.NF; ++IF) phase2_element(m, c, T1.data(), IF, C2);
   gather(m, C2, NV, F);
+  physics_tail(m, U, F);
 }
 
 // JacSchurKernel!: src/DyCore/JacSchur.jl:29-75 (AuxG[:,:,4] == 0 for Dry),
@@ -1697,6 +1741,48 @@ int orc_contributions(void *h, const double *U, const double *T1, double *C)
     else hypervisc1_element(*m, c, IF, Cv);
   }
   memcpy(C, Cv.data(), Cv.size() * sizeof(double));
+  return 0;
+}
+
+// Column physics: the surface latitude of every column from the bottom node
+// of its highest-numbered element node (MetricLowerBoundaryKernel!,
+// src/DyCore/DiscretizationCG.jl:159-178, cart2sphere src/Grids/Geometry.jl:65-73),
+// the layer-midpoint height zP (GridSizeSphereKernel!, DiscretizationCG.jl:119-144)
+// and the damping coefficient there.
+int orc_set_physics(void *h, int held_suarez, const double *hs8, int damping, double damp_H, double damp_stride,
+                    double damp_relax)
+{
+  Model *m = static_cast<Model *>(h);
+  m->held_suarez = held_suarez;
+  m->damping = damping;
+  for (int i = 0; i < 8; ++i) m->hs[i] = hs8 ? hs8[i] : 0.0;
+  const int nz = m->nz, NumG = m->NumG, DoF = m->DoF;
+  m->coslat.assign(NumG, 0.0);
+  m->sinlat.assign(NumG, 0.0);
+  m->dampc.assign((size_t)nz * NumG, 0.0);
+  const double pi = 3.141592653589793;
+  for (int IF = 0; IF < m->NF; ++IF)
+    for (int ID = 0; ID < DoF; ++ID) {
+      const int g = m->glob[ID + (size_t)DoF * IF];
+      const double x = XX(*m, ID, 0, 0, 0, IF), y = XX(*m, ID, 0, 1, 0, IF), z = XX(*m, ID, 0, 2, 0, IF);
+      const double r = std::sqrt(x * x + y * y + z * z);
+      const double lat = std::asin(z / r);
+      m->coslat[g] = std::cos(lat);
+      m->sinlat[g] = std::sin(lat);
+      for (int Iz = 0; Iz < nz; ++Iz) {
+        const double xm = 0.5 * (XX(*m, ID, 0, 0, Iz, IF) + XX(*m, ID, 1, 0, Iz, IF));
+        const double ym = 0.5 * (XX(*m, ID, 0, 1, Iz, IF) + XX(*m, ID, 1, 1, Iz, IF));
+        const double zm = 0.5 * (XX(*m, ID, 0, 2, Iz, IF) + XX(*m, ID, 1, 2, Iz, IF));
+        const double rm = std::sqrt(xm * xm + ym * ym + zm * zm);
+        const double zP = std::max(rm - m->Rad, 0.0);
+        double c = 0.0;
+        if (zP >= damp_H - damp_stride) {
+          const double sn = std::sin(0.5 * pi * (1.0 - (damp_H - zP) / damp_stride));
+          c = damp_relax * (sn * sn);
+        }
+        m->dampc[Iz + (size_t)nz * g] = c;
+      }
+    }
   return 0;
 }
 

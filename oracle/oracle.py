@@ -50,6 +50,8 @@ def lib():
         for f in ["orc_pressure", "orc_hypervisc1", "orc_rhs", "orc_jac"]:
             getattr(L, f).argtypes = [vp, vp, vp]
         L.orc_contributions.argtypes = [vp, vp, vp, vp]
+        L.orc_set_physics.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double]
         L.orc_schur.argtypes = [vp, vp, vp, ctypes.c_double]
         L.orc_ros_step.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int]
         L.orc_mass_integral.argtypes = [vp, vp]
@@ -157,6 +159,15 @@ class Oracle:
         T = np.zeros((self.nz, self.NumG, 5 + self.NumTr), order="F")
         lib().orc_hypervisc1(self.h, _p(U), _p(T))
         return T
+
+    def set_physics(self, held_suarez=None, damping=None):
+        """Column physics in the tendency tail: held_suarez = the 8 parameters
+        (k_a, k_f, k_s, DeltaT_y, DeltaTh_z, T_equator, T_min, sigma_b) or
+        None; damping = (H, StrideDamp, Relax) or None."""
+        hs = np.ascontiguousarray(held_suarez if held_suarez is not None else np.zeros(8), dtype=np.float64)
+        dH, dS, dR = damping if damping is not None else (0.0, 1.0, 0.0)
+        lib().orc_set_physics(self.h, int(held_suarez is not None), _p(hs), int(damping is not None),
+                              float(dH), float(dS), float(dR))
 
     def contributions(self, U, T1=None):
         """Element-node contributions before the DSS, shape (DoF, nf, nz, NF)
