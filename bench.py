@@ -57,6 +57,7 @@ def parse():
                     help="steps of the adjoint sensitivity study (120 x 120 s = 4 h)")
     ap.add_argument("--adjoint-fd", action="store_true",
                     help="add central-difference checks of the sensitivity gradient (about a minute)")
+    ap.add_argument("--no-output", action="store_true", help="skip the output-interpolation sub-measurement")
     ap.add_argument("--parallel", default="member", choices=["member", "shard"],
                     help="N > 1: one ensemble member per GPU (weak scaling) or one grid decomposed over the "
                          "GPUs with halo exchanges of the DSS (strong scaling)")
@@ -648,6 +649,44 @@ def run_ensemble(args, rank, world, local):
         torch.distributed.destroy_process_group()
 
 
+def run_output(dyc, Ut, cfg, rank, torch, reps=10):
+    """The VTK output path on the timed run's state: cgd_output_fields for the
+    reference's field list at OrdPrint 1 (device-resident, CUDA events on the
+    library's stream), and one VtkOutput.write (interpolation, copy to pinned
+    host memory, .vtu file) timed on the wall clock."""
+    from cgd_b200 import output
+    names = ("Rho", "u", "v", "wB", "Th", "Pres", "Vort") + tuple(f"Tr{q + 1}" for q in range(dyc.NumTr))
+    t0 = time.perf_counter()
+    w = output.VtkOutput(dyc, names=names, OrdPrint=1)
+    t_setup = time.perf_counter() - t0
+    out = torch.empty(len(names) * w.ncells, dtype=torch.float64, device=Ut.device)
+    stream = torch.cuda.ExternalStream(dyc.stream())
+    for _ in range(2):
+        dyc.output_fields(Ut, w.codes, w.inter, out)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        dyc.output_fields(Ut, w.codes, w.inter, out)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    S = (6 * cfg.nPanel ** 2 * cfg.OrdPoly ** 2 + 2) * cfg.nz * 8   # one (nz, NumG) field in bytes
+    NF, nz, DoF = 6 * cfg.nPanel ** 2, cfg.nz, (cfg.OrdPoly + 1) ** 2
+    metric_vort = 10 * DoF * nz * NF * 8                           # D11..D22 (both nodes), J of every level
+    algo = (5 + dyc.NumTr) * S + metric_vort + len(names) * w.ncells * 8
+    res = {"fields": list(names), "OrdPrint": 1, "cells": w.ncells, "ms_per_call": ms,
+           "algorithmic_bytes": algo, "achieved_GBs": algo / (ms * 1e-3) / 1e9, "setup_s": t_setup,
+           "launches_per_call": len(names)}
+    if rank == 0:
+        with tempfile.TemporaryDirectory() as tmp:
+            t0 = time.perf_counter()
+            path = w.write(Ut, os.path.join(tmp, "out"))
+            w.wait()
+            res["write_s"] = time.perf_counter() - t0
+            res["file_bytes"] = os.path.getsize(path)
+    return res
+
+
 def run_ours(args, cfg, rank, world, local):
     import torch
     torch.cuda.set_device(local)
@@ -713,6 +752,10 @@ def run_ours(args, cfg, rank, world, local):
         ensemble["single_member_dof_updates_per_s"] = value * unique_dof(cfg) / world
         ensemble["vs_single_member"] = ensemble["dof_updates_per_s"] / (value * unique_dof(cfg) / world)
 
+    outp = None
+    if args.precision == "fp64" and not args.no_output:
+        outp = run_output(dyc, Ut, cfg, rank, torch)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -754,6 +797,7 @@ def run_ours(args, cfg, rank, world, local):
             "mixed_cfg3": mixed_cfg3,
             "adjoint": adjoint,
             "ensemble": ensemble,
+            "output": outp,
             "gpu_launches": 15 * args.steps,
             "cpu_baseline": cpu,
             "clocks": clk,

@@ -34,7 +34,11 @@ EXPORTS = [
     "cgd_grid_barrier_check",
     "cgd_create_part", "cgd_set_exchange", "cgd_halo_buffers", "cgd_group_rhs", "cgd_group_ros_step",
     "cgd_metric_sphere", "cgd_mass_dz", "cgd_set_physics",
+    "cgd_vtk_inter", "cgd_interpolate", "cgd_interpolate_wb", "cgd_interpolate_vort", "cgd_output_fields",
 ]
+
+# output quantities of cgd_output_fields (CGD_OUT_* in include/cgd_b200.h)
+OUT_RHO, OUT_U, OUT_V, OUT_WB, OUT_TH, OUT_PRES, OUT_VORT, OUT_WB_UV, OUT_TR = 0, 1, 2, 3, 4, 5, 6, 7, 16
 
 
 class CgdConfig(ctypes.Structure):
@@ -120,6 +124,11 @@ def lib(exact=False):
         L.cgd_mass_dz.argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp]
         L.cgd_mass_dz.restype = ctypes.c_int
         L.cgd_grid_barrier_check.argtypes = [i32, i32, ctypes.c_double, ctypes.POINTER(i32)]
+        L.cgd_vtk_inter.argtypes = [i32, i32, vp, vp]
+        L.cgd_interpolate.argtypes = [vp, vp, vp, vp, i32, vp]
+        L.cgd_interpolate_wb.argtypes = [vp, vp, vp, vp, vp, i32, vp]
+        L.cgd_interpolate_vort.argtypes = [vp, vp, vp, i32, vp]
+        L.cgd_output_fields.argtypes = [vp, vp, vp, i32, vp, i32, vp]
         L.cgd_grid_barrier_check.restype = ctypes.c_int
         for f in ("cgd_prepare", "cgd_hypervisc_phase1", "cgd_rhs", "cgd_jac"):
             getattr(L, f).argtypes = [vp, vp, vp]

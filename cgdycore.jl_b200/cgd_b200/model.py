@@ -19,6 +19,10 @@ libcgd_b200.so:
   rosenbrock_schur(U, dt)     Integration.RosenbrockSchur! (RosenbrockSchur.jl:1)
   time_stepper(U, dt, n)      the Rosenbrock branch of TimeStepper! (TimeStepper.jl:103-124)
   mass_integral(U)            Parallels.GlobalIntegral (Exchange.jl:1163)
+  interpolate(c, inter, rhoc) Outputs.InterpolateGPU! / InterpolateRhoGPU! (vtkOutputKernel.jl:215,254)
+  interpolate_wb(u,v,w,inter) Outputs.InterpolateWBGPU! (vtkOutputKernel.jl:274)
+  interpolate_vort(U, inter)  Outputs.InterpolateVortGPU! (vtkOutputKernel.jl:186)
+  output_fields(U, codes, i)  the interpolation loop of unstructured_vtkSphere (vtkSphere.jl:337)
   fcn_adjoint(U, LF)          (no counterpart) (dF/dU)^T LF
   ros_step_adjoint(U0, L, dt) (no counterpart) adjoint of one step
   steps_adjoint(U0, L, dt, n) (no counterpart) checkpointed n-step gradient
@@ -366,6 +370,77 @@ class Dycore:
         _lib.check(self._L.cgd_mass_integral(self.h, _ptr(U, self.shape), mm, ctypes.byref(out)),
                    "cgd_mass_integral")
         return out.value
+
+    # ---- output interpolation (the reference's VTK output kernels)
+    def _cells(self, like, OP):
+        """Zeroed cell array (OrdPrint, OrdPrint, nz, NF) in Fortran order: a
+        numpy array, or for a tensor `like` a tensor of shape (NF, nz, OP, OP)
+        on its device (the same memory layout)."""
+        if isinstance(like, np.ndarray):
+            return np.zeros((OP, OP, self.nz, self.NF), order="F")
+        import torch
+        return torch.zeros((self.NF, self.nz, OP, OP), dtype=torch.float64, device=like.device)
+
+    @staticmethod
+    def _inter(inter):
+        """The weights (OrdPrint, OrdPrint, N, N) of output.vtk_inter (host)."""
+        inter = np.asfortranarray(inter, dtype=np.float64)
+        if inter.ndim != 4 or inter.shape[0] != inter.shape[1]:
+            raise ValueError("inter: (OrdPrint, OrdPrint, N, N)")
+        return inter, inter.shape[0], inter.ctypes.data
+
+    def interpolate(self, c, inter, rhoc=None, out=None):
+        """InterpolateGPU! / InterpolateRhoGPU!: c (nz, NumG) at the
+        OrdPrint x OrdPrint sub-cell centres, (OrdPrint, OrdPrint, nz, NF);
+        each nodal value divided by rhoc first when given."""
+        inter, OP, ip = self._inter(inter)
+        out = self._cells(c, OP) if out is None else out
+        two = (self.nz, self.NumG)
+        _lib.check(self._L.cgd_interpolate(self.h, _ptr(c, two), _ptr(rhoc, two) if rhoc is not None else None, ip,
+                                           OP, _ptr(out, (OP, OP, self.nz, self.NF), True)), "cgd_interpolate")
+        return out
+
+    def interpolate_wb(self, u, v, w, inter, out=None):
+        """InterpolateWBGPU!: layer-mean w with the surface value from u, v."""
+        inter, OP, ip = self._inter(inter)
+        out = self._cells(w, OP) if out is None else out
+        two = (self.nz, self.NumG)
+        _lib.check(self._L.cgd_interpolate_wb(self.h, _ptr(u, two), _ptr(v, two), _ptr(w, two), ip, OP,
+                                              _ptr(out, (OP, OP, self.nz, self.NF), True)), "cgd_interpolate_wb")
+        return out
+
+    def interpolate_vort(self, U, inter, out=None):
+        """InterpolateVortGPU!: element-local vertical vorticity of the state."""
+        inter, OP, ip = self._inter(inter)
+        out = self._cells(U, OP) if out is None else out
+        _lib.check(self._L.cgd_interpolate_vort(self.h, _ptr(U, self.shape), ip, OP,
+                                                _ptr(out, (OP, OP, self.nz, self.NF), True)), "cgd_interpolate_vort")
+        return out
+
+    def output_fields(self, U, fields, inter, out=None):
+        """The listed quantities (_lib.OUT_* codes) of the state in one call:
+        out holds len(fields) cell arrays (OrdPrint, OrdPrint, nz, NF) back
+        to back (numpy: shape (nfields, NF, nz, OP, OP); torch: flat)."""
+        inter, OP, ip = self._inter(inter)
+        codes = np.ascontiguousarray(fields, dtype=np.int32)
+        n = OP * OP * self.nz * self.NF * codes.size
+        if out is None:
+            if isinstance(U, np.ndarray):
+                out = np.zeros((codes.size, self.NF, self.nz, OP, OP))
+            else:
+                import torch
+                out = torch.empty(n, dtype=torch.float64, device=U.device)
+        if isinstance(out, np.ndarray):
+            if out.size != n or not out.flags.c_contiguous or out.dtype != np.float64:
+                raise ValueError("output array: C-contiguous float64 of nfields * OP^2 * nz * NF values")
+            op = out.ctypes.data
+        else:
+            if out.numel() != n or out.dtype.itemsize != 8 or not out.is_contiguous():
+                raise ValueError("output tensor: contiguous float64 of nfields * OP^2 * nz * NF values")
+            op = out.data_ptr()
+        _lib.check(self._L.cgd_output_fields(self.h, _ptr(U, self.shape), codes.ctypes.data, int(codes.size), ip, OP,
+                                             op), "cgd_output_fields")
+        return out
 
     def set_caller_stream(self, stream=None):
         """The stream whose queued work every call waits for before it reads

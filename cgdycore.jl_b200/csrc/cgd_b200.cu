@@ -10,6 +10,7 @@
 #include "cgd_phase2.cuh"
 #include "cgd_batch.cuh"
 #include "cgd_init.cuh"
+#include "cgd_output.cuh"
 #include "cgd_adjoint_launch.h"
 
 #include <cuda_runtime.h>
@@ -102,6 +103,10 @@ struct cgd_handle {
   double *sbuf = nullptr, *rbuf = nullptr;      // packed contributions, NC*nz per item
   cgd_exchange_fn xfn = nullptr;
   void *xuser = nullptr;
+  // output interpolation (allocated on first use): the weights, staged host
+  // inputs and staged host output
+  double *ointer = nullptr, *ostage = nullptr, *ocell = nullptr;
+  size_t ocell_n = 0;
   std::string last_error;
 };
 
@@ -1318,6 +1323,205 @@ int cgd_mass_integral(cgd_handle *h, const double *U, const double *MMass, doubl
   k_mass_partial<<<nb, 256, 0, h->stream>>>(Ud, mm, (long long)S, h->part);
   k_mass_final<<<1, 32, 0, h->stream>>>(h->part, nb, h->scal);
   CK(cudaMemcpyAsync(out, h->scal, 8, cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
+}
+
+// ---- output interpolation (the reference's VTK output path)
+int cgd_vtk_inter(int32_t OrdPoly, int32_t OrdPrint, const double *xw, double *inter)
+{
+  if (!xw || !inter || OrdPoly < 1 || OrdPoly > 4 || OrdPrint < 1 || OrdPrint > OUT_MAX_PRINT)
+    return CGD_ERR_INVALID_ARG;
+  const int N = OrdPoly + 1, OP = OrdPrint;
+  // DG.Lagrange (src/DG/Lagrange.jl:1-9)
+  auto lagrange = [&](double x, int iP) {
+    double f = 1.0;
+    for (int i = 0; i < N; ++i)
+      if (i != iP) f = f * (x - xw[i]) / (xw[iP] - xw[i]);
+    return f;
+  };
+  for (int i = 0; i < OP * OP * N * N; ++i) inter[i] = 0.0;
+  // the sub-cell corners as vtkStruct steps them (src/Outputs/vtkSphere.jl:199-219)
+  const double dd = 2.0 / OP;
+  double eta0 = -1.0;
+  for (int jRef = 0; jRef < OP; ++jRef) {
+    double ksi0 = -1.0;
+    const double eta1 = eta0 + dd;
+    for (int iRef = 0; iRef < OP; ++iRef) {
+      const double ksi1 = ksi0 + dd;
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) {
+          double &v = inter[iRef + OP * (jRef + OP * (i + N * j))];
+          v = v + lagrange(0.5 * (ksi0 + ksi1), i) * lagrange(0.5 * (eta0 + eta1), j);
+        }
+      ksi0 = ksi1;
+    }
+    eta0 = eta1;
+  }
+  return CGD_OK;
+}
+
+namespace {
+
+// Device copies for one interpolation call: the weights always (host or
+// device), an (nz, NumG) input into staging slot `slot` when it is host
+// memory.
+int out_prepare(cgd_handle *h, const double *inter, int OP)
+{
+  if (OP < 1 || OP > OUT_MAX_PRINT) return CGD_ERR_INVALID_ARG;
+  if (!h->ointer) {
+    if (int rc = dalloc(h, &h->ointer, (size_t)OUT_MAX_PRINT * OUT_MAX_PRINT * 25)) return rc;
+  }
+  CK(cudaMemcpyAsync(h->ointer, inter, (size_t)OP * OP * h->DoF * 8, cudaMemcpyDefault, h->stream));
+  return CGD_OK;
+}
+
+int out_input(cgd_handle *h, const double *a, int slot, const double **dev)
+{
+  if (!a || is_device_ptr(a)) {
+    *dev = a;
+    return CGD_OK;
+  }
+  const size_t S = (size_t)h->nz * h->NumG;
+  if (!h->ostage) {
+    if (int rc = dalloc(h, &h->ostage, 3 * S)) return rc;
+  }
+  CK(cudaMemcpyAsync(h->ostage + slot * S, a, S * 8, cudaMemcpyHostToDevice, h->stream));
+  *dev = h->ostage + slot * S;
+  return CGD_OK;
+}
+
+// Device destination for `count` doubles of cell values: the caller's
+// pointer, or the handle's staging buffer for host memory.
+int out_cells(cgd_handle *h, double *cell, size_t count, double **dev)
+{
+  if (is_device_ptr(cell)) {
+    *dev = cell;
+    return CGD_OK;
+  }
+  if (h->ocell_n < count) {
+    if (h->ocell) {
+      CK(cudaStreamSynchronize(h->stream));
+      for (size_t i = 0; i < h->bufs.size(); ++i)
+        if (h->bufs[i].p == h->ocell) {
+          cudaFree(h->ocell);
+          h->bufs.erase(h->bufs.begin() + i);
+          break;
+        }
+      h->ocell = nullptr;
+      h->ocell_n = 0;
+    }
+    if (int rc = dalloc(h, &h->ocell, count)) return rc;
+    h->ocell_n = count;
+  }
+  *dev = h->ocell;
+  return CGD_OK;
+}
+
+size_t out_count(const cgd_handle *h, int OP) { return (size_t)OP * OP * h->nz * h->NF; }
+
+unsigned out_blocks(const cgd_handle *h, int OP) { return (unsigned)((out_count(h, OP) + 255) / 256); }
+
+void launch_vort(cgd_handle *h, const double *U, int OP, double *cell)
+{
+  const int N = h->N, LT = 256 / (N * N);
+  const dim3 grid((h->nz + LT - 1) / LT, h->NF);
+  switch (N) {
+    case 2: k_interp_vort<2><<<grid, 256, 0, h->stream>>>(h->gp, U, h->ointer, OP, cell); break;
+    case 3: k_interp_vort<3><<<grid, 256, 0, h->stream>>>(h->gp, U, h->ointer, OP, cell); break;
+    case 4: k_interp_vort<4><<<grid, 256, 0, h->stream>>>(h->gp, U, h->ointer, OP, cell); break;
+    default: k_interp_vort<5><<<grid, 256, 0, h->stream>>>(h->gp, U, h->ointer, OP, cell); break;
+  }
+}
+
+}  // namespace
+
+int cgd_interpolate(cgd_handle *h, const double *c, const double *rhoc, const double *inter, int32_t OrdPrint,
+                    double *cCell)
+{
+  if (!h || !c || !inter || !cCell) return CGD_ERR_INVALID_ARG;
+  if (int erc = enter(h)) return erc;
+  if (int rc = out_prepare(h, inter, OrdPrint)) return rc;
+  const double *cd, *rd;
+  double *od;
+  if (int rc = out_input(h, c, 0, &cd)) return rc;
+  if (int rc = out_input(h, rhoc, 1, &rd)) return rc;
+  const size_t n = out_count(h, OrdPrint);
+  if (int rc = out_cells(h, cCell, n, &od)) return rc;
+  k_interp<<<out_blocks(h, OrdPrint), 256, 0, h->stream>>>(h->gp, cd, rd, INTERP_C, h->ointer, OrdPrint, od);
+  if (od != cCell) CK(cudaMemcpyAsync(cCell, od, n * 8, cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
+}
+
+int cgd_interpolate_wb(cgd_handle *h, const double *u, const double *v, const double *w, const double *inter,
+                       int32_t OrdPrint, double *cCell)
+{
+  if (!h || !u || !v || !w || !inter || !cCell) return CGD_ERR_INVALID_ARG;
+  if (int erc = enter(h)) return erc;
+  if (int rc = out_prepare(h, inter, OrdPrint)) return rc;
+  const double *ud, *vd, *wd;
+  double *od;
+  if (int rc = out_input(h, u, 0, &ud)) return rc;
+  if (int rc = out_input(h, v, 1, &vd)) return rc;
+  if (int rc = out_input(h, w, 2, &wd)) return rc;
+  const size_t n = out_count(h, OrdPrint);
+  if (int rc = out_cells(h, cCell, n, &od)) return rc;
+  k_interp_wb<<<out_blocks(h, OrdPrint), 256, 0, h->stream>>>(h->gp, ud, vd, wd, h->ointer, OrdPrint, od);
+  if (od != cCell) CK(cudaMemcpyAsync(cCell, od, n * 8, cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
+}
+
+int cgd_interpolate_vort(cgd_handle *h, const double *U, const double *inter, int32_t OrdPrint, double *cCell)
+{
+  if (!h || !U || !inter || !cCell) return CGD_ERR_INVALID_ARG;
+  if (int erc = enter(h)) return erc;
+  if (int rc = out_prepare(h, inter, OrdPrint)) return rc;
+  double *Ud, *od;
+  if (int rc = stage_in(h, U, h->Ubuf, true, &Ud)) return rc;
+  const size_t n = out_count(h, OrdPrint);
+  if (int rc = out_cells(h, cCell, n, &od)) return rc;
+  launch_vort(h, Ud, OrdPrint, od);
+  if (od != cCell) CK(cudaMemcpyAsync(cCell, od, n * 8, cudaMemcpyDeviceToHost, h->stream));
+  return finish(h);
+}
+
+int cgd_output_fields(cgd_handle *h, const double *U, const int32_t *fields, int32_t nfields, const double *inter,
+                      int32_t OrdPrint, double *out)
+{
+  if (!h || !U || !fields || nfields < 1 || !inter || !out) return CGD_ERR_INVALID_ARG;
+  for (int k = 0; k < nfields; ++k) {
+    const int f = fields[k];
+    const bool ok = (f >= CGD_OUT_RHO && f <= CGD_OUT_WB_UV) || (f >= CGD_OUT_TR && f < CGD_OUT_TR + h->NumTr);
+    if (!ok) return CGD_ERR_INVALID_ARG;
+  }
+  if (int erc = enter(h)) return erc;
+  if (int rc = out_prepare(h, inter, OrdPrint)) return rc;
+  double *Ud, *od;
+  if (int rc = stage_in(h, U, h->Ubuf, true, &Ud)) return rc;
+  const size_t n = out_count(h, OrdPrint);
+  if (int rc = out_cells(h, out, n * nfields, &od)) return rc;
+  const size_t fs = (size_t)h->nz * h->NumG;
+  const double *rho = Ud, *u = Ud + fs, *v = Ud + 2 * fs, *w = Ud + 3 * fs, *rth = Ud + 4 * fs;
+  const unsigned nb = out_blocks(h, OrdPrint);
+  const double *W = h->ointer;
+  for (int k = 0; k < nfields; ++k) {
+    double *cell = od + (size_t)k * n;
+    const int f = fields[k];
+    switch (f) {
+      case CGD_OUT_RHO: k_interp<<<nb, 256, 0, h->stream>>>(h->gp, rho, nullptr, INTERP_C, W, OrdPrint, cell); break;
+      case CGD_OUT_U: k_interp<<<nb, 256, 0, h->stream>>>(h->gp, u, nullptr, INTERP_C, W, OrdPrint, cell); break;
+      case CGD_OUT_V: k_interp<<<nb, 256, 0, h->stream>>>(h->gp, v, nullptr, INTERP_C, W, OrdPrint, cell); break;
+      case CGD_OUT_WB: k_interp_wb<<<nb, 256, 0, h->stream>>>(h->gp, u, u, w, W, OrdPrint, cell); break;
+      case CGD_OUT_WB_UV: k_interp_wb<<<nb, 256, 0, h->stream>>>(h->gp, u, v, w, W, OrdPrint, cell); break;
+      case CGD_OUT_TH: k_interp<<<nb, 256, 0, h->stream>>>(h->gp, rth, rho, INTERP_POTT, W, OrdPrint, cell); break;
+      case CGD_OUT_PRES: k_interp<<<nb, 256, 0, h->stream>>>(h->gp, rth, nullptr, INTERP_PRES, W, OrdPrint, cell); break;
+      case CGD_OUT_VORT: launch_vort(h, Ud, OrdPrint, cell); break;
+      default:   // tracer ratio rho*q / rho
+        k_interp<<<nb, 256, 0, h->stream>>>(h->gp, Ud + (size_t)(5 + f - CGD_OUT_TR) * fs, rho, INTERP_C, W, OrdPrint,
+                                            cell);
+        break;
+    }
+  }
+  if (od != out) CK(cudaMemcpyAsync(out, od, n * nfields * 8, cudaMemcpyDeviceToHost, h->stream));
   return finish(h);
 }
 

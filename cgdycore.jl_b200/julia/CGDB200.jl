@@ -8,6 +8,9 @@
 #   Jac!             = DyCore.JacSchurGPU!  (src/DyCore/JacSchur.jl:3)
 #   RosenbrockSchur! = Integration.RosenbrockSchur! (src/Integration/RosenbrockSchur.jl:1)
 #
+# and for the VTK output, the interpolation kernels of
+# Outputs.unstructured_vtkSphere (src/Outputs/vtkOutputKernel.jl).
+#
 # The arguments are the reference's own (CG, Metric, Phys, Cache, Exchange,
 # Global, Param, DiscType); the library keeps its device copies of the grid
 # in a handle created once from them.  State arrays (CuArray or Array,
@@ -282,6 +285,75 @@ function RosenbrockStepAdjointB200!(Lin, U0, Lout, dt, CG, Metric, Phys, Global)
     check(ccall((:cgd_ros_step_adjoint, libcgd), Cint,
                 (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Cdouble),
                 h.ptr, dptr(U0), dptr(Lout), dptr(Lin), dt), "cgd_ros_step_adjoint")
+  end
+end
+
+# ---- Output interpolation (src/Outputs/vtkOutputKernel.jl).  The reference's
+# kernels take (cCell, c, Inter, Glob); these take the model's Global instead
+# of Glob (the handle holds Glob and the metric).  Inter and the arrays may be
+# host Arrays or CuArrays; column slices such as U[:,:,RhoPos] are contiguous.
+
+# vtkStruct's vtkInter (src/Outputs/vtkSphere.jl:199-219) from CG.xwCPU.
+function VtkInterB200(OrdPoly, OrdPrint, xw)
+  inter = zeros(Float64, OrdPrint, OrdPrint, OrdPoly + 1, OrdPoly + 1)
+  x = Vector{Float64}(xw)
+  check(ccall((:cgd_vtk_inter, libcgd), Cint, (Int32, Int32, Ptr{Float64}, Ptr{Float64}),
+              OrdPoly, OrdPrint, x, inter), "cgd_vtk_inter")
+  inter
+end
+
+# InterpolateGPU!(cCell, c, Inter, Glob) (vtkOutputKernel.jl:215)
+function InterpolateB200!(cCell, c, Inter, Global)
+  h = handle(Global)
+  GC.@preserve cCell c Inter begin
+    check(ccall((:cgd_interpolate, libcgd), Cint,
+                (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int32, Ptr{Float64}),
+                h.ptr, dptr(c), C_NULL, dptr(Inter), size(Inter, 1), dptr(cCell)), "cgd_interpolate")
+  end
+end
+
+# InterpolateRhoGPU!(cCell, c, Rho, Inter, Glob) (vtkOutputKernel.jl:254)
+function InterpolateRhoB200!(cCell, c, Rho, Inter, Global)
+  h = handle(Global)
+  GC.@preserve cCell c Rho Inter begin
+    check(ccall((:cgd_interpolate, libcgd), Cint,
+                (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int32, Ptr{Float64}),
+                h.ptr, dptr(c), dptr(Rho), dptr(Inter), size(Inter, 1), dptr(cCell)), "cgd_interpolate")
+  end
+end
+
+# InterpolateWBGPU!(cCell, u, v, w, Inter, dXdxI, Glob) (vtkOutputKernel.jl:274)
+function InterpolateWBB200!(cCell, u, v, w, Inter, Global)
+  h = handle(Global)
+  GC.@preserve cCell u v w Inter begin
+    check(ccall((:cgd_interpolate_wb, libcgd), Cint,
+                (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int32, Ptr{Float64}),
+                h.ptr, dptr(u), dptr(v), dptr(w), dptr(Inter), size(Inter, 1), dptr(cCell)), "cgd_interpolate_wb")
+  end
+end
+
+# InterpolateVortGPU!(Vort, U, Inter, FE, Metric) (vtkOutputKernel.jl:186)
+function InterpolateVortB200!(Vort, U, Inter, Global)
+  h = handle(Global)
+  GC.@preserve Vort U Inter begin
+    check(ccall((:cgd_interpolate_vort, libcgd), Cint,
+                (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int32, Ptr{Float64}),
+                h.ptr, dptr(U), dptr(Inter), size(Inter, 1), dptr(Vort)), "cgd_interpolate_vort")
+  end
+end
+
+# CGD_OUT_* codes of cgd_output_fields by the reference's cNames
+const OUTPUT_CODES = Dict("Rho" => 0, "u" => 1, "v" => 2, "wB" => 3, "Th" => 4, "Pres" => 5, "Vort" => 6,
+                          "Tr1" => 16, "Tr2" => 17, "Tr3" => 18, "Tr4" => 19)
+
+# All of Global.Output.cNames in one call: out (OrdPrint, OrdPrint, nz, NF, nfields).
+function OutputFieldsB200!(out, U, cNames, Inter, Global)
+  h = handle(Global)
+  codes = Int32[OUTPUT_CODES[n] for n in cNames]
+  GC.@preserve out U Inter codes begin
+    check(ccall((:cgd_output_fields, libcgd), Cint,
+                (Ptr{Cvoid}, Ptr{Float64}, Ptr{Int32}, Int32, Ptr{Float64}, Int32, Ptr{Float64}),
+                h.ptr, dptr(U), codes, length(codes), dptr(Inter), size(Inter, 1), dptr(out)), "cgd_output_fields")
   end
 end
 

@@ -275,6 +275,58 @@ int64_t cgd_tape_bytes_per_step(const cgd_handle *h);
  * Replaces Parallels.GlobalIntegral (src/Parallels/Exchange.jl:1163-1166). */
 int cgd_mass_integral(cgd_handle *h, const double *U, const double *MMass, double *out);
 
+/* ---- Output: the state interpolated to OrdPrint x OrdPrint sub-cells per
+ * element and layer, the cell data of the reference's VTK files.
+ * inter (OrdPrint, OrdPrint, N, N): inter[I,J,i,j] = L_i(xi_I) L_j(eta_J),
+ * L the GLL Lagrange basis, (xi_I, eta_J) the sub-cell centres.
+ * cCell (OrdPrint, OrdPrint, nz, NF).  1 <= OrdPrint <= 8.  Inputs and
+ * outputs may be host or device memory (as the state pointers above). */
+
+/* The weights from the N = OrdPoly + 1 GLL points xw (host memory, no device
+ * work).  Replaces the vtkInter of Outputs.vtkStruct
+ * (src/Outputs/vtkSphere.jl:199-219). */
+int cgd_vtk_inter(int32_t OrdPoly, int32_t OrdPrint, const double *xw, double *inter);
+
+/* cCell from c (nz, NumG), each nodal value divided by rhoc (nz, NumG)
+ * first when rhoc is not NULL.  Replaces Outputs.InterpolateGPU! and
+ * InterpolateRhoGPU! (src/Outputs/vtkOutputKernel.jl:49-74,97-121,215-233,254-272). */
+int cgd_interpolate(cgd_handle *h, const double *c, const double *rhoc, const double *inter, int32_t OrdPrint,
+                    double *cCell);
+
+/* Layer-mean w (0.5 (w(l) + w(l-1)); in the lowest layer the surface value
+ * w0 = -(u dXdxI[3,1] + v dXdxI[3,2]) / dXdxI[3,3] of the lower node) from u,
+ * v, w (nz, NumG).  Replaces Outputs.InterpolateWBGPU!
+ * (src/Outputs/vtkOutputKernel.jl:123-159,274-291). */
+int cgd_interpolate_wb(cgd_handle *h, const double *u, const double *v, const double *w, const double *inter,
+                       int32_t OrdPrint, double *cCell);
+
+/* Element-local vertical vorticity of the state's u, v (no direct-stiffness
+ * summation), divided by J.  Replaces Outputs.InterpolateVortGPU!
+ * (src/Outputs/vtkOutputKernel.jl:1-47,186-212), whose atomic sums have no
+ * fixed order; here every sum runs in ascending node order. */
+int cgd_interpolate_vort(cgd_handle *h, const double *U, const double *inter, int32_t OrdPrint, double *cCell);
+
+/* Output quantities of cgd_output_fields, by the reference's cNames
+ * (unstructured_vtkSphere, src/Outputs/vtkSphere.jl:337-510). */
+#define CGD_OUT_RHO 0     /* "Rho" */
+#define CGD_OUT_U 1       /* "u" */
+#define CGD_OUT_V 2       /* "v" */
+#define CGD_OUT_WB 3      /* "wB": as the reference calls it, with u passed for v (vtkSphere.jl:401-407) */
+#define CGD_OUT_TH 4      /* "Th": (p0/p)^(Rd/Cpd) T of the dry model (Cache.AuxG[:,:,3]) */
+#define CGD_OUT_PRES 5    /* "Pres": the dry model's pressure (Cache.AuxG[:,:,1]) */
+#define CGD_OUT_VORT 6    /* "Vort" */
+#define CGD_OUT_WB_UV 7   /* layer-mean w with the surface value from u and v */
+#define CGD_OUT_TR 16     /* "Tr1" = CGD_OUT_TR, "Tr2" = CGD_OUT_TR + 1, ...: rho*q / rho */
+
+/* The listed quantities of the state U (nz, NumG, NV) in one call, each
+ * launched on the handle's stream as soon as the previous one is queued:
+ * out holds nfields cCell arrays back to back (one copy to the host at the
+ * end when out is host memory).  Replaces the interpolation and copy loop of
+ * Outputs.unstructured_vtkSphere (src/Outputs/vtkSphere.jl:356-510); the
+ * file itself is written by the caller. */
+int cgd_output_fields(cgd_handle *h, const double *U, const int32_t *fields, int32_t nfields, const double *inter,
+                      int32_t OrdPrint, double *out);
+
 /* Allocation-free Jacobian + column Schur solve.  Some callers cannot let a
  * library allocate device memory: a host runtime whose device memory belongs
  * to its own pool allocator (CUDA.jl, PyTorch), where a cudaMalloc or

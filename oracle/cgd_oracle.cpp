@@ -1824,4 +1824,143 @@ double orc_mass_integral(void *h, const double *U)
   return acc;
 }
 
+// ---------------------------------------------------------------------------
+// Output interpolation (src/Outputs).  Cell (I,J) of element IF, layer Iz:
+// the GLL interpolant at the sub-cell centre, Inter[I,J,iP,jP] summed over
+// the element's nodes in the reference's loop order (jP outer, iP inner).
+// ---------------------------------------------------------------------------
+// DG.Lagrange: src/DG/Lagrange.jl:1-9
+static double lagrange(double x, const double *xP, int n, int iP)
+{
+  double f = 1;
+  for (int i = 0; i < n; ++i)
+    if (i != iP) f = f * (x - xP[i]) / (xP[iP] - xP[i]);
+  return f;
+}
+
+int orc_vtk_inter(int OrdPoly, int OrdPrint, const double *xw, double *inter)
+{
+  // vtkStruct's vtkInter: src/Outputs/vtkSphere.jl:199-219
+  const int N = OrdPoly + 1, OP = OrdPrint;
+  std::fill(inter, inter + (size_t)OP * OP * N * N, 0.0);
+  const double dd = 2.0 / OP;
+  double eta0 = -1;
+  for (int jRef = 1; jRef <= OP; ++jRef) {
+    double ksi0 = -1;
+    const double eta1 = eta0 + dd;
+    for (int iRef = 1; iRef <= OP; ++iRef) {
+      const double ksi1 = ksi0 + dd;
+      for (int j = 1; j <= N; ++j)
+        for (int i = 1; i <= N; ++i) {
+          double &v = inter[(iRef - 1) + OP * ((jRef - 1) + OP * ((i - 1) + N * (j - 1)))];
+          v = v + lagrange(0.5 * (ksi0 + ksi1), xw, N, i - 1) * lagrange(0.5 * (eta0 + eta1), xw, N, j - 1);
+        }
+      ksi0 = ksi1;
+    }
+    eta0 = eta1;
+  }
+  return 0;
+}
+
+// kind 0: InterpolateKernel! (src/Outputs/vtkOutputKernel.jl:49-74), or with
+// rhoc InterpolateRhoKernel! (:97-121); kind 1: of the dry pressure, kind 2:
+// of the dry potential temperature (p, T, PotT of src/Models/Equation.jl:24-32,
+// c = rho*theta, rhoc = rho).
+int orc_interpolate(void *h, const double *c, const double *rhoc, int kind, const double *inter, int OP,
+                    double *cell)
+{
+  Model *m = static_cast<Model *>(h);
+  const int N = m->N, nz = m->nz, OP2 = OP * OP;
+  const Phys &ph = m->phys;
+  for (int IF = 0; IF < m->NF; ++IF)
+    for (int Iz = 0; Iz < nz; ++Iz)
+      for (int J = 0; J < OP; ++J)
+        for (int I = 0; I < OP; ++I) {
+          double acc = 0;
+          for (int jP = 0; jP < N; ++jP)
+            for (int iP = 0; iP < N; ++iP) {
+              const int iD = iP + N * jP;
+              const size_t o = Iz + (size_t)nz * m->glob[iD + (size_t)m->DoF * IF];
+              const double w = inter[I + OP * J + (size_t)OP2 * iD];
+              if (kind == 1) {
+                acc += w * pressure(ph, c[o]);
+              } else if (kind == 2) {
+                const double p = pressure(ph, c[o]);
+                const double T = p / (ph.Rd * rhoc[o]);
+                acc += w * (std::pow(ph.p0 / p, ph.Rd / ph.Cpd) * T);
+              } else if (rhoc) {
+                acc += w * c[o] / rhoc[o];
+              } else {
+                acc += w * c[o];
+              }
+            }
+          cell[I + OP * (J + (size_t)OP * (Iz + (size_t)nz * IF))] = acc;
+        }
+  return 0;
+}
+
+// InterpolateWBKernel!: src/Outputs/vtkOutputKernel.jl:123-159
+int orc_interpolate_wb(void *h, const double *u, const double *v, const double *w, const double *inter, int OP,
+                       double *cell)
+{
+  Model *m = static_cast<Model *>(h);
+  const int N = m->N, nz = m->nz, OP2 = OP * OP;
+  for (int IF = 0; IF < m->NF; ++IF)
+    for (int Iz = 0; Iz < nz; ++Iz)
+      for (int J = 0; J < OP; ++J)
+        for (int I = 0; I < OP; ++I) {
+          double acc = 0;
+          for (int jP = 0; jP < N; ++jP)
+            for (int iP = 0; iP < N; ++iP) {
+              const int iD = iP + N * jP;
+              const size_t o = Iz + (size_t)nz * m->glob[iD + (size_t)m->DoF * IF];
+              const double wi = 0.5 * inter[I + OP * J + (size_t)OP2 * iD];
+              if (Iz == 0) {
+                const double w0 = -(u[o] * DXI(*m, 3, 1, 0, iD, Iz, IF) + v[o] * DXI(*m, 3, 2, 0, iD, Iz, IF)) /
+                                  DXI(*m, 3, 3, 0, iD, Iz, IF);
+                acc += wi * (w[o] + w0);
+              } else {
+                acc += wi * (w[o] + w[o - 1]);
+              }
+            }
+          cell[I + OP * (J + (size_t)OP * (Iz + (size_t)nz * IF))] = acc;
+        }
+  return 0;
+}
+
+// InterpolateRotKernel!: src/Outputs/vtkOutputKernel.jl:1-47 (its atomic
+// sums in ascending node order: the xi sum, then the eta sum, from 0).
+int orc_interpolate_vort(void *h, const double *U, const double *inter, int OP, double *cell)
+{
+  Model *m = static_cast<Model *>(h);
+  const int N = m->N, DoF = m->DoF, nz = m->nz, OP2 = OP * OP;
+  const size_t S = (size_t)nz * m->NumG;
+  std::vector<double> tx(DoF), ty(DoF), rot(DoF);
+  for (int IF = 0; IF < m->NF; ++IF)
+    for (int Iz = 0; Iz < nz; ++Iz) {
+      for (int ID = 0; ID < DoF; ++ID) {
+        const size_t o = Iz + (size_t)nz * m->glob[ID + (size_t)DoF * IF];
+        const double uu = U[o + S], vv = U[o + 2 * S];
+        tx[ID] = (DXI(*m, 1, 1, 0, ID, Iz, IF) + DXI(*m, 1, 1, 1, ID, Iz, IF)) * vv -
+                 (DXI(*m, 1, 2, 0, ID, Iz, IF) + DXI(*m, 1, 2, 1, ID, Iz, IF)) * uu;
+        ty[ID] = (DXI(*m, 2, 1, 0, ID, Iz, IF) + DXI(*m, 2, 1, 1, ID, Iz, IF)) * vv -
+                 (DXI(*m, 2, 2, 0, ID, Iz, IF) + DXI(*m, 2, 2, 1, ID, Iz, IF)) * uu;
+      }
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) {
+          double acc = 0;
+          for (int I = 0; I < N; ++I) acc += m->DS[i + N * I] * tx[I + N * j];
+          for (int J = 0; J < N; ++J) acc += m->DS[j + N * J] * ty[i + N * J];
+          rot[i + N * j] = acc / (JJ(*m, i + N * j, 0, Iz, IF) + JJ(*m, i + N * j, 1, Iz, IF));
+        }
+      for (int J = 0; J < OP; ++J)
+        for (int I = 0; I < OP; ++I) {
+          double acc = 0;
+          for (int iD = 0; iD < DoF; ++iD) acc += inter[I + OP * J + (size_t)OP2 * iD] * rot[iD];
+          cell[I + OP * (J + (size_t)OP * (Iz + (size_t)nz * IF))] = acc;
+        }
+    }
+  return 0;
+}
+
 } // extern "C"

@@ -63,6 +63,17 @@ int orc_ros_step(void *h, double *U, double dt, int nsteps);
 /* sum(rho * MMass) */
 double orc_mass_integral(void *h, const double *U);
 
+/* Output interpolation to OrdPrint x OrdPrint sub-cells (src/Outputs):
+ * inter (OrdPrint, OrdPrint, N, N), cell (OrdPrint, OrdPrint, nz, NF).
+ * kind 0: c (divided by rhoc when not NULL), 1: dry pressure of c = rho*theta,
+ * 2: dry potential temperature of c = rho*theta and rhoc = rho. */
+int orc_vtk_inter(int OrdPoly, int OrdPrint, const double *xw, double *inter);
+int orc_interpolate(void *h, const double *c, const double *rhoc, int kind, const double *inter, int OrdPrint,
+                    double *cell);
+int orc_interpolate_wb(void *h, const double *u, const double *v, const double *w, const double *inter,
+                       int OrdPrint, double *cell);
+int orc_interpolate_vort(void *h, const double *U, const double *inter, int OrdPrint, double *cell);
+
 #ifdef __cplusplus
 }
 #endif

@@ -56,6 +56,10 @@ def lib():
         L.orc_ros_step.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int]
         L.orc_mass_integral.argtypes = [vp, vp]
         L.orc_mass_integral.restype = ctypes.c_double
+        L.orc_vtk_inter.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp]
+        L.orc_interpolate.argtypes = [vp, vp, vp, ctypes.c_int, vp, ctypes.c_int, vp]
+        L.orc_interpolate_wb.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int, vp]
+        L.orc_interpolate_vort.argtypes = [vp, vp, vp, ctypes.c_int, vp]
         _lib = L
     return _lib
 
@@ -209,3 +213,111 @@ class Oracle:
     def mass_integral(self, U):
         U = np.asfortranarray(U)
         return lib().orc_mass_integral(self.h, _p(U))
+
+    # ---- output interpolation (src/Outputs/vtkOutputKernel.jl)
+    def _cells(self, OP):
+        return np.zeros((OP, OP, self.nz, self.NF), order="F")
+
+    def interpolate(self, c, inter, rhoc=None, kind=0):
+        """InterpolateKernel! (rhoc None) / InterpolateRhoKernel!; kind 1 the
+        dry pressure of c = rho*theta, kind 2 the dry potential temperature
+        (c = rho*theta, rhoc = rho).  Cells (OP, OP, nz, NF)."""
+        inter = np.asfortranarray(inter, dtype=np.float64)
+        OP = inter.shape[0]
+        c = np.asfortranarray(c, dtype=np.float64)
+        r = np.asfortranarray(rhoc, dtype=np.float64) if rhoc is not None else None
+        out = self._cells(OP)
+        lib().orc_interpolate(self.h, _p(c), _p(r) if r is not None else None, int(kind), _p(inter), OP, _p(out))
+        return out
+
+    def interpolate_wb(self, u, v, w, inter):
+        inter = np.asfortranarray(inter, dtype=np.float64)
+        OP = inter.shape[0]
+        u, v, w = (np.asfortranarray(a, dtype=np.float64) for a in (u, v, w))
+        out = self._cells(OP)
+        lib().orc_interpolate_wb(self.h, _p(u), _p(v), _p(w), _p(inter), OP, _p(out))
+        return out
+
+    def interpolate_vort(self, U, inter):
+        inter = np.asfortranarray(inter, dtype=np.float64)
+        OP = inter.shape[0]
+        U = np.asfortranarray(U, dtype=np.float64)
+        out = self._cells(OP)
+        lib().orc_interpolate_vort(self.h, _p(U), _p(inter), OP, _p(out))
+        return out
+
+
+def vtk_inter(OrdPoly, OrdPrint, xw):
+    """vtkStruct's vtkInter (src/Outputs/vtkSphere.jl:199-219):
+    (OrdPrint, OrdPrint, N, N), Fortran order."""
+    N = OrdPoly + 1
+    xw = np.ascontiguousarray(xw, dtype=np.float64)
+    out = np.zeros(OrdPrint * OrdPrint * N * N)
+    lib().orc_vtk_inter(int(OrdPoly), int(OrdPrint), _p(xw), _p(out))
+    return out.reshape((OrdPrint, OrdPrint, N, N), order="F")
+
+
+def cell_points_loops(X, xw, OrdPrint, Rad, RadPrint=1000.0, flat=False, H=1.0, dTol=1e-8):
+    """Pure-Python loops over vtkStruct's corner points (src/Outputs/
+    vtkSphere.jl:122-178) with TransSphereX! (src/Grids/Trans.jl:77-99):
+    8 corners per sub-cell, cells ordered (iRef, jRef, iz, iF) fastest first.
+    X (N*N, 2, 3, nz, NF).  For small grids only."""
+    import math
+    DoF, _, _, nz, NF = X.shape
+    N = len(xw)
+    xwZ = [-1.0, 1.0]
+
+    def lag(x, xP, iP):
+        f = 1.0
+        for i in range(len(xP)):
+            if i != iP:
+                f = f * (x - xP[i]) / (xP[iP] - xP[i])
+        return f
+
+    def trans(ksi, eta, zeta, iz, iF):
+        XP = [0.0, 0.0, 0.0]
+        for j in range(N):
+            Lj = lag(eta, xw, j)
+            for i in range(N):
+                Li = lag(ksi, xw, i) * Lj
+                for k in range(2):
+                    Fac = Li * lag(zeta, xwZ, k)
+                    for l in range(3):
+                        XP[l] += Fac * X[i + N * j, k, l, iz, iF]
+        r = math.sqrt(XP[0] * XP[0] + XP[1] * XP[1] + XP[2] * XP[2])
+        z = max(r - Rad, 0.0)
+        return [x / r * (RadPrint + z) for x in XP]
+
+    pts = []
+    dd = 2.0 / OrdPrint
+    for iF in range(NF):
+        for iz in range(nz):
+            eta0 = -1.0
+            for jRef in range(OrdPrint):
+                ksi0 = -1.0
+                eta1 = eta0 + dd
+                for iRef in range(OrdPrint):
+                    ksi1 = ksi0 + dd
+                    corners = [(ksi0, eta0, -1.0), (ksi1, eta0, -1.0), (ksi1, eta1, -1.0), (ksi0, eta1, -1.0),
+                               (ksi0, eta0, 1.0), (ksi1, eta0, 1.0), (ksi1, eta1, 1.0), (ksi0, eta1, 1.0)]
+                    x = [trans(a, b, c, iz, iF) for a, b, c in corners]
+                    if flat:
+                        sph = []
+                        for (xx, yy, zz) in x:   # Grids.cart2sphere (src/Grids/Geometry.jl:65-75)
+                            r = math.sqrt(xx * xx + yy * yy + zz * zz)
+                            lam = math.atan2(yy, xx)
+                            if yy < 0:
+                                lam += 2 * math.pi
+                            sph.append([lam, math.asin(zz / r), r])
+                        lams = [q[0] for q in sph]
+                        if abs(min(lams) - max(lams)) > 2 * math.pi - dTol:
+                            for q in sph:
+                                if q[0] > math.pi:
+                                    q[0] -= 2 * math.pi
+                                    if q[0] > 3 * math.pi:
+                                        q[0] -= 2 * math.pi
+                        x = [[q[0], q[1], max(q[2] - Rad, 0.0) / H * 3] for q in sph]
+                    pts.extend(x)
+                    ksi0 = ksi1
+                eta0 = eta1
+    return np.array(pts).T    # (3, 8 * cells)
