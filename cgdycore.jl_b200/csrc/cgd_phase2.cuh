@@ -45,7 +45,7 @@ enum {
 // quantities of the CTA's own levels per (level, node)
 enum {
   O_D110 = 0, O_D111, O_D120, O_D121, O_D210, O_D211, O_D220, O_D221, O_J1, O_FC,
-  O_N     // the DSS'd hyperviscosity cache (5 + NumTr fields) has an array of its own, stored like T1
+  O_N     // the DSS'd hyperviscosity cache (5 + NumTr fields) is staged into the warps' scratch
 };
 
 // Warps (levels for p = 4) per CTA: 8, two 256-thread CTAs per SM at 128
@@ -56,22 +56,35 @@ enum {
 template <int N, int NT, typename R, int W = 0>
 struct P2Cfg {
   static constexpr int WARPS = W > 0 ? W : 8;
-  static constexpr int MINB = WARPS >= 16 ? 1 : 2;   // CTAs per SM the registers are sized for
   static constexpr int DoF = N * N;
   static constexpr int LPW = 32 / DoF;           // levels per warp
   static constexpr int LC = WARPS * LPW;         // levels per CTA
   static constexpr int RP = LC + 4;              // staged planes
   static constexpr int THREADS = 32 * WARPS;
   // scratch quantities per warp (the largest derivative round: 5+NT, 4+2NT,
-  // 6 for each half of the momentum round, 6+NT) and the scratch row length
+  // 6 for each half of the momentum round, 6+NT) and the scratch row length;
+  // before round 1 the scratch holds the warp's levels of the DSS'd phase-1
+  // cache (5 + NT fields, stored as R), staged with the rest
   static constexpr int NSCR = (4 + 2 * NT) > (6 + NT) ? (4 + 2 * NT) : (6 + NT);
+  static_assert(NSCR >= 5 + NT, "the scratch holds the phase-1 cache");
   static constexpr int SCS = LPW * DoF;
+  // warp stride of the scratch, odd in elements: the staging copies of the
+  // cache (consecutive threads, consecutive levels, so consecutive warps'
+  // regions) then fall into different shared-memory banks
+  static constexpr int SCW = NSCR * SCS + ((NSCR * SCS) % 2 == 0 ? 1 : 0);
   // the own levels' phase-1 cache: float in the mixed form (as stored), else double
   using CT = typename std::conditional<sizeof(R) == sizeof(float), float, double>::type;
+  static_assert(sizeof(CT) == sizeof(R), "cache and scratch share their type");
   static constexpr size_t SMEM = ((size_t)(Q_TR0 + NT) * RP * DoF + (size_t)O_N * LC * DoF +
                                    (size_t)(2 + NT) * (LC + 1) * DoF) * sizeof(double) +
-                                  (size_t)(5 + NT) * LC * DoF * sizeof(CT) +
-                                  (size_t)WARPS * NSCR * SCS * sizeof(R);
+                                  (size_t)WARPS * SCW * sizeof(R);
+  // CTAs per SM the registers are sized for (128 registers a thread).  At
+  // p = 4 with two tracers two CTAs take 154 KB of shared memory and leave
+  // about 92 KB of the SM's unified array to L1, which the 8-byte cp.async
+  // copies of the staging share sectors through: 1.347 ms per launch on the
+  // drop-in grid, against 1.656 ms with the array carved out as shared
+  // memory (28 KB of L1) and 1.901 ms with three CTAs of 80 registers.
+  static constexpr int MINB = WARPS >= 16 ? 1 : 2;
 };
 
 template <int N, int NT, typename R, int W = 0>
@@ -90,8 +103,7 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   using CTc = typename CF::CT;
   double *ow = pw + (size_t)(Q_TR0 + NT) * RP * DoF;             // [O][LC][DoF]
   double *fx = ow + (size_t)O_N * LC * DoF;                     // [2+NT][LC+1][DoF] interface fluxes
-  CTc *otc = reinterpret_cast<CTc *>(fx + (size_t)(2 + NT) * (LC + 1) * DoF);   // [5+NT][LC][DoF] cache
-  R *scr = reinterpret_cast<R *>(otc + (size_t)(5 + NT) * LC * DoF);            // [warp][NSCR][SCS]
+  R *scr = reinterpret_cast<R *>(fx + (size_t)(2 + NT) * (LC + 1) * DoF);   // [warp][SCW >= NSCR*SCS]
   const double *mte = P.met + (size_t)IF * NCOMP * cs;
 #define PW(q, p, id) pw[((size_t)(q) * RP + (p)) * DoF + (id)]
 
@@ -120,15 +132,17 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
       cp_async8(o + O_D220 * os, mt + C_D22_0 * cs); cp_async8(o + O_D221 * os, mt + C_D22_1 * cs);
       cp_async8(o + O_J1 * os, mt + C_J1 * cs);
       cp_async8(o + O_FC * os, mt + C_FCOR * cs);
-      CTc *oc = otc + (size_t)(p - 2) * DoF + ID;
+      // the cache goes to the scratch slots SC(f, ID) of the level's warp
+      const int li = p - 2;
+      CTc *oc = reinterpret_cast<CTc *>(scr) + ((size_t)(li / LPW) * CF::SCW + (li % LPW) * DoF + ID);
       if (MIX) {   // the mixed form's phase-1 cache is stored as float, and staged as float
         const float *T = reinterpret_cast<const float *>(T1) + (size_t)nz * g + lev;
 #pragma unroll
-        for (int f = 0; f < 5 + NT; ++f) cp_async4(reinterpret_cast<float *>(oc) + f * os, T + f * fs);
+        for (int f = 0; f < 5 + NT; ++f) cp_async4(reinterpret_cast<float *>(oc) + f * CF::SCS, T + f * fs);
       } else {
         const double *T = T1 + (size_t)nz * g + lev;
 #pragma unroll
-        for (int f = 0; f < 5 + NT; ++f) cp_async8(reinterpret_cast<double *>(oc) + f * os, T + f * fs);
+        for (int f = 0; f < 5 + NT; ++f) cp_async8(reinterpret_cast<double *>(oc) + f * CF::SCS, T + f * fs);
       }
     }
     cp_async8(&PW(Q_RHO, p, ID), Ug);
@@ -147,9 +161,10 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
     cp_async8(&PW(Q_M1, p, ID), P.M + lev + (size_t)nz * (g + (size_t)NumG));
     cp_async8(&PW(Q_P, p, ID), Pr + lev + (size_t)nz * g);
   }
+  // theta and the tracer ratios of the staged planes, each formed by the
+  // thread that copied its rho*theta, rho*q and rho (its own copies have
+  // landed after its wait), then one barrier
   cp_async_wait_all();
-  __syncthreads();
-  // theta and the tracer ratios of the staged planes
 #pragma unroll
   for (int r = 0; r < 2; ++r) {
     const int s = threadIdx.x + r * CF::THREADS;
@@ -207,7 +222,7 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   const int I = ID % N, Jn = ID / N;
   const int p0 = lv - (L0 - 2);          // own plane
   constexpr int SCS = CF::SCS;
-  R *sw = scr + (size_t)warp * CF::NSCR * SCS + sub * DoF;     // this level's scratch row base
+  R *sw = scr + (size_t)warp * CF::SCW + sub * DoF;     // this level's scratch row base
 #define SC(q, id) sw[(q) * SCS + (id)]
 
   // derivative coefficients of this node
@@ -220,7 +235,7 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   // own quantities
   const int li = lv - L0;                // own row of the per-level arrays
 #define OW(q) ow[((size_t)(q) * LC + li) * DoF + ID]
-#define OT(f) otc[((size_t)(f) * LC + li) * DoF + ID]   // own level's DSS'd phase-1 cache
+#define OT(f) SC(f, ID)   // own level's DSS'd phase-1 cache, in the scratch until round 1 overwrites it
   double rho = 1, u = 0, v = 0, wl = 0, wh = 0, M0 = 1, M1 = 0, MC = 1, Js = 1, J0 = 0, J1 = 0;
   double e310 = 0, e311 = 0, e320 = 0, e321 = 0, e330 = 1, e331 = 1;
   if (act) {
@@ -246,13 +261,14 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   // ---- round 1: first derivatives of the DSS'd hyperviscosity cache ----
   if (act) {
     const R d11 = (R)(D11), d12 = (R)(D12), d21 = (R)(D21), d22 = (R)(D22);
-    const R c1 = (R)OT(0), c2 = (R)OT(1), c3 = (R)OT(2), c4 = (R)OT(3), c5 = (R)OT(4);
+    // each lane reads and writes only its own column ID of the scratch; the
+    // tracer caches stay in place as SC(5 + q)
+    const R c1 = OT(0), c2 = OT(1), c3 = OT(2), c4 = OT(3), c5 = OT(4);
     SC(0, ID) = d11 * c2 - d12 * c1;       // Curl12(Cache1, Cache2)
     SC(1, ID) = d21 * c2 - d22 * c1;
     SC(2, ID) = d11 * c3 + d12 * c4;       // Contra12(Cache3, Cache4)
     SC(3, ID) = d21 * c3 + d22 * c4;
     SC(4, ID) = c5;
-    for (int q = 0; q < NT; ++q) SC(5 + q, ID) = (R)OT(5 + q);
   }
   __syncwarp();
   R b1 = 0, b2 = 0, b3 = 0, b4 = 0;
