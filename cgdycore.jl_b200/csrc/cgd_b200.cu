@@ -170,13 +170,23 @@ bool is_device_ptr(const void *p)
 }
 
 
+template <int N, int NT, typename R>
+void launch_hv1r(cgd_handle *h, const double *U, double *C)
+{
+  using T = HV1Tile<N, R>;
+  constexpr size_t smem = HV1Smem<N, NT, R, T::LT>::BYTES;
+  static std::atomic<unsigned long long> attr{0};
+  if (first_on_device(attr))
+    cudaFuncSetAttribute(k_hypervisc1<N, NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  dim3 grid((h->nz + T::LT - 1) / T::LT, h->NF);   // the level tiles of one element run back to back
+  k_hypervisc1<N, NT, R><<<grid, T::THREADS, smem, h->stream>>>(h->gp, U, C);
+}
+
 template <int N, int NT>
 void launch_hv1t(cgd_handle *h, const double *U, double *C)
 {
-  constexpr int LT = 256 / (N * N);
-  dim3 grid((h->nz + LT - 1) / LT, h->NF);   // the level tiles of one element run back to back
-  if (h->mix) k_hypervisc1<N, NT, float><<<grid, 256, 0, h->stream>>>(h->gp, U, C);
-  else k_hypervisc1<N, NT, double><<<grid, 256, 0, h->stream>>>(h->gp, U, C);
+  if (h->mix) launch_hv1r<N, NT, float>(h, U, C);
+  else launch_hv1r<N, NT, double>(h, U, C);
 }
 
 template <int N>

@@ -171,11 +171,26 @@ __device__ __forceinline__ void recu4(double cLL, double cL, double cR, double c
 // shared arrays of phase 1: planes 0-3 curl/contra of (u,v), 4 theta, 5-8
 // the first derivatives, then per tracer its ratio and the two components of
 // its gradient, each LT levels x DoF nodes
-template <int N, int NT, typename R>
+template <int N, int NT, typename R, int LT_ = 256 / (N * N)>
 struct HV1Smem {
-  static constexpr int DoF = N * N, LT = 256 / DoF;
+  static constexpr int DoF = N * N, LT = LT_;
   static constexpr int PLANES = 9 + 3 * NT;
   static constexpr size_t BYTES = (size_t)PLANES * LT * DoF * sizeof(R);
+};
+
+// Level tile of k_hypervisc1.  At p = 4 in FP64, 16 levels (400 threads,
+// three CTAs per SM): a warp then reads runs of 16 consecutive levels of two
+// nodes instead of 10 levels of three or four, so the metric and state loads
+// touch fewer L1 lines (the kernel is bound by the L1/shared-memory pipe):
+// 0.416 -> 0.310 ms on the drop-in grid.  Elsewhere 256 / N^2 levels (256
+// threads, four CTAs per SM), which the FP32 form also keeps (0.286 ms against
+// 0.316 ms with 16 levels).
+template <int N, typename R>
+struct HV1Tile {
+  static constexpr bool WIDE = N == 5 && sizeof(R) == sizeof(double);
+  static constexpr int LT = WIDE ? 16 : 256 / (N * N);
+  static constexpr int THREADS = WIDE ? LT * N * N : 256;
+  static constexpr int MINB = WIDE ? 3 : 4;
 };
 template <int N, int NT, typename R>
 __device__ __forceinline__ R *hv1_static_smem()
@@ -186,13 +201,12 @@ __device__ __forceinline__ R *hv1_static_smem()
 }
 
 // sbuf: the shared arrays (hv1_static_smem, or a kernel's dynamic buffer)
-template <int N, int NT, typename R>
+template <int N, int NT, typename R, int LT = 256 / (N * N)>
 __device__ __forceinline__ void hypervisc1_body(const GP &P, const double *__restrict__ U, double *__restrict__ C,
                                                 const int tile, const int IF, R *sbuf)
 {
   constexpr bool MIX = sizeof(R) == sizeof(float);
   constexpr int DoF = N * N;
-  constexpr int LT = 256 / DoF;
   R(*s)[LT * DoF] = reinterpret_cast<R(*)[LT * DoF]>(sbuf);
   const int t = threadIdx.x;
   const int lvl = t % LT, ID = t / LT;
@@ -313,11 +327,13 @@ __device__ __forceinline__ void hypervisc1_body(const GP &P, const double *__res
   }
 }
 
+// Shared arrays: HV1Smem<N, NT, R, HV1Tile<N, R>::LT>::BYTES of dynamic shared memory.
 template <int N, int NT, typename R>
-__global__ void __launch_bounds__(256, 4) k_hypervisc1(const GP P, const double *__restrict__ U,
-                                                      double *__restrict__ C)
+__global__ void __launch_bounds__(HV1Tile<N, R>::THREADS, HV1Tile<N, R>::MINB)
+    k_hypervisc1(const GP P, const double *__restrict__ U, double *__restrict__ C)
 {
-  hypervisc1_body<N, NT, R>(P, U, C, blockIdx.x, blockIdx.y, hv1_static_smem<N, NT, R>());
+  extern __shared__ __align__(16) unsigned char hv1_dyn[];
+  hypervisc1_body<N, NT, R, HV1Tile<N, R>::LT>(P, U, C, blockIdx.x, blockIdx.y, reinterpret_cast<R *>(hv1_dyn));
 }
 
 // Contributions and the phase-1 cache: double, or float in the mixed form
