@@ -252,15 +252,19 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   }
   const double rJs = 1.0 / Js, rMC = 1.0 / MC;
   (void)rJs; (void)rMC;
-  // the horizontal metric of the own level, re-read from shared memory where used
-#define D11 (OW(O_D110) + OW(O_D111))
-#define D12 (OW(O_D120) + OW(O_D121))
-#define D21 (OW(O_D210) + OW(O_D211))
-#define D22 (OW(O_D220) + OW(O_D221))
+  // the horizontal metric of the own level, held in registers through the
+  // rounds (each __syncwarp would otherwise make the compiler re-read it from
+  // shared memory): the components and the sums over the two nodes
+  double c110 = 0.0, c111 = 0.0, c120 = 0.0, c121 = 0.0, c210 = 0.0, c211 = 0.0, c220 = 0.0, c221 = 0.0;
+  if (act) {
+    c110 = OW(O_D110); c111 = OW(O_D111); c120 = OW(O_D120); c121 = OW(O_D121);
+    c210 = OW(O_D210); c211 = OW(O_D211); c220 = OW(O_D220); c221 = OW(O_D221);
+  }
+  const double d11s = c110 + c111, d12s = c120 + c121, d21s = c210 + c211, d22s = c220 + c221;
 
   // ---- round 1: first derivatives of the DSS'd hyperviscosity cache ----
   if (act) {
-    const R d11 = (R)(D11), d12 = (R)(D12), d21 = (R)(D21), d22 = (R)(D22);
+    const R d11 = (R)d11s, d12 = (R)d12s, d21 = (R)d21s, d22 = (R)d22s;
     // each lane reads and writes only its own column ID of the scratch; the
     // tracer caches stay in place as SC(5 + q)
     const R c1 = OT(0), c2 = OT(1), c3 = OT(2), c4 = OT(3), c5 = OT(4);
@@ -274,7 +278,7 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   R b1 = 0, b2 = 0, b3 = 0, b4 = 0;
   R e3t[NT > 0 ? NT : 1], e4t[NT > 0 ? NT : 1];
   if (act) {
-    const R d11 = (R)(D11), d12 = (R)(D12), d21 = (R)(D21), d22 = (R)(D22);
+    const R d11 = (R)d11s, d12 = (R)d12s, d21 = (R)d21s, d22 = (R)d22s;
     {
       R Dxc = DI[0] * SC(4, N * Jn), Dyc = DJ[0] * SC(4, I);
       R cu = DI[0] * SC(0, N * Jn) + DJ[0] * SC(1, I);
@@ -340,7 +344,7 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
       DyDiv = rsum1(DyDiv, WJ[k], SC(1, I + N * k));
       DivTh = rsum2(DivTh, WI[k], SC(2, k + N * Jn), WJ[k], SC(3, I + N * k));
     }
-    const R d11 = (R)(D11), d12 = (R)(D12), d21 = (R)(D21), d22 = (R)(D22);
+    const R d11 = (R)d11s, d12 = (R)d12s, d21 = (R)d21s, d22 = (R)d22s;
     const R FuC = d12 * DxCurl + d22 * DyCurl;
     const R FvC = -d11 * DxCurl - d21 * DyCurl;
     const R FuD = d11 * DxDiv + d21 * DyDiv;
@@ -382,8 +386,8 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   const double tw0 = e320 * u - e310 * v, tw1 = e321 * u - e311 * v;
   R U1 = 0, U2 = 0, V1 = 0, V2 = 0, W1 = 0, W2 = 0;
   if (act) {
-    const R d110 = (R)OW(O_D110), d111 = (R)OW(O_D111), d120 = (R)OW(O_D120), d121 = (R)OW(O_D121);
-    const R d210 = (R)OW(O_D210), d220 = (R)OW(O_D220), d221 = (R)OW(O_D221);
+    const R d110 = (R)c110, d111 = (R)c111, d120 = (R)c120, d121 = (R)c121;
+    const R d210 = (R)c210, d220 = (R)c220, d221 = (R)c221;
     const R wlR = (R)wl, whR = (R)wh;
     SC(0, ID) = -d120 * wlR;  SC(1, ID) = -d121 * whR;    // tempuZ1
     SC(2, ID) = -d220 * wlR;  SC(3, ID) = -d221 * whR;    // tempuZ2
@@ -405,8 +409,8 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   }
   __syncwarp();
   if (act) {
-    const R d110 = (R)OW(O_D110), d111 = (R)OW(O_D111), d120 = (R)OW(O_D120), d121 = (R)OW(O_D121);
-    const R d210 = (R)OW(O_D210), d211 = (R)OW(O_D211), d220 = (R)OW(O_D220), d221 = (R)OW(O_D221);
+    const R d110 = (R)c110, d111 = (R)c111, d120 = (R)c120, d121 = (R)c121;
+    const R d210 = (R)c210, d211 = (R)c211, d220 = (R)c220, d221 = (R)c221;
     const R uR = (R)u, vR = (R)v, whR = (R)wh;
     SC(0, ID) = -d111 * whR;                              // tempvZ1 (upper)
     SC(1, ID) = -d211 * whR;                              // tempvZ2 (upper)
@@ -479,7 +483,7 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
   const double K1s = 0.5 * (u * u + v * v) + 0.5 * (wl * wl);   // K on the bottom node
   const double K2s = 0.5 * (u * u + v * v) + 0.5 * (wh * wh);   // K on the top node
   if (act) {
-    const double d11 = D11, d12 = D12, d21 = D21, d22 = D22;
+    const double d11 = d11s, d12 = d12s, d21 = d21s, d22 = d22s;
     SC(0, ID) = (R)K1s;
     SC(1, ID) = (R)K2s;
     SC(2, ID) = (R)(-rho * (d11 * u + d12 * v));           // Contra12(-Rho, u, v)
@@ -514,8 +518,8 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
       DXp = rsum1(DXp, DI[k], pa[k + N * Jn]);
       DYp = rsum1(DYp, DJ[k], pa[I + N * k]);
     }
-    const double d110 = OW(O_D110), d111 = OW(O_D111), d120 = OW(O_D120), d121 = OW(O_D121);
-    const double d210 = OW(O_D210), d211 = OW(O_D211), d220 = OW(O_D220), d221 = OW(O_D221);
+    const double d110 = c110, d111 = c111, d120 = c120, d121 = c121;
+    const double d210 = c210, d211 = c211, d220 = c220, d221 = c221;
     const double d11 = d110 + d111, d12 = d120 + d121, d21 = d210 + d211, d22 = d220 + d221;
     double GuF1 = -(d110 * DXK1 + d210 * DYK1);
     double GvF1 = -(d120 * DXK1 + d220 * DYK1);
@@ -606,10 +610,6 @@ __device__ __forceinline__ void phase2_body(const GP &P, const double *__restric
 #undef CGD_DIVR
 #undef FX
 #undef CGD_DIVW
-#undef D11
-#undef D12
-#undef D21
-#undef D22
 #undef OW
 #undef OT
 #undef SC
