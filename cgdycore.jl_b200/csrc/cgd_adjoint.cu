@@ -23,7 +23,9 @@ cudaError_t rhs_adjoint_t(const GP &gp, const double *U, const double *T1, const
   if (e != cudaSuccess) return e;
   const dim3 grid((gp.nz + CF::LC - 1) / CF::LC, gp.NF);
   k_phase2_adj<N><<<grid, CF::THREADS, CF::SMEM, stream>>>(gp, U, pres, T1, LF, LU, LT1);
-  k_hypervisc1_adj<N><<<grid, CF::THREADS, 0, stream>>>(gp, U, LT1, LU);
+  using HT = AdjHV1Tile<N>;
+  const dim3 grid1((gp.nz + HT::LT - 1) / HT::LT, gp.NF);
+  k_hypervisc1_adj<N><<<grid1, HT::THREADS, 0, stream>>>(gp, U, LT1, LU);
   return cudaGetLastError();
 }
 

@@ -624,24 +624,33 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS, 2) k_phase2_adj(const GP P, co
 
 // Reverse of phase 1 (no tracers), given lambda_T1 (the adjoint of the DSS'd
 // cache, broadcast to the element nodes).  Phase 1 is linear in u, v and
-// theta = rho*theta / rho.
+// theta = rho*theta / rho.  Laid out like the forward phase 1: one CTA per
+// (element, tile of LT levels), one thread per (node, level), level fastest,
+// so the metric, cache and state loads and the atomic adds into LU are runs
+// of consecutive levels; the two derivative rounds meet at CTA barriers.
 template <int N>
-__global__ void __launch_bounds__(32 * ADJ_WARPS, 5) k_hypervisc1_adj(const GP P, const double *__restrict__ U,
-                                                                  const double *__restrict__ LT1,
-                                                                  double *__restrict__ LU)
+struct AdjHV1Tile {
+  static constexpr int LT = N == 5 ? 16 : 256 / (N * N);
+  static constexpr int THREADS = LT * N * N;
+};
+
+template <int N>
+__global__ void __launch_bounds__(AdjHV1Tile<N>::THREADS, 3) k_hypervisc1_adj(const GP P, const double *__restrict__ U,
+                                                                          const double *__restrict__ LT1,
+                                                                          double *__restrict__ LU)
 {
-  constexpr int DoF = N * N, LPW = 32 / DoF, LC = ADJ_WARPS * LPW;
-  __shared__ double scr[ADJ_WARPS][5][32];
+  constexpr int DoF = N * N, LT = AdjHV1Tile<N>::LT;
+  __shared__ double s[5][LT * DoF];
   const int nz = P.nz, NumG = P.NumG;
   const int IF = blockIdx.y;
   const size_t cs = (size_t)DoF * nz, fs = (size_t)nz * NumG;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int sub = lane / DoF, ID = lane - sub * DoF;
-  const int l = blockIdx.x * LC + warp * LPW + sub;
-  const bool act = sub < LPW && l < nz;
+  const int t = threadIdx.x;
+  const int lvl = t % LT, ID = t / LT;
+  const int l = blockIdx.x * LT + lvl;
+  const bool act = ID < DoF && l < nz;
   const int I = ID % N, Jn = ID / N;
-  double *sw = &scr[warp][0][sub * DoF];
-#define SC(q, id) sw[(q) * 32 + (id)]
+  const int si = lvl * DoF + ID, row = lvl * DoF;
+#define SC(q, id) s[q][row + (id)]
   double DTI[N], DTJ[N], WTI[N], WTJ[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) {
@@ -651,7 +660,7 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS, 5) k_hypervisc1_adj(const GP P
     WTJ[k] = P.DW[k + N * Jn];
   }
   int g = 0;
-  double d11 = 0, d12 = 0, d21 = 0, d22 = 0, Js = 1, MC = 1, a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0;
+  double d11 = 0, d12 = 0, d21 = 0, d22 = 0, Js = 1, MC = 1;
   if (act) {
     g = P.glob[IF * DoF + ID];
     const double *mt = P.met + ((size_t)IF * NCOMP * DoF + ID) * nz + l;
@@ -665,14 +674,13 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS, 5) k_hypervisc1_adj(const GP P
     // out0 = -FuC/MC, out1 = -FvC/MC, out2 = FuD/MC, out3 = FvD/MC, out4 = DivTh/MC
     const double iMC = 1.0 / MC;
     const double aFuC = -L[0] * iMC, aFvC = -L[fs] * iMC, aFuD = L[2 * fs] * iMC, aFvD = L[3 * fs] * iMC;
-    a4 = L[4 * fs] * iMC;   // DivTh
-    a0 = d12 * aFuC - d11 * aFvC;   // DxCurl
-    a1 = d22 * aFuC - d21 * aFvC;   // DyCurl
-    a2 = d11 * aFuD + d12 * aFvD;   // DxDiv
-    a3 = d21 * aFuD + d22 * aFvD;   // DyDiv
+    s[4][si] = L[4 * fs] * iMC;           // DivTh
+    s[0][si] = d12 * aFuC - d11 * aFvC;   // DxCurl
+    s[1][si] = d22 * aFuC - d21 * aFvC;   // DyCurl
+    s[2][si] = d11 * aFuD + d12 * aFvD;   // DxDiv
+    s[3][si] = d21 * aFuD + d22 * aFvD;   // DyDiv
   }
-  if (act) { SC(0, ID) = a0; SC(1, ID) = a1; SC(2, ID) = a2; SC(3, ID) = a3; SC(4, ID) = a4; }
-  __syncwarp();
+  __syncthreads();
   double as5 = 0, as6 = 0, as7 = 0, as8 = 0;
   if (act) {
 #pragma unroll
@@ -683,17 +691,17 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS, 5) k_hypervisc1_adj(const GP P
       as8 += WTJ[k] * SC(4, I + N * k);
     }
   }
-  __syncwarp();
+  __syncthreads();
   // s5 = cu/Js, s6 = dv/Js, s7 = d11 GDx + d12 GDy, s8 = d21 GDx + d22 GDy,
   // GDx = (d11 Dxc + d21 Dyc)/Js, GDy = (d12 Dxc + d22 Dyc)/Js
   if (act) {
     const double aGDx = d11 * as7 + d21 * as8, aGDy = d12 * as7 + d22 * as8, iJs = 1.0 / Js;
-    SC(0, ID) = as5 * iJs;
-    SC(1, ID) = as6 * iJs;
-    SC(2, ID) = (d11 * aGDx + d12 * aGDy) * iJs;
-    SC(3, ID) = (d21 * aGDx + d22 * aGDy) * iJs;
+    s[0][si] = as5 * iJs;
+    s[1][si] = as6 * iJs;
+    s[2][si] = (d11 * aGDx + d12 * aGDy) * iJs;
+    s[3][si] = (d21 * aGDx + d22 * aGDy) * iJs;
   }
-  __syncwarp();
+  __syncthreads();
   if (!act) return;
   double as0 = 0, as1 = 0, as2 = 0, as3 = 0, as4 = 0;
 #pragma unroll
