@@ -88,20 +88,27 @@ struct AdjCfg {
   static constexpr int LC = ADJ_WARPS * LPW;
   static constexpr int RP = LC + 4;
   static constexpr int THREADS = 32 * ADJ_WARPS;
-  static constexpr size_t SMEM =
-      ((size_t)A_NQ * RP * DoF + (size_t)B_NQ * LC * DoF + (size_t)ADJ_WARPS * ADJ_NS * 32) * sizeof(double);
+  // staged planes, own-level quantities, per-warp scratch, and the limiter
+  // coefficients of the LC + 1 interfaces L0-1 .. L0+LC-1
+  static constexpr size_t SMEM = ((size_t)A_NQ * RP * DoF + (size_t)B_NQ * LC * DoF + (size_t)ADJ_WARPS * ADJ_NS * 32 +
+                                  (size_t)4 * (LC + 1) * DoF) * sizeof(double);
 };
 
-// Stage the planes L0-2 .. L0+LC+1 of one element (as the forward kernel).
+// Stage the planes L0-2 .. L0+LC+1 of one element (as the forward kernel):
+// every value is copied with cp.async, so all of a thread's copies are in
+// flight at once; after its own copies land, the thread forms 1/rho, theta
+// and dp/d(rho*theta) of its slots.  The caller's barrier follows.
 template <int N>
 __device__ __forceinline__ void adj_stage(const GP &P, const double *__restrict__ U, const double *__restrict__ Pr,
-                                          const double *__restrict__ T1, double *pw, double *ow, int IF, int L0)
+                                          const double *__restrict__ T1, double *pw, double *ow, double *rk, int IF,
+                                          int L0)
 {
   using CF = AdjCfg<N>;
   constexpr int DoF = CF::DoF, LC = CF::LC, RP = CF::RP;
   const int nz = P.nz, NumG = P.NumG;
   const size_t cs = (size_t)DoF * nz, fs = (size_t)nz * NumG;
   const double *mte = P.met + (size_t)IF * NCOMP * cs;
+#define AWs(q) pw[((q) * RP + p) * DoF + ID]
   for (int s = threadIdx.x; s < DoF * RP; s += CF::THREADS) {
     const int ID = s / RP, p = s % RP;
     const int lev = L0 - 2 + p;
@@ -109,40 +116,53 @@ __device__ __forceinline__ void adj_stage(const GP &P, const double *__restrict_
     const int g = P.glob[IF * DoF + ID];
     const double *Ug = U + (size_t)nz * g + lev;
     const double *mt = mte + (size_t)ID * nz + lev;
-#define AWs(q) pw[((q) * RP + p) * DoF + ID]
-    const double rho = Ug[0], rth = Ug[4 * fs];
-    AWs(A_RHO) = rho;
-    AWs(A_IR) = 1.0 / rho;
-    AWs(A_TH) = rth / rho;
+    cp_async8(&AWs(A_RHO), Ug);
+    cp_async8(&AWs(A_TH), Ug + 4 * fs);   // rho*theta for now
+    if (p >= 1 && p <= LC + 1 && lev < nz - 1) {   // interface lev, between levels lev and lev + 1
+      double *r = rk + (size_t)(p - 1) * DoF + ID;
+      constexpr size_t rs = (size_t)(LC + 1) * DoF;
+      cp_async8(r, mt + C_RK0 * cs); cp_async8(r + rs, mt + C_RK1 * cs);
+      cp_async8(r + 2 * rs, mt + C_RK2 * cs); cp_async8(r + 3 * rs, mt + C_RK3 * cs);
+    }
     if (p >= 2 && p <= LC + 1) {
       double *o = ow + (size_t)(p - 2) * DoF + ID;
       constexpr size_t os = (size_t)LC * DoF;
-      o[B_D110 * os] = mt[C_D11_0 * cs]; o[B_D111 * os] = mt[C_D11_1 * cs];
-      o[B_D120 * os] = mt[C_D12_0 * cs]; o[B_D121 * os] = mt[C_D12_1 * cs];
-      o[B_D210 * os] = mt[C_D21_0 * cs]; o[B_D211 * os] = mt[C_D21_1 * cs];
-      o[B_D220 * os] = mt[C_D22_0 * cs]; o[B_D221 * os] = mt[C_D22_1 * cs];
-      o[B_J1 * os] = mt[C_J1 * cs];
-      o[B_FC * os] = mt[C_FCOR * cs];
+      cp_async8(o + B_D110 * os, mt + C_D11_0 * cs); cp_async8(o + B_D111 * os, mt + C_D11_1 * cs);
+      cp_async8(o + B_D120 * os, mt + C_D12_0 * cs); cp_async8(o + B_D121 * os, mt + C_D12_1 * cs);
+      cp_async8(o + B_D210 * os, mt + C_D21_0 * cs); cp_async8(o + B_D211 * os, mt + C_D21_1 * cs);
+      cp_async8(o + B_D220 * os, mt + C_D22_0 * cs); cp_async8(o + B_D221 * os, mt + C_D22_1 * cs);
+      cp_async8(o + B_J1 * os, mt + C_J1 * cs);
+      cp_async8(o + B_FC * os, mt + C_FCOR * cs);
       if (T1) {
         const double *T = T1 + (size_t)nz * g + lev;
-        for (int f = 0; f < 5; ++f) o[(B_C1 + f) * os] = T[f * fs];
+        for (int f = 0; f < 5; ++f) cp_async8(o + (B_C1 + f) * os, T + f * fs);
       }
     }
     if (p == 0 || p == RP - 1) continue;
-    AWs(A_U) = Ug[fs];
-    AWs(A_V) = Ug[2 * fs];
-    AWs(A_W) = Ug[3 * fs];
-    AWs(A_D310) = mt[C_D31_0 * cs]; AWs(A_D311) = mt[C_D31_1 * cs];
-    AWs(A_D320) = mt[C_D32_0 * cs]; AWs(A_D321) = mt[C_D32_1 * cs];
-    AWs(A_D330) = mt[C_D33_0 * cs]; AWs(A_D331) = mt[C_D33_1 * cs];
-    AWs(A_J0) = mt[C_J0 * cs];
-    AWs(A_M0) = P.M[lev + (size_t)nz * g];
-    AWs(A_M1) = P.M[lev + (size_t)nz * (g + (size_t)NumG)];
-    const double pr = Pr ? Pr[lev + (size_t)nz * g] : 0.0;
-    AWs(A_P) = pr;
-    AWs(A_DPD) = pr / ((1.0 - P.kappa) * rth);   // dp/d(rho*theta)
-#undef AWs
+    cp_async8(&AWs(A_U), Ug + fs);
+    cp_async8(&AWs(A_V), Ug + 2 * fs);
+    cp_async8(&AWs(A_W), Ug + 3 * fs);
+    cp_async8(&AWs(A_D310), mt + C_D31_0 * cs); cp_async8(&AWs(A_D311), mt + C_D31_1 * cs);
+    cp_async8(&AWs(A_D320), mt + C_D32_0 * cs); cp_async8(&AWs(A_D321), mt + C_D32_1 * cs);
+    cp_async8(&AWs(A_D330), mt + C_D33_0 * cs); cp_async8(&AWs(A_D331), mt + C_D33_1 * cs);
+    cp_async8(&AWs(A_J0), mt + C_J0 * cs);
+    cp_async8(&AWs(A_M0), P.M + lev + (size_t)nz * g);
+    cp_async8(&AWs(A_M1), P.M + lev + (size_t)nz * (g + (size_t)NumG));
+    if (Pr) cp_async8(&AWs(A_P), Pr + lev + (size_t)nz * g);
+    else AWs(A_P) = 0.0;
   }
+  cp_async_wait_all();
+  for (int s = threadIdx.x; s < DoF * RP; s += CF::THREADS) {
+    const int ID = s / RP, p = s % RP;
+    const int lev = L0 - 2 + p;
+    if (lev < 0 || lev >= nz) continue;
+    const double rho = AWs(A_RHO), rth = AWs(A_TH);
+    AWs(A_IR) = 1.0 / rho;
+    AWs(A_TH) = rth / rho;
+    if (p == 0 || p == RP - 1) continue;
+    AWs(A_DPD) = AWs(A_P) / ((1.0 - P.kappa) * rth);   // dp/d(rho*theta)
+  }
+#undef AWs
 }
 
 // Reverse of phase 2 (no tracers): LU += (d phase2 / d U)^T lambda and
@@ -166,13 +186,22 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS, 2) k_phase2_adj(const GP P, co
   double *pw = sm;
   double *ow = pw + (size_t)A_NQ * RP * DoF;
   double *scr = ow + (size_t)B_NQ * LC * DoF;
-  adj_stage<N>(P, U, Pr, T1, pw, ow, IF, L0);
-  __syncthreads();
-
+  double *rk = scr + (size_t)ADJ_WARPS * ADJ_NS * 32;   // [4][LC+1][DoF]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / DoF, ID = lane - sub * DoF;
   const int lv = L0 + warp * LPW + sub;
   const bool act = sub < LPW && lv < nz;
+  // lambda of this node and level, loaded while the planes are staged
+  double lam_r = 0, lam_u = 0, lam_v = 0, lam_th = 0, lam_whi = 0, lam_wlo = 0;
+  if (act) {
+    const double *L = LF + (size_t)nz * P.glob[IF * DoF + ID] + lv;
+    lam_r = L[0]; lam_u = L[fs]; lam_v = L[2 * fs]; lam_th = L[4 * fs];
+    if (lv < nz - 1) lam_whi = L[3 * fs];
+    if (lv > 0) lam_wlo = L[3 * fs - 1];
+  }
+  adj_stage<N>(P, U, Pr, T1, pw, ow, rk, IF, L0);
+  __syncthreads();
+
   const int I = ID % N, Jn = ID / N;
   const int p0 = lv - (L0 - 2), li = lv - L0;
   double *sw = scr + (size_t)warp * ADJ_NS * 32 + sub * DoF;
@@ -216,7 +245,6 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS, 2) k_phase2_adj(const GP P, co
   double d110 = 0, d111 = 0, d120 = 0, d121 = 0, d210 = 0, d211 = 0, d220 = 0, d221 = 0;
   double d11 = 0, d12 = 0, d21 = 0, d22 = 0;
   double e310 = 0, e311 = 0, e320 = 0, e321 = 0, e330 = 1, e331 = 1;
-  double lam_r = 0, lam_u = 0, lam_v = 0, lam_th = 0, lam_whi = 0, lam_wlo = 0;
   double GDx = 0, GDy = 0, U1 = 0, U2 = 0, V1 = 0, V2 = 0, W1 = 0, W2 = 0, Gradu = 0, Gradv = 0;
   double iMC = 1, iJs = 1, irho = 1, i33 = 0.5;   // reciprocals used throughout
   if (act) {
@@ -235,10 +263,6 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS, 2) k_phase2_adj(const GP P, co
     d110 = BW(B_D110, ID); d111 = BW(B_D111, ID); d120 = BW(B_D120, ID); d121 = BW(B_D121, ID);
     d210 = BW(B_D210, ID); d211 = BW(B_D211, ID); d220 = BW(B_D220, ID); d221 = BW(B_D221, ID);
     d11 = d110 + d111; d12 = d120 + d121; d21 = d210 + d211; d22 = d220 + d221;
-    const double *L = LF + (size_t)nz * g + lv;
-    lam_r = L[0]; lam_u = L[fs]; lam_v = L[2 * fs]; lam_th = L[4 * fs];
-    if (top) lam_whi = L[3 * fs];
-    if (bot) lam_wlo = L[3 * fs - 1];
     // hyperviscosity: gradient of the cached theta Laplacian
     double Dxc = 0, Dyc = 0, DXp = 0, DYp = 0;
 #pragma unroll
@@ -563,9 +587,9 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS, 2) k_phase2_adj(const GP P, co
   // ---- interface fluxes of rho and rho*theta (top: interface lv, bottom: lv-1) ----
   auto iface = [&](int il, double aWc, double aF) {
     const int pl = il - (L0 - 2);
-    const double *mt = P.met + ((size_t)IF * NCOMP * DoF + ID) * nz + il;
-    const size_t cs = (size_t)DoF * nz;
-    const double kR1 = mt[C_RK0 * cs], kL1 = mt[C_RK1 * cs], kL2 = mt[C_RK2 * cs], kR2 = mt[C_RK3 * cs];
+    const double *rki = rk + (size_t)(il - (L0 - 1)) * DoF + ID;
+    constexpr size_t rs = (size_t)(LC + 1) * DoF;
+    const double kR1 = rki[0], kL1 = rki[rs], kL2 = rki[2 * rs], kR2 = rki[3 * rs];
     const int lm = il > 0 ? il - 1 : il, lp2 = il + 2 < nz ? il + 2 : il + 1;
     const double wI = AW(A_W, pl, ID);
     const double rL = AW(A_RHO, pl, ID), uL = AW(A_U, pl, ID), vL = AW(A_V, pl, ID);
