@@ -88,10 +88,11 @@ struct AdjCfg {
   static constexpr int LC = ADJ_WARPS * LPW;
   static constexpr int RP = LC + 4;
   static constexpr int THREADS = 32 * ADJ_WARPS;
-  // staged planes, own-level quantities, per-warp scratch, and the limiter
-  // coefficients of the LC + 1 interfaces L0-1 .. L0+LC-1
+  // staged planes, own-level quantities, per-warp scratch, the limiter
+  // coefficients of the LC + 1 interfaces L0-1 .. L0+LC-1, and the CTA's sums
+  // of its state-adjoint contributions (5 fields of the RP planes)
   static constexpr size_t SMEM = ((size_t)A_NQ * RP * DoF + (size_t)B_NQ * LC * DoF + (size_t)ADJ_WARPS * ADJ_NS * 32 +
-                                  (size_t)4 * (LC + 1) * DoF) * sizeof(double);
+                                  (size_t)4 * (LC + 1) * DoF + (size_t)5 * RP * DoF) * sizeof(double);
 };
 
 // Stage the planes L0-2 .. L0+LC+1 of one element (as the forward kernel):
@@ -187,6 +188,11 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS, 2) k_phase2_adj(const GP P, co
   double *ow = pw + (size_t)A_NQ * RP * DoF;
   double *scr = ow + (size_t)B_NQ * LC * DoF;
   double *rk = scr + (size_t)ADJ_WARPS * ADJ_NS * 32;   // [4][LC+1][DoF]
+  // [5][RP][DoF]: the contributions of the CTA's nodes to the state adjoint
+  // at levels L0-2 .. L0+LC+1, summed here (shared-memory atomics) and added
+  // to LU once per (field, level, node) at the end
+  double *sacc = rk + (size_t)4 * (LC + 1) * DoF;
+  for (int s = threadIdx.x; s < 5 * RP * DoF; s += CF::THREADS) sacc[s] = 0.0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / DoF, ID = lane - sub * DoF;
   const int lv = L0 + warp * LPW + sub;
@@ -220,8 +226,7 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS, 2) k_phase2_adj(const GP P, co
   }
   const bool top = act && lv < nz - 1, bot = act && lv > 0;
   const int g = act ? P.glob[IF * DoF + ID] : 0;
-  double *LUg = LU + (size_t)nz * g;
-#define ADDU(f, lev, val) atomicAdd(LUg + (lev) + (size_t)(f) * fs, (val))
+#define ADDU(f, lev, val) atomicAdd(sacc + ((f) * RP + (lev) - (L0 - 2)) * DoF + ID, (val))
   // wl of any node of this plane (the surface value from no normal flow)
   auto wl_at = [&](int n) {
     return lv == 0 ? -(AW(A_D310, p0, n) * AW(A_U, p0, n) + AW(A_D320, p0, n) * AW(A_V, p0, n)) / AW(A_D330, p0, n)
@@ -582,7 +587,7 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS, 2) k_phase2_adj(const GP P, co
     atomicAdd(T + 3 * fs, d12 * aa3 + d22 * aa4);
     atomicAdd(T + 4 * fs, ac5);
   }
-  if (!act) return;
+  if (act) {
 
   // ---- interface fluxes of rho and rho*theta (top: interface lv, bottom: lv-1) ----
   auto iface = [&](int il, double aWc, double aF) {
@@ -640,6 +645,17 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS, 2) k_phase2_adj(const GP P, co
   ADDU(1, lv, au);
   ADDU(2, lv, av);
   ADDU(3, lv, awh);
+  }
+  // the CTA's sums into the state adjoint, level fastest
+  __syncthreads();
+  for (int s = threadIdx.x; s < 5 * RP * DoF; s += CF::THREADS) {
+    const int f = s / (RP * DoF), r = s - f * (RP * DoF);
+    const int n = r / RP, p = r - n * RP;
+    const int lev = L0 - 2 + p;
+    const double x = sacc[(f * RP + p) * DoF + n];
+    if (lev < 0 || lev >= nz || x == 0.0) continue;
+    atomicAdd(LU + (size_t)nz * P.glob[IF * DoF + n] + lev + (size_t)f * fs, x);
+  }
 #undef ADDU
 #undef SC
 #undef AW
