@@ -1903,6 +1903,12 @@ int cgd_kernel_times(cgd_handle *h, char *names, int32_t names_len, double *ms, 
 // Batched ensemble (cgd_batch_*): the members' steps as one graph of 15
 // launches over flat work lists.
 // ===========================================================================
+// Work lists of an ensemble: 0 phase-1 tiles of 256/N^2 levels, 1 column-level
+// blocks of 256 (pressure, gather), 2 phase-2 chunks, 3 column blocks, 4 phase-2
+// chunks of the 16-warp form, 5 phase-1 tiles of the split form (HV1Tile: 16
+// levels at p = 4 in FP64, else as list 0)
+constexpr int BATCH_LISTS = 6;
+
 struct cgd_batch {
   std::vector<cgd_handle *> mem;
   int N = 0, NT = 0, nzmax = 0;
@@ -1917,8 +1923,8 @@ struct cgd_batch {
   static constexpr int NORD = 3;
   static constexpr int FORM_SPLIT = 0, FORM_SPLIT16 = 1, FORM_FUSED = 2, NFORM = 3;
   static constexpr int NCAND = NFORM * NORD;
-  WItem *w[NORD][5] = {};
-  int n[5] = {};
+  WItem *w[NORD][BATCH_LISTS] = {};
+  int n[BATCH_LISTS] = {};
   cudaGraph_t graph[NCAND] = {};
   cudaGraphExec_t gexec[NCAND] = {};
   bool use[NCAND] = {};
@@ -1971,13 +1977,14 @@ int batch_fail(cgd_batch *b, cudaError_t e, const char *what)
 // Work items of every kernel of a stage for every member, in one of three
 // orders: members one after the other, the largest member first, or the
 // members' items interleaved one by one.
-void batch_lists(const cgd_batch *b, int order, std::vector<WItem> out[5])
+void batch_lists(const cgd_batch *b, int order, std::vector<WItem> out[BATCH_LISTS])
 {
   const int nm = (int)b->mem.size();
-  std::vector<std::vector<WItem>> per[5];
-  for (int k = 0; k < 5; ++k) per[k].resize(nm);
+  std::vector<std::vector<WItem>> per[BATCH_LISTS];
+  for (int k = 0; k < BATCH_LISTS; ++k) per[k].resize(nm);
   const int DoF = b->N * b->N;
   const int LT = 256 / DoF;
+  const int LTW = b->mix ? LT : (b->N == 5 ? HV1Tile<5, double>::LT : LT);   // list 5
   int LC = 0, LCA = 0;   // phase-2 levels per CTA: default, alternative (p = 4 only)
   switch (b->N) {
     case 2: LC = LCA = P2Cfg<2, 0, double>::LC; break;
@@ -1996,6 +2003,8 @@ void batch_lists(const cgd_batch *b, int order, std::vector<WItem> out[5])
     for (int c = 0; c < (h->NumG + COL_WARPS - 1) / COL_WARPS; ++c) per[3][m].push_back({m, c, 0});
     for (int IF = 0; IF < h->NF; ++IF)
       for (int c = 0; c < (h->nz + LCA - 1) / LCA; ++c) per[4][m].push_back({m, c, IF});
+    for (int IF = 0; IF < h->NF; ++IF)
+      for (int t = 0; t < (h->nz + LTW - 1) / LTW; ++t) per[5][m].push_back({m, t, IF});
   }
   std::vector<int> ord(nm);
   for (int m = 0; m < nm; ++m) ord[m] = m;
@@ -2003,7 +2012,7 @@ void batch_lists(const cgd_batch *b, int order, std::vector<WItem> out[5])
     std::stable_sort(ord.begin(), ord.end(), [&](int a, int c) {
       return (long long)b->mem[a]->NF * b->mem[a]->nz > (long long)b->mem[c]->NF * b->mem[c]->nz;
     });
-  for (int k = 0; k < 5; ++k) {
+  for (int k = 0; k < BATCH_LISTS; ++k) {
     out[k].clear();
     if (order == 2) {
       size_t mx = 0;
@@ -2026,6 +2035,8 @@ void batch_enqueue_t(cgd_batch *b, WItem *const *w, bool p2alt)
   const size_t csmem = (size_t)COL_WARPS * COL_ARR * b->nzmax * sizeof(double);
   if (first_on_device(attr)) {
     cudaFuncSetAttribute(kb_phase2<N, NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
+    cudaFuncSetAttribute(kb_hypervisc1w<N, NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)HV1Smem<N, NT, R, HV1Tile<N, R>::LT>::BYTES);
     if constexpr (N == 5)
       cudaFuncSetAttribute(kb_phase2<N, NT, R, P2_ALT_WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)CFA::SMEM);
@@ -2035,7 +2046,8 @@ void batch_enqueue_t(cgd_batch *b, WItem *const *w, bool p2alt)
   }
   kb_pressure<<<b->n[1], 256, 0, b->stream>>>(w[1], 0);
   for (int stage = 0; stage < 3; ++stage) {
-    kb_hypervisc1<N, NT, R><<<b->n[0], 256, 0, b->stream>>>(w[0], stage);
+    using HT = HV1Tile<N, R>;
+    kb_hypervisc1w<N, NT, R><<<b->n[5], HT::THREADS, HV1Smem<N, NT, R, HT::LT>::BYTES, b->stream>>>(w[5], stage);
     kb_gather<sizeof(R) == sizeof(float)><<<b->n[1], 256, 0, b->stream>>>(w[1]);
     if constexpr (N == 5) {
       if (p2alt) kb_phase2<N, NT, R, P2_ALT_WARPS><<<b->n[4], CFA::THREADS, CFA::SMEM, b->stream>>>(w[4], stage);
@@ -2250,9 +2262,9 @@ int cgd_batch_create(cgd_handle *const *members, int32_t nmembers, int32_t flags
     }
     const int nord = b->autotune ? cgd_batch::NORD : 1;
     for (int o = 0; o < nord && !rc; ++o) {
-      std::vector<WItem> lists[5];
+      std::vector<WItem> lists[BATCH_LISTS];
       batch_lists(b, o, lists);
-      for (int k = 0; k < 5; ++k) {
+      for (int k = 0; k < BATCH_LISTS; ++k) {
         b->n[k] = (int)lists[k].size();
         void *p = nullptr;
         e = cudaMalloc(&p, lists[k].size() * sizeof(WItem));
@@ -2280,7 +2292,7 @@ void cgd_batch_destroy(cgd_batch *b)
     if (b->graph[c]) cudaGraphDestroy(b->graph[c]);
   }
   for (int o = 0; o < cgd_batch::NORD; ++o)
-    for (int k = 0; k < 5; ++k)
+    for (int k = 0; k < BATCH_LISTS; ++k)
       if (b->w[o][k]) cudaFree(b->w[o][k]);
   for (void *p : b->scratch) cudaFree(p);
   for (double *p : b->C2) if (p) cudaFree(p);

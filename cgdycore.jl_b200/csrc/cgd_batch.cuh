@@ -39,12 +39,17 @@ __constant__ GP c_bgp[BMAX];
 __constant__ BMember c_bm[BMAX];
 __constant__ RK c_brk;
 
+// Phase 1 of the split form, with the single-member kernel's level tile
+// (HV1Tile) and its dynamic shared memory.
 template <int N, int NT, typename R>
-__global__ void __launch_bounds__(256, 4) kb_hypervisc1(const WItem *__restrict__ w, const int stage)
+__global__ void __launch_bounds__(HV1Tile<N, R>::THREADS, HV1Tile<N, R>::MINB)
+    kb_hypervisc1w(const WItem *__restrict__ w, const int stage)
 {
+  extern __shared__ __align__(16) unsigned char hvb_dyn[];
   const WItem it = w[blockIdx.x];
   const BMember &B = c_bm[it.m];
-  hypervisc1_body<N, NT, R>(c_bgp[it.m], stage == 0 ? B.U : B.Vst, B.C, it.x, it.y, hv1_static_smem<N, NT, R>());
+  hypervisc1_body<N, NT, R, HV1Tile<N, R>::LT>(c_bgp[it.m], stage == 0 ? B.U : B.Vst, B.C, it.x, it.y,
+                                               reinterpret_cast<R *>(hvb_dyn));
 }
 
 __global__ void __launch_bounds__(256) kb_pressure(const WItem *__restrict__ w, const int stage_state)
