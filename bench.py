@@ -751,6 +751,13 @@ def run_ours(args, cfg, rank, world, local):
         ensemble = ensemble_measure(args.ensemble_steps, 3, rank, ranks, torch)
         ensemble["single_member_dof_updates_per_s"] = value * unique_dof(cfg) / world
         ensemble["vs_single_member"] = ensemble["dof_updates_per_s"] / (value * unique_dof(cfg) / world)
+        if adjoint is not None:
+            # the members carry no tracers (5 fields per DOF); the same grid
+            # without tracers, stepped alone (the adjoint leg's forward step)
+            dof5 = unique_dof(cfg) // (5 + cfg.NumTr) * 5
+            single5 = dof5 / (adjoint["forward_step_ms"] * 1e-3)
+            ensemble["single_member_no_tracers_dof_updates_per_s"] = single5
+            ensemble["vs_single_member_no_tracers"] = ensemble["dof_updates_per_s"] / single5
 
     outp = None
     if args.precision == "fp64" and not args.no_output:

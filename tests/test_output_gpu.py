@@ -18,6 +18,29 @@ def case(oracle_mod):
     return o, g, U, nu
 
 
+@pytest.mark.parametrize("shape", [(3, 2, 7, 0), (4, 3, 8, 1), (2, 1, 5, 0)])
+def test_interpolate_lower_orders(built_lib, cuda_ok, oracle_mod, shape):
+    """Polynomial orders 1-3 (the vorticity kernel's other node counts),
+    OrdPrint 2, exact build, every kernel bit for bit."""
+    from _cases import make_case
+    from cgd_b200 import Dycore, _lib
+    from cgd_b200 import output
+    n, p, nz, nt = shape
+    o, g, U, nu = make_case(oracle_mod, n, p, nz, nt, "quadratic")
+    U = o.ros_step(U, 300.0, 1)
+    d = Dycore(g, nt, nu, exact=True)
+    inter = output.vtk_inter(p, 2, g.xw)
+    f = lambda k: np.asfortranarray(U[..., k])
+    assert np.array_equal(d.interpolate(f(1), inter), o.interpolate(f(1), inter))
+    assert np.array_equal(d.interpolate(f(4), inter, rhoc=f(0)), o.interpolate(f(4), inter, rhoc=f(0)))
+    assert np.array_equal(d.interpolate_wb(f(1), f(2), f(3), inter), o.interpolate_wb(f(1), f(2), f(3), inter))
+    assert np.array_equal(d.interpolate_vort(U, inter), o.interpolate_vort(U, inter))
+    out = d.output_fields(U, [_lib.OUT_PRES, _lib.OUT_VORT], inter)
+    assert np.array_equal(out[0].reshape(-1), o.interpolate(f(4), inter, kind=1).reshape(-1, order="F"))
+    assert np.array_equal(out[1].reshape(-1), o.interpolate_vort(U, inter).reshape(-1, order="F"))
+    d.close()
+
+
 def _tensor(a):
     import torch
     return torch.from_numpy(np.ascontiguousarray(np.asarray(a).transpose(*reversed(range(a.ndim))))).cuda()
