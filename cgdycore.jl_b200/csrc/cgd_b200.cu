@@ -100,6 +100,14 @@ struct cgd_handle {
   int nghost = 0, nsend = 0;
   std::vector<int32_t> nb_rank, send_ptr, recv_ptr;
   int *send_list = nullptr;                     // device copy
+  // elements [0, nbnd) touch other ranks (all sent contributions are theirs);
+  // the interior's phase 1 and phase 2 run on `side` while the boundary's
+  // contributions are exchanged
+  int nbnd = 0;
+  cudaStream_t side = nullptr;
+  cudaEvent_t xa = nullptr, xb = nullptr;
+  // element range of the next phase-1 / phase-2 launch ([el0, el0 + neln), all when neln < 0)
+  int el0 = 0, neln = -1;
   double *sbuf = nullptr, *rbuf = nullptr;      // packed contributions, NC*nz per item
   cgd_exchange_fn xfn = nullptr;
   void *xuser = nullptr;
@@ -170,6 +178,16 @@ bool is_device_ptr(const void *p)
 }
 
 
+// The element range of a phase-1 or phase-2 launch: all elements, or the
+// range the decomposed step set (cgd_handle::el0, neln).
+GP ranged_gp(const cgd_handle *h, int &nIF)
+{
+  GP gp = h->gp;
+  nIF = h->neln < 0 ? h->NF : h->neln;
+  gp.IF0 = h->neln < 0 ? 0 : h->el0;
+  return gp;
+}
+
 template <int N, int NT, typename R>
 void launch_hv1r(cgd_handle *h, const double *U, double *C)
 {
@@ -178,8 +196,11 @@ void launch_hv1r(cgd_handle *h, const double *U, double *C)
   static std::atomic<unsigned long long> attr{0};
   if (first_on_device(attr))
     cudaFuncSetAttribute(k_hypervisc1<N, NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  dim3 grid((h->nz + T::LT - 1) / T::LT, h->NF);   // the level tiles of one element run back to back
-  k_hypervisc1<N, NT, R><<<grid, T::THREADS, smem, h->stream>>>(h->gp, U, C);
+  int nIF;
+  const GP gp = ranged_gp(h, nIF);
+  if (nIF <= 0) return;
+  dim3 grid((h->nz + T::LT - 1) / T::LT, nIF);   // the level tiles of one element run back to back
+  k_hypervisc1<N, NT, R><<<grid, T::THREADS, smem, h->stream>>>(gp, U, C);
 }
 
 template <int N, int NT>
@@ -209,8 +230,11 @@ void launch_p2r(cgd_handle *h, const double *U, const double *Pr, const double *
   if (first_on_device(attr)) {
     cudaFuncSetAttribute(k_phase2<N, NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
   }
-  dim3 grid((h->nz + CF::LC - 1) / CF::LC, h->NF);
-  k_phase2<N, NT, R><<<grid, CF::THREADS, CF::SMEM, h->stream>>>(h->gp, U, Pr, T1, C);
+  int nIF;
+  const GP gp = ranged_gp(h, nIF);
+  if (nIF <= 0) return;
+  dim3 grid((h->nz + CF::LC - 1) / CF::LC, nIF);
+  k_phase2<N, NT, R><<<grid, CF::THREADS, CF::SMEM, h->stream>>>(gp, U, Pr, T1, C);
 }
 
 template <int N, int NT>
@@ -464,11 +488,22 @@ int callback_exchange(cgd_handle *h, int nf)
 // One step (or, with rhs_only, one tendency into F) of every part of a
 // decomposed grid, the parts' pieces interleaved with the exchanges.  n > 1:
 // an in-process group on parts[0]'s stream; n == 1: one rank of a
-// multi-process run, exchanging through its callback.
+// multi-process run, exchanging through its callback.  At both DSS points
+// the boundary elements' kernel runs first on the main stream, whose packing
+// and exchange then follow, while the interior elements' kernel runs on the
+// side stream; the main stream waits for it before the gather.
 int part_pieces(cgd_handle *const *parts, int n, double *const *U, double dt, bool rhs_only, double *const *F)
 {
   cgd_handle *h0 = parts[0];
+  cgd_handle *h = h0;   // for CK()
   const int nf1 = 5 + h0->NumTr, nf2 = h0->NV + 1;
+  bool interior = false;
+  for (int r = 0; r < n; ++r) interior = interior || parts[r]->nbnd < parts[r]->NF;
+  if (interior && !h0->side) {
+    CK(cudaStreamCreateWithFlags(&h0->side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h0->xa, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h0->xb, cudaEventDisableTiming));
+  }
   auto xchg = [&](int nf) -> int {
     for (int r = 0; r < n; ++r) halo_pack(parts[r], nf);
     int rc = n > 1 ? group_exchange(parts, n, nf, h0->stream) : callback_exchange(h0, nf);
@@ -476,20 +511,44 @@ int part_pieces(cgd_handle *const *parts, int n, double *const *U, double dt, bo
     for (int r = 0; r < n; ++r) halo_unpack(parts[r], nf);
     return CGD_OK;
   };
-  int e = 0;
+  // kern(r) launches part r's phase-1 or phase-2 kernel on its stream over
+  // its current element range
+  auto split = [&](int nf, auto &&kern) -> int {
+    if (!interior) {
+      for (int r = 0; r < n; ++r) kern(r);
+      return xchg(nf);
+    }
+    const cudaStream_t main = h0->stream;
+    CK(cudaEventRecord(h0->xa, main));
+    CK(cudaStreamWaitEvent(h0->side, h0->xa, 0));
+    for (int r = 0; r < n; ++r) {   // boundary elements, main stream
+      parts[r]->el0 = 0;
+      parts[r]->neln = parts[r]->nbnd;
+      kern(r);
+    }
+    for (int r = 0; r < n; ++r) {   // interior elements, side stream
+      cgd_handle *q = parts[r];
+      q->el0 = q->nbnd;
+      q->neln = q->NF - q->nbnd;
+      q->stream = h0->side;
+      kern(r);
+      q->stream = main;
+      q->neln = -1;
+    }
+    CK(cudaEventRecord(h0->xb, h0->side));
+    if (int rc = xchg(nf)) return rc;
+    CK(cudaStreamWaitEvent(main, h0->xb, 0));
+    return CGD_OK;
+  };
   if (rhs_only) {
+    if (int rc = split(nf1, [&](int r) { hv1(parts[r], U[r], parts[r]->C); })) return rc;
     for (int r = 0; r < n; ++r) {
-      cgd_handle *h = parts[r];
-      hv1(h, U[r], h->C);
+      cgd_handle *q = parts[r];
+      gather(q, q->C, q->T1, false);
+      pressure(q, U[r], q->pres);
     }
-    if (int rc = xchg(nf1)) return rc;
-    for (int r = 0; r < n; ++r) {
-      cgd_handle *h = parts[r];
-      gather(h, h->C, h->T1, false);
-      pressure(h, U[r], h->pres);
-      phase2(h, U[r], h->pres, h->T1, h->C);
-    }
-    if (int rc = xchg(nf2)) return rc;
+    if (int rc = split(nf2, [&](int r) { phase2(parts[r], U[r], parts[r]->pres, parts[r]->T1, parts[r]->C); }))
+      return rc;
     for (int r = 0; r < n; ++r) {
       gather(parts[r], parts[r]->C, F[r], true);
       physics(parts[r], U[r], parts[r]->pres, F[r]);
@@ -498,11 +557,18 @@ int part_pieces(cgd_handle *const *parts, int n, double *const *U, double dt, bo
   }
   std::vector<ColArgs> a(n);
   for (int r = 0; r < n; ++r) a[r] = step_args(parts[r], U[r], dt);
+  int e = 0;
   for (int stage = 0; stage < 3; ++stage) {
-    for (int r = 0; r < n; ++r) stage_piece(parts[r], U[r], a[r], stage, 0, e);
-    if (int rc = xchg(nf1)) return rc;
-    for (int r = 0; r < n; ++r) stage_piece(parts[r], U[r], a[r], stage, 1, e);
-    if (int rc = xchg(nf2)) return rc;
+    auto vsrc = [&](int r) -> const double * { return stage == 0 ? U[r] : parts[r]->Vst; };
+    if (stage == 0)
+      for (int r = 0; r < n; ++r) pressure(parts[r], U[r], parts[r]->pres);
+    if (int rc = split(nf1, [&](int r) { hv1(parts[r], vsrc(r), parts[r]->C); })) return rc;
+    for (int r = 0; r < n; ++r) gather(parts[r], parts[r]->C, parts[r]->T1, false);
+    auto p2 = [&](int r) {
+      cgd_handle *q = parts[r];
+      phase2(q, vsrc(r), stage == 0 ? q->pres : q->pres_st, q->T1, q->C);
+    };
+    if (int rc = split(nf2, p2)) return rc;
     for (int r = 0; r < n; ++r) stage_piece(parts[r], U[r], a[r], stage, 2, e);
   }
   return CGD_OK;
@@ -679,6 +745,14 @@ static int create_impl(const cgd_config *cfg, const int64_t *glob, const double 
     h->decomposed = true;
     h->nghost = nghost;
     h->nsend = nsend;
+    // the interior overlaps the exchanges only when every sent contribution
+    // is a boundary element's
+    h->nbnd = NF;
+    if (halo->nb_boundary >= 0 && halo->nb_boundary <= NF) {
+      bool ok = true;
+      for (int i = 0; i < nsend; ++i) ok = ok && halo->send_list[i] / DoF < halo->nb_boundary;
+      if (ok) h->nbnd = halo->nb_boundary;
+    }
     h->nb_rank.assign(halo->nb_rank, halo->nb_rank + nnb);
     h->send_ptr.assign(halo->send_ptr, halo->send_ptr + nnb + 1);
     h->recv_ptr.assign(halo->recv_ptr, halo->recv_ptr + nnb + 1);
@@ -844,6 +918,9 @@ void cgd_destroy(cgd_handle *h)
   for (int i = 0; i <= NPROF; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
   if (h->order_ev) cudaEventDestroy(h->order_ev);
+  if (h->xa) cudaEventDestroy(h->xa);
+  if (h->xb) cudaEventDestroy(h->xb);
+  if (h->side) cudaStreamDestroy(h->side);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }

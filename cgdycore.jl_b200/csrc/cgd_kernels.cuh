@@ -87,6 +87,7 @@ constexpr int MAXNV = 5 + MAXTR;
 struct GP {
   int N, DoF, nz, NF, NumG, NumTr, NV;
   int NC;                   // contribution slots per element node: NV fields + the lower-node w of phase 2
+  int IF0;                  // first element of a launch over a range of elements (k_hypervisc1, k_phase2)
   const double *met;        // [IF][comp][ID][nz]
   const double *M;          // (nz, NumG, 2)
   const double *dz;         // (nz, NumG)
@@ -333,7 +334,8 @@ __global__ void __launch_bounds__(HV1Tile<N, R>::THREADS, HV1Tile<N, R>::MINB)
     k_hypervisc1(const GP P, const double *__restrict__ U, double *__restrict__ C)
 {
   extern __shared__ __align__(16) unsigned char hv1_dyn[];
-  hypervisc1_body<N, NT, R, HV1Tile<N, R>::LT>(P, U, C, blockIdx.x, blockIdx.y, reinterpret_cast<R *>(hv1_dyn));
+  hypervisc1_body<N, NT, R, HV1Tile<N, R>::LT>(P, U, C, blockIdx.x, P.IF0 + blockIdx.y,
+                                               reinterpret_cast<R *>(hv1_dyn));
 }
 
 // Contributions and the phase-1 cache: double, or float in the mixed form

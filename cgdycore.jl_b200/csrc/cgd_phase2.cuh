@@ -621,7 +621,7 @@ __global__ void __launch_bounds__(P2Cfg<N, NT, R>::THREADS, P2Cfg<N, NT, R>::MIN
     k_phase2(const GP P, const double *__restrict__ U, const double *__restrict__ Pr, const double *__restrict__ T1,
              double *__restrict__ C)
 {
-  phase2_body<N, NT, R>(P, U, Pr, T1, C, blockIdx.x, blockIdx.y);
+  phase2_body<N, NT, R>(P, U, Pr, T1, C, blockIdx.x, P.IF0 + blockIdx.y);
 }
 
 }  // namespace cgd
