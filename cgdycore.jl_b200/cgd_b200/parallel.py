@@ -218,3 +218,19 @@ class TorchTransport:
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
+
+
+def global_mass_integral(local, group=None, device=None):
+    """Parallels.GlobalIntegral (src/Parallels/Exchange.jl:1163-1166) over a
+    decomposed grid: the sum over the ranks of each rank's mass integral
+    (`local`, e.g. Dycore.mass_integral of the rank's part, whose MMass
+    counts a DOF on its owner only; HaloPlan.local_grid), by one FP64
+    all-reduce.  device: where the reduced value lives (a CUDA device for
+    NCCL, None for host tensors with gloo).  The order of the ranks' partial
+    sums is the collective's, so the result agrees with a single-process sum
+    to rounding."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(local)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return float(t.item())

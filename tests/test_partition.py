@@ -122,8 +122,14 @@ def _gloo_worker(rank, world, port, out):
         C2 = o.contributions(U, T1)
         f = _ordered_dss(P, C2[..., P.elems], _exchange(P, T, C2[..., P.elems]))
         ok2 = np.array_equal(f, o.rhs(U)[:, P.dofs, :])
+        # the global mass integral from the ranks' partial sums (each DOF on its owner)
+        from cgd_b200.parallel import global_mass_integral
+        MM = np.asarray(P.local_grid(g).MMass)
+        part = float((U[:, P.dofs, 0] * MM).sum())
+        tot = global_mass_integral(part)
+        ok3 = abs(tot - o.mass_integral(U)) <= 1e-13 * abs(o.mass_integral(U))
         with open(os.path.join(out, f"r{rank}.txt"), "w") as fh:
-            fh.write(f"{int(ok1)} {int(ok2)} {P.n_ghost} {P.send_list.size}")
+            fh.write(f"{int(ok1)} {int(ok2)} {P.n_ghost} {P.send_list.size} {int(ok3)}")
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -137,7 +143,8 @@ def test_two_gloo_ranks_dss_matches_single_process(tmp_path, oracle_mod):
     s.close()
     mp.start_processes(_gloo_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
     for r in range(2):
-        ok1, ok2, ng, ns = open(tmp_path / f"r{r}.txt").read().split()
+        ok1, ok2, ng, ns, ok3 = open(tmp_path / f"r{r}.txt").read().split()
         assert ok1 == "1", f"rank {r}: phase-1 DSS differs from the single-process one"
         assert ok2 == "1", f"rank {r}: tendency differs from the single-process one"
+        assert ok3 == "1", f"rank {r}: the all-reduced mass integral differs from the single-process one"
         assert int(ng) > 0 and int(ns) > 0
