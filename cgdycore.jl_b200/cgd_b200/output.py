@@ -234,6 +234,7 @@ class VtkOutput:
         if isinstance(U, np.ndarray):
             out = self.d.output_fields(U, self.codes, self.inter)
             return {n: out[k].reshape(-1) for k, n in enumerate(self.vtk_names)}
+        self.wait()   # a background write may still read the pinned buffer
         host = self._device_to_host(U)
         self._event.synchronize()
         return self._split(host)
