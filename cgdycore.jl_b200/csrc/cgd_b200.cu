@@ -64,7 +64,7 @@ struct cgd_handle {
   std::vector<Buf> bufs;
   double *met = nullptr, *M = nullptr, *dz = nullptr;
   int *glob = nullptr, *inv_ptr = nullptr;
-  long long *inv_off = nullptr;
+  long long *inv_off = nullptr, *inv_tab = nullptr;
   double *C = nullptr, *T1 = nullptr, *Vst = nullptr, *k1 = nullptr, *k2 = nullptr;
   double *Ubuf = nullptr, *Fbuf = nullptr, *bands = nullptr, *part = nullptr, *scal = nullptr;
   double *jbg = nullptr;   // Jacobian bands of the current step, [8][NumG][nz-1]
@@ -827,6 +827,13 @@ static int create_impl(const cgd_config *cfg, const int64_t *glob, const double 
   TRY(dalloc(h, &h->glob, glob0.size()));
   TRY(dalloc(h, &h->inv_ptr, ptr.size()));
   TRY(dalloc(h, &h->inv_off, off.size()));
+  // the first four contributors of every DOF in one 32-byte row (-1 past the
+  // count; a DOF with more than four is marked -1 in its first entry)
+  std::vector<long long> tab((size_t)4 * NumG, -1);
+  for (int g = 0; g < NumG; ++g)
+    if (ptr[g + 1] - ptr[g] <= 4)
+      for (int q = ptr[g]; q < ptr[g + 1]; ++q) tab[(size_t)4 * g + (q - ptr[g])] = off[q];
+  TRY(dalloc(h, &h->inv_tab, tab.size()));
   // contribution buffer: the local elements, then the ghost pseudo-elements
   const size_t ghost_elems = ((size_t)nghost + DoF - 1) / DoF;
   TRY(dalloc(h, &h->C, ENL * (NV + 1) + ghost_elems * DoF * nz * (NV + 1)));
@@ -862,7 +869,7 @@ static int create_impl(const cgd_config *cfg, const int64_t *glob, const double 
   }
   if ((!dev_metric && up(h->met, met.data(), met.size() * 8)) || cudaGetLastError() != cudaSuccess || up(h->M, M, 2 * S * 8) || up(h->dz, dz, S * 8) ||
       up(h->glob, glob0.data(), glob0.size() * 4) || up(h->inv_ptr, ptr.data(), ptr.size() * 4) ||
-      up(h->inv_off, off.data(), off.size() * 8) ||
+      up(h->inv_off, off.data(), off.size() * 8) || up(h->inv_tab, tab.data(), tab.size() * 8) ||
       (halo && nsend && up(h->send_list, halo->send_list, (size_t)nsend * 4))) {
     cudaError_t e = cudaGetLastError();
     cuda_fail(h, e, "cgd_create upload");
@@ -879,6 +886,7 @@ static int create_impl(const cgd_config *cfg, const int64_t *glob, const double 
   GP &P = h->gp;
   P.N = N; P.DoF = DoF; P.nz = nz; P.NF = NF; P.NumG = NumG; P.NumTr = h->NumTr; P.NV = NV; P.NC = NV + 1;
   P.met = h->met; P.M = h->M; P.dz = h->dz; P.glob = h->glob; P.inv_ptr = h->inv_ptr; P.inv_off = h->inv_off;
+  P.inv_tab = h->inv_tab;
   P.pref = h->pref; P.thref = h->thref;
   for (int i = 0; i < 25; ++i) { P.D[i] = 0.0; P.DW[i] = 0.0; }
   for (int i = 0; i < N * N; ++i) { P.D[i] = DS[i]; P.DW[i] = DW[i]; }

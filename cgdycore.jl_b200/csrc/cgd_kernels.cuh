@@ -94,6 +94,7 @@ struct GP {
   const int *glob;          // [IF*DoF + ID], 0-based
   const int *inv_ptr;       // NumG + 1
   const long long *inv_off; // (IF*NC*DoF + ID)*nz for every contributor
+  const long long *inv_tab; // 4 per DOF: its first four inv_off entries, -1 past the count (-1 first: > 4)
   double D[25], DW[25];     // D[i + N*j] = DS[i,j]
   const double *pref;       // mixed form: per-level FP64 reference pressure and theta
   const double *thref;
@@ -393,33 +394,30 @@ template <bool WSPLIT, bool C32>
 __device__ __forceinline__ void gather_node(const GP &P, const double *__restrict__ C, int g, int l, size_t fstr,
                                             double *acc)
 {
-  const int q0 = P.inv_ptr[g], q1 = P.inv_ptr[g + 1];
-  const int nq = q1 - q0;
+  // one 32-byte row of the table gives the count and the offsets, so the
+  // contribution loads wait on a single index load
+  const longlong2 *t = reinterpret_cast<const longlong2 *>(P.inv_tab) + 2 * (size_t)g;
+  const longlong2 ta = t[0], tb = t[1];
   const bool wtop = WSPLIT && l == P.nz - 1;
-  long long o[4];
+  long long o[4] = {ta.x + l, ta.y + l, tb.x + l, tb.y + l};
+  const int nq = ta.x < 0 ? 0 : 1 + (ta.y >= 0) + (tb.x >= 0) + (tb.y >= 0);
   switch (nq) {
     case 1:
-      o[0] = P.inv_off[q0] + l;
       gather_nq<1, WSPLIT, C32>(P, C, o, wtop, fstr, acc);
       return;
     case 2:
-#pragma unroll
-      for (int j = 0; j < 2; ++j) o[j] = P.inv_off[q0 + j] + l;
       gather_nq<2, WSPLIT, C32>(P, C, o, wtop, fstr, acc);
       return;
     case 3:
-#pragma unroll
-      for (int j = 0; j < 3; ++j) o[j] = P.inv_off[q0 + j] + l;
       gather_nq<3, WSPLIT, C32>(P, C, o, wtop, fstr, acc);
       return;
     case 4:
-#pragma unroll
-      for (int j = 0; j < 4; ++j) o[j] = P.inv_off[q0 + j] + l;
       gather_nq<4, WSPLIT, C32>(P, C, o, wtop, fstr, acc);
       return;
     default:
       break;
   }
+  const int q0 = P.inv_ptr[g], q1 = P.inv_ptr[g + 1];
 #pragma unroll
   for (int f = 0; f < MAXNV; ++f) {
     if (f < P.NV) {
