@@ -183,8 +183,7 @@ struct HV1Smem {
 // Level tile of k_hypervisc1.  At p = 4 in FP64, 16 levels (400 threads,
 // three CTAs per SM): a warp then reads runs of 16 consecutive levels of two
 // nodes instead of 10 levels of three or four, so the metric and state loads
-// touch fewer L1 lines (the kernel is bound by the L1/shared-memory pipe):
-// 0.416 -> 0.310 ms on the drop-in grid.  Elsewhere 256 / N^2 levels (256
+// touch fewer L1 lines: 0.416 -> 0.310 ms on the drop-in grid.  Elsewhere 256 / N^2 levels (256
 // threads, four CTAs per SM), which the FP32 form also keeps (0.286 ms against
 // 0.316 ms with 16 levels).
 template <int N, typename R>
