@@ -8,8 +8,8 @@ Bars (from the hot-path contract):
 Two builds are checked.  The exact build evaluates the reference's
 expressions in the same order without contraction and sums the DSS in the
 oracle's order, so its results are asserted bit-identical.  The fast build
-(FMA contraction, reciprocal multiplies by time-invariant sums) is held to
-the tolerances.
+(reciprocal multiplies by time-invariant sums, the warp-scan tridiagonal
+solve; no contraction either) is held to the tolerances.
 """
 import numpy as np
 import pytest
