@@ -146,6 +146,29 @@ def oracle_steps_per_s(cfg, nsteps, warmup, threads):
     return nsteps / t, n
 
 
+def oracle_rhs_threads(cfg, threads):
+    """One tendency evaluation of the CPU restatement on all host threads and
+    on one thread (the same state): seconds each."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from cgd_b200 import physics as Ph
+    z = cfg.levels()
+    o = oracle.Oracle(cfg.nPanel, cfg.OrdPoly, cfg.nz, cfg.NumTr, z, H=cfg.H,
+                      nu=Ph.hyperdiffusion(cfg.nPanel, cfg.OrdPoly), Up=cfg.Up)
+    U = o.init_state(Ph.tracer_centres(cfg.NumTr, cfg.seed_tracer) if cfg.NumTr else None)
+    Ph.theta_noise(U, cfg.theta_noise, cfg.seed_theta)
+    out = []
+    for n in (threads, 1):
+        oracle.set_threads(n)
+        o.rhs(U)
+        t0 = time.perf_counter()
+        F = o.rhs(U)
+        out.append(time.perf_counter() - t0)
+        assert np.all(np.isfinite(F))
+    oracle.set_threads(threads)
+    return out
+
+
 def cpu_model():
     try:
         for line in open("/proc/cpuinfo"):
@@ -771,6 +794,13 @@ def run_ours(args, cfg, rank, world, local):
                "sample": f"{args.cpu_steps} full-grid Rosenbrock-W steps after 1 warm-up step of the same "
                          f"configuration; C++ FP64 restatement of the reference CPU path, OpenMP on {n} "
                          f"threads ({cpu_model()})"}
+        # one thread against all of them, on one tendency evaluation (a step
+        # on one thread would take tens of seconds)
+        tn, t1 = oracle_rhs_threads(cfg, n)
+        cpu["one_thread"] = {"tendency_s": t1, "tendency_s_all_threads": tn, "thread_speedup": t1 / tn,
+                             "steps_per_s_estimate": v * tn / t1,
+                             "sample": "one full-grid tendency evaluation after one untimed one, on 1 and on "
+                                       f"{n} threads; steps/s scaled by their ratio"}
 
     if rank == 0:
         peak, kind = measured_peak_hbm()
