@@ -627,7 +627,7 @@ def ensemble_measure(K, warmup, rank, ranks, torch):
             "ms_per_step": res["fp64"]["t"] / K * 1e3, "dof_per_ensemble_step": dof,
             "members": len(members), "grids": E["grids"], "per_grid": E["per_grid"], "dt": E["dt"],
             "hours": E["hours"], "steps_total": nsteps, "tuning_fp64": res["fp64"]["tuning"],
-            "chosen_form_fp64": "fused" if "stage=fused" in res["fp64"]["tuning"] else "split",
+            "chosen_form_fp64": res["fp64"]["tuning"].split("stage=")[1].split(";")[0],
             "mixed": {"dof_updates_per_s": vm, "speedup_vs_fp64": vm / v64,
                       "ms_per_step": res["mixed"]["t"] / K * 1e3, "tuning": res["mixed"]["tuning"],
                       "p1_rel_l2_vs_fp64": {"max": max(errs), "median": float(np.median(errs))},
@@ -635,7 +635,8 @@ def ensemble_measure(K, warmup, rank, ranks, torch):
             "mass_drift_fp64_max": float(max(abs(x) for x in res["fp64"]["drift"])),
             "finite": res["fp64"]["finite"] and res["mixed"]["finite"],
             "perturbation": f"theta +-{E['theta_amp']} K, u,v +-{E['wind_amp']} m/s, seed {E['seed0']}+member",
-            "gpu_launches": (3 if "stage=fused" in res["fp64"]["tuning"] else 15) * K}
+            "gpu_launches": {"fused": 3, "members": 15 * len(members)}.get(
+                res["fp64"]["tuning"].split("stage=")[1].split(";")[0], 15) * K}
 
 
 def run_ensemble(args, rank, world, local):

@@ -22,6 +22,7 @@ NOALLOC_SCRATCH_DOUBLES = 4 * 1024 * 1024
 FLAG_CHECK_FINITE = 1
 BATCH_AUTOTUNE = 1
 BATCH_FUSED = 2
+BATCH_MEMBERS = 4
 
 # every symbol declared in include/cgd_b200.h
 EXPORTS = [

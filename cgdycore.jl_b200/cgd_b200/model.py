@@ -502,17 +502,19 @@ class Ensemble:
     """Batched ensemble of Dycore members (same OrdPoly, NumTr and precision;
     any nPanel and nz): one ensemble step is one CUDA graph over flat work
     lists spanning every member (cgd_batch_step), either 15 launches or, with
-    fused=True (OrdPoly 4), one persistent cooperative launch per stage.
-    autotune=True times every work-list order in both forms and keeps the
-    fastest.  States are CUDA torch tensors, one per member, stepped in
+    fused=True (OrdPoly 4), one persistent cooperative launch per stage; or,
+    with members=True, one graph branch per member running that member's own
+    step.  autotune=True times every work-list order in every form and keeps
+    the fastest.  States are CUDA torch tensors, one per member, stepped in
     place."""
 
-    def __init__(self, members, autotune=False, fused=False):
+    def __init__(self, members, autotune=False, fused=False, members_form=False):
         self.members = list(members)
         self._L = self.members[0]._L
         arr = (ctypes.c_void_p * len(self.members))(*[m.h for m in self.members])
         b = ctypes.c_void_p()
-        flags = (_lib.BATCH_AUTOTUNE if autotune else 0) | (_lib.BATCH_FUSED if fused else 0)
+        flags = ((_lib.BATCH_AUTOTUNE if autotune else 0) | (_lib.BATCH_FUSED if fused else 0) |
+                 (_lib.BATCH_MEMBERS if members_form else 0))
         _lib.check(self._L.cgd_batch_create(arr, len(self.members), flags, ctypes.byref(b)), "cgd_batch_create")
         self.b = b
 
@@ -525,8 +527,8 @@ class Ensemble:
         _lib.check(self._L.cgd_batch_step(self.b, ptrs, dt, int(nsteps)), "cgd_batch_step")
 
     def tuning(self):
-        buf = ctypes.create_string_buffer(512)
-        _lib.check(self._L.cgd_batch_tuning(self.b, buf, 512), "cgd_batch_tuning")
+        buf = ctypes.create_string_buffer(1024)
+        _lib.check(self._L.cgd_batch_tuning(self.b, buf, 1024), "cgd_batch_tuning")
         return buf.value.decode()
 
     def stream(self):

@@ -2004,9 +2004,12 @@ struct cgd_batch {
   // work lists, one set per candidate order; a candidate is (order, form):
   // candidate c runs order c % NORD in form c / NORD: split into 15 launches
   // (FORM_SPLIT), split with phase 2 in 16-level CTAs (FORM_SPLIT16, p = 4),
-  // or as three fused stage launches (FORM_FUSED)
+  // as three fused stage launches (FORM_FUSED), or every member's own
+  // single-member step on its own stream inside the graph (FORM_MEMBERS;
+  // orders 0 and 1: one member after the other, as given or the largest
+  // first; order 2: all members as concurrent branches)
   static constexpr int NORD = 3;
-  static constexpr int FORM_SPLIT = 0, FORM_SPLIT16 = 1, FORM_FUSED = 2, NFORM = 3;
+  static constexpr int FORM_SPLIT = 0, FORM_SPLIT16 = 1, FORM_FUSED = 2, FORM_MEMBERS = 3, NFORM = 4;
   static constexpr int NCAND = NFORM * NORD;
   WItem *w[NORD][BATCH_LISTS] = {};
   int n[BATCH_LISTS] = {};
@@ -2025,14 +2028,27 @@ struct cgd_batch {
   std::vector<GP> gps;
   std::vector<BMember> bms;
   std::vector<void *> scratch;
+  // the members form: fork and join events, and the states and time steps
+  // its graphs were captured with (their kernels take the state pointers)
+  cudaEvent_t fork_ev = nullptr;
+  std::vector<cudaEvent_t> join_ev;
+  std::vector<double *> gU[NCAND];
+  std::vector<double> gdt[NCAND];
   std::string last_error;
 };
 
 namespace {
 
 const char *const ORDER_NAME[cgd_batch::NORD] = {"member-major", "largest-member-first", "members-interleaved"};
-const char *const FORM_NAME[cgd_batch::NFORM] = {"split", "split16", "fused"};
+const char *const FORM_NAME[cgd_batch::NFORM] = {"split", "split16", "fused", "members"};
 int form_of(int cand) { return cand / cgd_batch::NORD; }
+// the order's name; in the members form order 2 forks the members at once
+const char *order_name(int cand)
+{
+  return form_of(cand) == cgd_batch::FORM_MEMBERS && cand % cgd_batch::NORD == 2
+             ? "members-concurrent"
+             : ORDER_NAME[cand % cgd_batch::NORD];
+}
 // levels per phase-2 CTA of a form
 int phase2_levels(int N, int form)
 {
@@ -2243,6 +2259,39 @@ cudaError_t fused_setup_r(cgd_batch *b)
   }
 }
 
+// The members form: every member's step (the single-member kernels, its own
+// buffers) on the member's stream, forked from the batch stream and joined
+// back.  Orders 0 and 1 chain the members one after the other (as given, or
+// the largest first): each member then runs alone on the device, as in
+// cgd_ros_step.  Order 2 forks all members at once, one independent branch
+// each.
+cudaError_t batch_enqueue_members(cgd_batch *b, int order, double *const *U, const double *dt)
+{
+  const int nm = (int)b->mem.size();
+  const bool serial = order < 2;
+  std::vector<int> ord(nm);
+  for (int m = 0; m < nm; ++m) ord[m] = m;
+  if (order == 1)
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int c) {
+      return (long long)b->mem[a]->NF * b->mem[a]->nz > (long long)b->mem[c]->NF * b->mem[c]->nz;
+    });
+  cudaError_t e = serial ? cudaSuccess : cudaEventRecord(b->fork_ev, b->stream);
+  for (int m : ord) {
+    if (e != cudaSuccess) break;
+    cgd_handle *h = b->mem[m];
+    if (serial) e = cudaEventRecord(b->fork_ev, b->stream);   // after the previous member's join
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h->stream, b->fork_ev, 0);
+    if (e != cudaSuccess) break;
+    h->capturing = true;   // no profiling events inside the graph
+    enqueue_step(h, U[m], dt[m]);
+    h->capturing = false;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventRecord(b->join_ev[m], h->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join_ev[m], 0);
+  }
+  return e;
+}
+
 cudaError_t batch_enqueue(cgd_batch *b, int cand)
 {
   WItem *const *w = b->w[cand % cgd_batch::NORD];
@@ -2320,13 +2369,21 @@ int cgd_batch_create(cgd_handle *const *members, int32_t nmembers, int32_t flags
       fused_ok = coop && b->fgrid > 0;
     }
     if (want_fused && !fused_ok) { rc = CGD_ERR_UNSUPPORTED; break; }
-    const int first = want_fused ? cgd_batch::FORM_FUSED * cgd_batch::NORD : 0;
+    const bool want_members = (flags & CGD_BATCH_MEMBERS) != 0;
+    const int first = want_fused ? cgd_batch::FORM_FUSED * cgd_batch::NORD
+                                 : want_members ? cgd_batch::FORM_MEMBERS * cgd_batch::NORD : 0;
     for (int c = 0; c < cgd_batch::NCAND; ++c) {
       const int form = form_of(c);
       const bool avail = form == cgd_batch::FORM_SPLIT || (form == cgd_batch::FORM_SPLIT16 && b->N == 5) ||
-                         (form == cgd_batch::FORM_FUSED && fused_ok);
+                         (form == cgd_batch::FORM_FUSED && fused_ok) ||
+                         form == cgd_batch::FORM_MEMBERS;
       b->use[c] = b->autotune ? avail : c == first;
     }
+    e = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming);
+    b->join_ev.assign(nmembers, nullptr);
+    for (int m = 0; m < nmembers && e == cudaSuccess; ++m)
+      e = cudaEventCreateWithFlags(&b->join_ev[m], cudaEventDisableTiming);
+    if (e != cudaSuccess) { rc = batch_fail(b, e, "cgd_batch_create events"); break; }
     if (!b->autotune) b->chosen = first;
     if (fused_ok) {
       void *p = nullptr;
@@ -2384,6 +2441,9 @@ void cgd_batch_destroy(cgd_batch *b)
   for (double *p : b->Vst2) if (p) cudaFree(p);
   if (b->bar) cudaFree(b->bar);
   if (b->order_ev) cudaEventDestroy(b->order_ev);
+  if (b->fork_ev) cudaEventDestroy(b->fork_ev);
+  for (cudaEvent_t ev : b->join_ev)
+    if (ev) cudaEventDestroy(ev);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -2415,8 +2475,26 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
                           b->C2.empty() ? nullptr : b->C2[m], b->Vst2.empty() ? nullptr : b->Vst2[m]};
     }
   };
+  // the members form's graph for the given states and time steps (captured
+  // again when they change)
+  auto capture_members = [&](int c, double *const *state) -> int {
+    const std::vector<double *> su(state, state + nm);
+    const std::vector<double> sd(dt, dt + nm);
+    if (b->gexec[c] && b->gU[c] == su && b->gdt[c] == sd) return CGD_OK;
+    if (b->gexec[c]) { cudaGraphExecDestroy(b->gexec[c]); b->gexec[c] = nullptr; }
+    if (b->graph[c]) { cudaGraphDestroy(b->graph[c]); b->graph[c] = nullptr; }
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    const cudaError_t le = batch_enqueue_members(b, c % cgd_batch::NORD, state, dt);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph[c]);
+    if (le != cudaSuccess) return batch_fail(b, le, "cgd_batch_step members capture");
+    if (e != cudaSuccess) return batch_fail(b, e, "cgd_batch_step capture");
+    BCK(cudaGraphInstantiate(&b->gexec[c], b->graph[c], 0));
+    b->gU[c] = su;
+    b->gdt[c] = sd;
+    return CGD_OK;
+  };
   for (int c = 0; c < cgd_batch::NCAND; ++c) {
-    if (!b->use[c] || b->gexec[c]) continue;
+    if (!b->use[c] || b->gexec[c] || form_of(c) == cgd_batch::FORM_MEMBERS) continue;
     BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     const cudaError_t le = batch_enqueue(b, c);
     cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph[c]);
@@ -2458,6 +2536,7 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
       set_members(copies.data());
       int rc = batch_upload(b);
       if (rc) return rc;
+      if (form_of(c) == cgd_batch::FORM_MEMBERS && (rc = capture_members(c, copies.data()))) return rc;
       BCK(cudaGraphLaunch(b->gexec[c], b->stream));
       BCK(cudaEventRecord(e0, b->stream));
       BCK(cudaGraphLaunch(b->gexec[c], b->stream));
@@ -2479,6 +2558,7 @@ int cgd_batch_step(cgd_batch *b, double *const *U, const double *dt, int32_t nst
   set_members(U);
   int rc = batch_upload(b);
   if (rc) return rc;
+  if (form_of(b->chosen) == cgd_batch::FORM_MEMBERS && (rc = capture_members(b->chosen, U))) return rc;
   for (int s = 0; s < nsteps; ++s) BCK(cudaGraphLaunch(b->gexec[b->chosen], b->stream));
   BCK(cudaStreamSynchronize(b->stream));
   BCK(cudaGetLastError());
@@ -2535,14 +2615,15 @@ int cgd_batch_tuning(cgd_batch *b, char *desc, int32_t len)
 {
   if (!b || !desc || len < 1) return CGD_ERR_INVALID_ARG;
   const int form = form_of(b->chosen);
-  std::string s = std::string("order=") + ORDER_NAME[b->chosen % cgd_batch::NORD] + ";stage=" +
-                  (form == cgd_batch::FORM_FUSED ? "fused" : "split") + ";phase2_levels=" +
+  std::string s = std::string("order=") + order_name(b->chosen) + ";stage=" +
+                  (form == cgd_batch::FORM_FUSED ? "fused" : form == cgd_batch::FORM_MEMBERS ? "members" : "split") +
+                  ";phase2_levels=" +
                   std::to_string(phase2_levels(b->N, form));
   if (b->tuned) {
     char buf[96];
     for (int c = 0; c < cgd_batch::NCAND; ++c) {
       if (!b->use[c]) continue;
-      snprintf(buf, sizeof buf, ";%s/%s=%.3fms", ORDER_NAME[c % cgd_batch::NORD], FORM_NAME[form_of(c)],
+      snprintf(buf, sizeof buf, ";%s/%s=%.3fms", order_name(c), FORM_NAME[form_of(c)],
                b->tune_ms[c]);
       s += buf;
     }

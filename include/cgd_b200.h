@@ -372,14 +372,23 @@ int cgd_jac_schur_solve_noalloc(const cgd_config *cfg, const double *U, const do
  * step returns CGD_ERR_TIMEOUT).  Calls on different batches must not run
  * concurrently: they share those constant tables.  The member handles must
  * stay alive and must not be stepped on their own while their batch steps.
+ * With CGD_BATCH_MEMBERS the graph instead holds every member's own step
+ * (the single-member kernels and buffers, bit-identical to cgd_ros_step of
+ * that member) on the member's stream, forked from the batch stream and
+ * joined back, the members one after the other (members form); its kernels
+ * take the state pointers, so its graph is captured again when the states
+ * or time steps passed to cgd_batch_step change.
  * With CGD_BATCH_AUTOTUNE the first cgd_batch_step times the candidates -
  * each work-list order (member-major, largest member first, interleaved) in
  * the split form and, for OrdPoly 4, in the split form with phase 2 in
- * 8-level instead of 16-level CTAs and in the fused form - on copies of the
- * states and keeps the fastest; cgd_batch_tuning reports it.
+ * 8-level instead of 16-level CTAs and in the fused form, and the members
+ * form with the members in the given order, the largest first, or all at
+ * once as concurrent branches - on copies of the states and keeps the
+ * fastest; cgd_batch_tuning reports it.
  * No counterpart in the reference, which runs one configuration per job. */
 #define CGD_BATCH_AUTOTUNE 1
 #define CGD_BATCH_FUSED 2
+#define CGD_BATCH_MEMBERS 4
 typedef struct cgd_batch cgd_batch;
 int cgd_batch_create(cgd_handle *const *members, int32_t nmembers, int32_t flags, cgd_batch **out);
 /* U[m] device pointers, dt[m] step sizes; nsteps ensemble steps, in place. */

@@ -1,10 +1,11 @@
 """Batched ensemble on the GPU: members on different grids (nPanel, nz) and
 with different dt advance together through cgd_batch_step, one graph per
-ensemble step: 15 launches (split form) or one persistent cooperative launch
-per stage (fused form).  Both forms run the single-member kernel bodies on
-the same data in the same order, so every member must come out bit-identical
-to stepping it on its own, in either form and with or without the
-autotuner."""
+ensemble step: 15 launches (split form), one persistent cooperative launch
+per stage (fused form), or one graph branch per member running that
+member's own step (members form).  All forms run the single-member kernel
+bodies on the same data in the same order, so every member must come out
+bit-identical to stepping it on its own, in every form and with or without
+the autotuner."""
 import numpy as np
 import pytest
 
@@ -33,10 +34,11 @@ def _host(t):
     return t.cpu().numpy().transpose(2, 1, 0)
 
 
-@pytest.mark.parametrize("exact,autotune,precision,fused", [(True, False, "fp64", False), (False, True, "fp64", False),
-                                                            (False, False, "mixed", False), (True, False, "fp64", True),
-                                                            (False, False, "fp64", True), (False, False, "mixed", True)])
-def test_batch_matches_members(oracle_mod, built_lib, cuda_ok, exact, autotune, precision, fused):
+@pytest.mark.parametrize("exact,autotune,precision,form", [
+    (True, False, "fp64", "split"), (False, True, "fp64", "split"), (False, False, "mixed", "split"),
+    (True, False, "fp64", "fused"), (False, False, "fp64", "fused"), (False, False, "mixed", "fused"),
+    (True, False, "fp64", "members"), (False, False, "mixed", "members")])
+def test_batch_matches_members(oracle_mod, built_lib, cuda_ok, exact, autotune, precision, form):
     import torch
     from cgd_b200 import Ensemble
     mem = _members(oracle_mod, exact, precision)
@@ -49,18 +51,22 @@ def test_batch_matches_members(oracle_mod, built_lib, cuda_ok, exact, autotune, 
     # fresh handles for the batch (a mixed handle keeps the reference profile
     # of its first state, the same here)
     mem2 = _members(oracle_mod, exact, precision)
-    ens = Ensemble([d for d, _, _ in mem2], autotune=autotune, fused=fused)
+    ens = Ensemble([d for d, _, _ in mem2], autotune=autotune, fused=form == "fused",
+                   members_form=form == "members")
     states = [_dev(U) for _, U, _ in mem2]
     ens.step(states, [dt for _, _, dt in mem2], 2)
+    # the last step on copies: new state pointers (the members form captures
+    # its graph again)
+    states = [s.clone() for s in states]
     ens.step(states, [dt for _, _, dt in mem2], 1)
     torch.cuda.synchronize()
     for r, s in zip(ref, states):
         assert np.array_equal(_host(s), r)
     desc = ens.tuning()
     assert desc.startswith("order=")
-    assert ("stage=fused" in desc) == fused or autotune
-    if autotune:   # three orders x split, split with 8-level phase-2 CTAs, fused (OrdPoly 4)
-        assert desc.count("ms") == 9, desc
+    assert f"stage={form}" in desc or autotune
+    if autotune:   # three orders x split, split with 8-level phase-2 CTAs, fused (OrdPoly 4), members
+        assert desc.count("ms") == 12, desc
         assert "phase2_levels=" in desc
     ens.close()
     for d, _, _ in mem + mem2:
