@@ -187,11 +187,12 @@ mutable struct Batch
   members::Vector{Handle}
 end
 
-function Batch(members::Vector{Handle}; autotune = true, fused = false)
+function Batch(members::Vector{Handle}; autotune = true, fused = false, members_form = false)
   out = Ref{Ptr{Cvoid}}(C_NULL)
   ptrs = [m.ptr for m in members]
+  flags = (autotune ? 1 : 0) | (fused ? 2 : 0) | (members_form ? 4 : 0)
   check(ccall((:cgd_batch_create, libcgd), Cint, (Ptr{Ptr{Cvoid}}, Int32, Int32, Ref{Ptr{Cvoid}}),
-              ptrs, Int32(length(ptrs)), Int32((autotune ? 1 : 0) | (fused ? 2 : 0)), out), "cgd_batch_create")
+              ptrs, Int32(length(ptrs)), Int32(flags), out), "cgd_batch_create")
   b = Batch(out[], members)
   finalizer(x -> ccall((:cgd_batch_destroy, libcgd), Cvoid, (Ptr{Cvoid},), x.ptr), b)
   b
