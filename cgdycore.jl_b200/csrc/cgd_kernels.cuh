@@ -499,10 +499,17 @@ struct ColArgs {
 };
 
 constexpr int COL_WARPS = 8;
-// per warp: fv of rho, w, rho*theta, 8 bands, tri[3], x, and the step's
-// initial rho, w, rho*theta (copied in asynchronously at the start and read
-// by the stage update at the end); each nz long
-constexpr int COL_ARR = 18;
+// per warp: fv of rho, w, rho*theta, 8 bands, tri[3], x; each nz long.  (The
+// step's initial rho, w, rho*theta were once copied into three more arrays
+// by cp.async at the start for the update at the end; reading them at the
+// update instead is faster: 0.426/0.449 -> 0.411/0.427 ms for the second and
+// third stage on the drop-in grid, the smaller arrays leaving more L1.)
+constexpr int COL_ARR = 15;
+// CTAs per SM the column kernel's registers are sized for: five for the first
+// stage (48 registers; 0.474 -> 0.464 ms on the drop-in grid), four for the
+// others (64 registers; five cost them 4-20 %)
+template <int MODE>
+constexpr int col_min_blocks() { return MODE == 0 ? 5 : 4; }
 
 // dPresdRhoTh (src/Models/Equation.jl:33-36) of one level
 __device__ __forceinline__ double dpdrhoth(const GP &P, double RhoTh0)
@@ -651,7 +658,6 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
   double *jb = sw + 3 * LS;             // [8][nz]
   double *tri = jb + 8 * LS;            // [3][nz]
   double *xs = tri + 3 * LS;            // [nz]
-  double *vns = xs + LS;                // [3][nz]: Vn of rho, w, rho*theta
   const size_t fs = (size_t)nz * NumG;
   const double fac = A.fac;
   // k1, k2 of the Schur fields (rho, w, rho*theta), kept for the update
@@ -665,10 +671,6 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
     if (!valid || l >= nz) continue;
     const size_t o0 = l + (size_t)nz * g;
     if (MODE <= 2) {
-      // the step's initial rho, w, rho*theta for the update at the end, in flight meanwhile
-      cp_async8(vns + l, A.Vn + o0);
-      cp_async8(vns + LS + l, A.Vn + o0 + 3 * fs);
-      cp_async8(vns + 2 * LS + l, A.Vn + o0 + 4 * fs);
       const size_t fstr = (size_t)P.DoF * nz;
       double gacc[MAXNV];
       gather_node<true, C32>(P, A.C, g, l, fstr, gacc);
@@ -807,7 +809,6 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
   __syncthreads();
 #endif
   if (!valid) return;
-  if (MODE <= 2) cp_async_wait_all();   // this lane's copies of Vn (its own levels only)
   // SchurSolveBKernel! and the stage update of rho, w, rho*theta; each lane
   // owns levels lane and lane + 32
 #pragma unroll
@@ -841,16 +842,16 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
       const size_t o = o0 + f * fs;
       const double k = kk[sf];
       if (MODE == 0) {
-        const double vn = vns[sf * LS + l];
+        const double vn = A.Vn[o];
         A.kout[o] = k;
         A.Vout[o] = vn + A.rk.a[1][0] * k;
       } else if (MODE == 1) {
-        const double vn = vns[sf * LS + l];
+        const double vn = A.Vn[o];
         A.kout[o] = k;
         A.Vout[o] = vn + A.rk.a[2][0] * s1[it][sf] + A.rk.a[2][1] * k;
       } else if (MODE == 2) {
-        // Vout may alias Vn: this lane alone read index o (at the start) and writes it
-        const double vn = vns[sf * LS + l];
+        // Vout may alias Vn: this lane alone reads index o and then writes it
+        const double vn = A.Vn[o];
         A.Vout[o] = vn + A.rk.m[0] * s1[it][sf] + A.rk.m[1] * s2[it][sf] + A.rk.m[2] * k;
         if (A.kout) A.kout[o] = k;   // the last stage's k of rho, w, rho*theta (adjoint replay only)
       } else {
@@ -865,7 +866,7 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
 }
 
 template <int MODE, bool C32>
-__global__ void __launch_bounds__(32 * COL_WARPS, 4) k_column(const GP P, const ColArgs A)
+__global__ void __launch_bounds__(32 * COL_WARPS, col_min_blocks<MODE>()) k_column(const GP P, const ColArgs A)
 {
   column_body<MODE, C32>(P, A, blockIdx.x);
 }
