@@ -663,6 +663,20 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
   // k1, k2 of the Schur fields (rho, w, rho*theta), kept for the update
   double s1[2][3], s2[2][3];
 
+  // stages 2 and 3: the stored bands of the step are copied into the warp's
+  // band rows first, so that they are in flight with the gather's loads
+  if ((MODE == 1 || MODE == 2) && valid) {
+    const size_t js = (size_t)NumG * n;
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+      const int l = lane + 32 * it;
+      if (l >= n) continue;
+      const double *jg = A.jbg + (size_t)g * n + l;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) cp_async8(jb + r * LS + l, jg + r * js);
+    }
+  }
+
   // 1. tendency (owner gather) + stage corrections; fields outside the Schur
   //    system finished here; bands
 #pragma unroll
@@ -727,8 +741,9 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
       }
     }
   }
-  if (MODE <= 2) {
-    if (MODE == 0) __syncwarp();
+  if (MODE == 1 || MODE == 2) cp_async_wait_all();   // this lane's band copies; the warp sync below publishes them
+  if (MODE == 0) {
+    __syncwarp();
 #pragma unroll
     for (int it = 0; it < 2; ++it) {
       const int l = lane + 32 * it;
@@ -745,9 +760,6 @@ __device__ __forceinline__ void column_body(const GP &P, const ColArgs &A, const
           jb[r * LS + l] = b[r];
           jg[r * js] = b[r];
         }
-      } else {
-#pragma unroll
-        for (int r = 0; r < 8; ++r) jb[r * LS + l] = jg[r * js];
       }
     }
   }
