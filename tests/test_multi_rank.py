@@ -71,3 +71,27 @@ def test_single_rank_plumbing():
     r.barrier()
     assert r.max(2.5) == 2.5
     assert bench.aggregate(1, 100, 2.0) == 50.0
+
+
+def test_reference_arm_line_on_rank_zero(capsys):
+    """Rank 0 prints one JSON line with the contract's keys: the CPU
+    restatement's rate as value, cpu_baseline describing the same run, and an
+    e2e object with no host-device bytes (the CPU arm copies nothing)."""
+    import json
+
+    import bench
+    from cgd_b200 import physics as Ph
+
+    class A:
+        steps, warmup, gpus = 1, 1, 1
+    bench.run_reference(A, Ph.CONFIGS["small"], rank=0)
+    lines = [l for l in capsys.readouterr().out.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "steps/s" and d["higher_is_better"] is True
+    assert d["steps"] == 1 and d["warmup"] == 1 and d["n_gpus"] == 1
+    assert d["value"] > 0 and abs(d["ms_per_step"] - 1e3 / d["value"]) <= 1e-6 * d["ms_per_step"]
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]
+    assert cb["value"] == d["value"] and cb["unit"] == d["unit"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
