@@ -4,6 +4,11 @@ The oracle is an FP64 CPU restatement of CGDycore.jl's spectral-element hot
 path (see cgd_oracle.cpp for the file:line of every restated function).  It is
 used by the tests, by ``__graft_entry__.smoke()`` and by the CPU-baseline leg
 of ``bench.py`` to check the product; the product never imports it.
+
+Pinning: the Glob numbering is pinned bit for bit to the reference's own
+GlobInd golden file; the floating-point restatement is parity unpinned (the
+reference records no floating-point vectors for this path and Julia cannot
+run here), checked by analytic invariants only.
 """
 import ctypes
 import os
